@@ -1,0 +1,244 @@
+"""ctypes binding of the C ABI in ``include/fastctqw_b200.h``.
+
+The shared library ``lib/libfastctqw_b200.so`` (built by ``python -m fastctqw_b200.build``)
+is the only compute path.  There is no CPU fallback: if the library or an sm_100 device
+is missing, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libfastctqw_b200.so")
+
+F32, F64, C64, C128 = 0, 1, 2, 3
+DTYPE_CODE = {np.dtype(np.float32): F32, np.dtype(np.float64): F64,
+              np.dtype(np.complex64): C64, np.dtype(np.complex128): C128}
+CODE_DTYPE = {v: k for k, v in DTYPE_CODE.items()}
+
+FORM_PLAIN, FORM_MIXED, FORM_SIMT, FORM_FP64 = 0, 1, 2, 3
+FORMS = {"plain": FORM_PLAIN, "mixed": FORM_MIXED, "simt": FORM_SIMT, "fp64": FORM_FP64}
+OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE, OPT_DEBUG_STAGE = range(9)
+
+OK, ERR_TYPE, ERR_VALUE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_NONFINITE, ERR_SINGULAR, ERR_NODEV, ERR_FREED = range(10)
+
+
+class FxStats(ctypes.Structure):
+    _fields_ = [("m", ctypes.c_int32), ("s", ctypes.c_int32), ("form", ctypes.c_int32),
+                ("structured", ctypes.c_int32), ("rank1_shift", ctypes.c_int32),
+                ("symmetric", ctypes.c_int32), ("gemm_launches", ctypes.c_int32),
+                ("launches", ctypes.c_int32), ("norm1", ctypes.c_double),
+                ("d", ctypes.c_double * 5), ("ms_total", ctypes.c_double),
+                ("flops", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        out = {k: getattr(self, k) for k, _ in self._fields_ if k != "d"}
+        out["d4"], out["d6"], out["d8"], out["d10"], out["log2_abs27"] = list(self.d)
+        return out
+
+
+_lib = None
+_lock = threading.Lock()
+
+# (name, argtypes) of every symbol declared in include/fastctqw_b200.h
+SIGNATURES = {
+    "fx_create": [ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "fx_destroy": [ctypes.c_void_p],
+    "fx_free": [ctypes.c_void_p],
+    "fx_get_n": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)],
+    "fx_set_option": [ctypes.c_void_p, ctypes.c_int, ctypes.c_double],
+    "fx_get_stats": [ctypes.c_void_p, ctypes.POINTER(FxStats)],
+    "fx_last_error": [ctypes.c_void_p],
+    "fx_run_host": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    "fx_run_device": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    "fx_walk_device": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                       ctypes.c_void_p, ctypes.c_void_p],
+    "fx_walk_host": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    "fx_fetch_u": [ctypes.c_void_p, ctypes.c_void_p],
+    "fx_product_f32": [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                       ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                       ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int64,
+                       ctypes.c_float, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
+    "fx_product_error": [],
+    "fx_gpu_memory_gb": [],
+    "fx_device_ok": [],
+    "fx_version": [],
+}
+RESTYPES = {"fx_last_error": ctypes.c_char_p, "fx_version": ctypes.c_char_p,
+            "fx_product_error": ctypes.c_char_p,
+            "fx_gpu_memory_gb": ctypes.c_double}
+
+
+def lib() -> ctypes.CDLL:
+    """Load the native library (once).  Raises ImportError when it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"native library missing: {LIB_PATH} (build it with python -m fastctqw_b200.build)")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, args in SIGNATURES.items():
+                f = getattr(L, name)
+                f.argtypes = args
+                f.restype = RESTYPES.get(name, ctypes.c_int)
+            _lib = L
+    return _lib
+
+
+def last_error(h=None) -> str:
+    msg = lib().fx_last_error(h)
+    return msg.decode() if msg else ""
+
+
+def check(rc: int, h=None) -> None:
+    if rc == OK:
+        return
+    msg = last_error(h) or f"error code {rc}"
+    if rc == ERR_TYPE:
+        raise TypeError(msg)
+    if rc in (ERR_VALUE, ERR_NONFINITE):
+        raise ValueError(msg)
+    if rc == ERR_NOMEM:
+        raise MemoryError(msg)
+    raise RuntimeError(msg)
+
+
+def product_f32(form: str, A, Bt, alpha=1.0, beta=0.0, C=None, gamma=0.0, D=None):
+    """D = alpha A Bt^T + beta C + gamma I with torch CUDA float32 tensors (diagnostic)."""
+    import torch
+    M, K = A.shape
+    N = Bt.shape[0]
+    if D is None:
+        D = torch.empty((M, N), device=A.device, dtype=torch.float32)
+    rc = lib().fx_product_f32(FORMS[form], M, N, K, A.data_ptr(), A.stride(0), Bt.data_ptr(),
+                              Bt.stride(0), alpha, beta, C.data_ptr() if C is not None else None,
+                              C.stride(0) if C is not None else 0, gamma, D.data_ptr(), D.stride(0),
+                              torch.cuda.current_stream().cuda_stream)
+    if rc != OK:
+        raise RuntimeError(lib().fx_product_error().decode())
+    return D
+
+
+def device_ok() -> bool:
+    return bool(lib().fx_device_ok())
+
+
+class Engine:
+    """Owner of one native fx_engine handle (workspace for n x n matrices of one dtype)."""
+
+    def __init__(self, n: int, dtype) -> None:
+        self.dtype = np.dtype(dtype)
+        if self.dtype not in DTYPE_CODE:
+            raise TypeError(f"unsupported dtype {self.dtype}")
+        if int(n) < 0:
+            raise ValueError("n must be non-negative")
+        self.n = int(n)
+        h = ctypes.c_void_p()
+        check(lib().fx_create(self.n, DTYPE_CODE[self.dtype], ctypes.byref(h)))
+        self._h = h
+        self._freed = False
+
+    # -- options
+    def set_option(self, key: int, value: float) -> None:
+        check(lib().fx_set_option(self._h, int(key), float(value)), self._h)
+
+    def configure(self, form: str | None = None, shift: int | None = None,
+                  structure: bool | None = None, force_m: int | None = None,
+                  force_s: int | None = None, ipe: bool | None = None,
+                  timeout_ms: float | None = None, debug_stage: int | None = None) -> None:
+        if form is not None:
+            if form not in FORMS:
+                raise ValueError(f"form must be one of {sorted(FORMS)}")
+            self.set_option(OPT_FORM, FORMS[form])
+        if shift is not None:
+            self.set_option(OPT_SHIFT, shift)
+        if structure is not None:
+            self.set_option(OPT_STRUCTURE, int(bool(structure)))
+        if force_m is not None:
+            self.set_option(OPT_FORCE_M, force_m)
+        if force_s is not None:
+            self.set_option(OPT_FORCE_S, force_s)
+        if ipe is not None:
+            self.set_option(OPT_IPE, int(bool(ipe)))
+        if timeout_ms is not None:
+            self.set_option(OPT_TIMEOUT_MS, timeout_ms)
+        if debug_stage is not None:
+            self.set_option(OPT_DEBUG_STAGE, debug_stage)
+
+    def stats(self) -> dict:
+        st = FxStats()
+        check(lib().fx_get_stats(self._h, ctypes.byref(st)), self._h)
+        return st.as_dict()
+
+    # -- host buffers
+    def _host_in(self, A) -> np.ndarray:
+        A = np.ascontiguousarray(A, dtype=self.dtype)  # forcecast, like pybind11 array_t<T>
+        if A.shape != (self.n, self.n):
+            raise ValueError(f"Input matrix must have shape ({self.n}, {self.n}).")
+        return A
+
+    def run_host(self, A) -> np.ndarray:
+        A = self._host_in(A)
+        U = np.empty((self.n, self.n), dtype=self.dtype)
+        check(lib().fx_run_host(self._h, A.ctypes.data, U.ctypes.data), self._h)
+        return U
+
+    def walk_host(self, A, psi0) -> np.ndarray:
+        A = self._host_in(A)
+        vdt = np.complex128 if self.dtype in (np.dtype(np.complex128), np.dtype(np.float64)) else np.complex64
+        psi0 = np.ascontiguousarray(psi0, dtype=vdt).reshape(-1)
+        if psi0.shape != (self.n,):
+            raise ValueError(f"state must have length {self.n}")
+        psi = np.empty(self.n, dtype=vdt)
+        check(lib().fx_walk_host(self._h, A.ctypes.data, psi0.ctypes.data, psi.ctypes.data), self._h)
+        return psi
+
+    def fetch_u(self) -> np.ndarray:
+        """U of the last walk_host call (it stays on the device until asked for)."""
+        U = np.empty((self.n, self.n), dtype=self.dtype)
+        check(lib().fx_fetch_u(self._h, U.ctypes.data), self._h)
+        return U
+
+    # -- device buffers (torch tensors or raw pointers)
+    @staticmethod
+    def _ptr(x) -> int:
+        return x.data_ptr() if hasattr(x, "data_ptr") else int(x)
+
+    @staticmethod
+    def _stream(stream) -> int:
+        if stream is None:
+            try:
+                import torch
+                return torch.cuda.current_stream().cuda_stream
+            except Exception:  # noqa: BLE001 - plain pointer callers pass their own stream
+                return 0
+        return int(getattr(stream, "cuda_stream", stream))
+
+    def run_device(self, dA, dU, stream=None) -> None:
+        check(lib().fx_run_device(self._h, self._ptr(dA), self._ptr(dU), self._stream(stream)), self._h)
+
+    def walk_device(self, dA, dpsi0, dpsi, dU=None, stream=None) -> None:
+        check(lib().fx_walk_device(self._h, self._ptr(dA), self._ptr(dpsi0), self._ptr(dpsi),
+                                   self._ptr(dU) if dU is not None else None,
+                                   self._stream(stream)), self._h)
+
+    def free(self) -> None:
+        if not self._freed:
+            check(lib().fx_free(self._h), self._h)
+            self._freed = True
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().fx_destroy(self._h)
+            self._h = None
+            self._freed = True
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

@@ -1,0 +1,507 @@
+// Matrix product on the int8 tensor cores (tcgen05.mma kind::i8) with EXACT accumulation:
+// an Ozaki-style splitting (Ozaki, Ogita, Oishi, Rump 2012, "Error-free transformations of
+// matrix multiplication by using fast routines of matrix multiplication").
+//
+// Every row i of the left factor A (and every row j of the transposed right factor Bt) is
+// scaled by a power of two 2^-e so that |x| <= 127.5/128, then cut into S signed slices by
+// round-to-nearest (unbiased -- truncation toward zero biases every product coherently):
+//     x = sum_{p=1..S} s_p 2^(-7p) + r,   s_1 in [-127, 127], s_p in [-64, 64],  |r| <= 2^-(7S+1).
+// The product sum_k x_ik y_jk is assembled from the slice products with p + q <= S + 1,
+// grouped by "level" l = p + q in S int32 accumulators in tensor memory (TMEM):
+//     L_l = sum_{p+q=l} S_p T_q^T        (exact for K <= 32768)
+// and the epilogue forms  D = 2^(e_i + f_j - 14) * sum_l 2^(-7(l-2)) L_l  in FP64 before the
+// single rounding to the output type.  There is no accumulation error; the error is the slice
+// remainder (2^-(7S+1) relative to the row maximum) and the final rounding.  The FP32
+// accumulator of the BF16 MMAs, by contrast, truncates at every K = 16 step (error linear in
+// K), which the 2^s amplification of the squaring phase cannot afford.
+//
+//   S = 4: 10 int8 MMAs per K step (the time of 5 BF16 products), 28-bit slices, 128 x 128
+//          tiles, 4 x 128 TMEM columns.
+//   S = 5: 15 int8 MMAs (7.5 BF16 products), 35-bit slices for FP64 operands whose rows are
+//          dominated by a few entries (the diagonal of the walk generators), 128 x 96 tiles,
+//          5 x 96 TMEM columns.
+//
+// Kernel layout: persistent CTAs, K step 64 bytes (64B swizzle), one stage = S A-slice tiles +
+// S Bt-slice tiles, 3 stages; warp 0 TMA producer, warp 1 MMA issuer, warps 2-5 epilogue.
+// Symmetric-output mode computes only tiles touching the upper triangle and mirrors them.
+// All waits are bounded (see fx_tc_common.cuh).
+#include "fx_kernels.cuh"
+#include "fx_tc_common.cuh"
+
+namespace fx {
+namespace {
+using namespace tc;
+
+constexpr int kBM = 128, kBK = 64;  // kBK in int8 elements (= bytes)
+constexpr int kMaxSlices = 5;
+constexpr int kThreads = 192;
+constexpr int kMaxTerms = 2;
+constexpr int kStages = 3;
+
+template <int S>
+struct I8Cfg {
+  static constexpr int kBN = S == 4 ? 128 : 96;          // S levels x kBN TMEM columns <= 512
+  static constexpr int kATile = kBM * kBK;                 // bytes of one A slice tile
+  static constexpr int kBTile = kBN * kBK;
+  static constexpr int kStage = S * (kATile + kBTile);
+  static constexpr int kSmem = kStages * kStage + 1024;
+};
+
+struct I8Params {
+  CUtensorMap map_a[kMaxTerms][kMaxSlices];
+  CUtensorMap map_b[kMaxTerms][kMaxSlices];
+  int nterms;
+  int M, N, K;
+  int tiles_m, tiles_n, ntiles;
+  int bn;
+  int sym;
+  const int* aexp;   // per row of D
+  const int* bexp;   // per column of D
+  double alpha, beta, gamma;
+  const void* C;
+  int64_t ldc;
+  void* D;
+  int64_t ldd;
+  int* err;
+  unsigned long long timeout_ns;
+};
+
+__host__ __device__ constexpr uint32_t idesc_i8(int m, int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = (int)r[i];
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Tile id -> (mb, nb).  Symmetric mode enumerates, row by row, the tiles that touch the upper
+// triangle: in tile row mb those with nb >= floor(mb * kBM / bn).
+__device__ __forceinline__ void tile_of(const I8Params& p, int tile, int& mb, int& nb) {
+  if (p.sym) {
+    int r = 0, rem = tile;
+    for (;;) {
+      const int first = (r * kBM) / p.bn;
+      const int cnt = p.tiles_n - first;
+      if (rem < cnt) {
+        mb = r;
+        nb = first + rem;
+        return;
+      }
+      rem -= cnt;
+      ++r;
+    }
+  }
+  constexpr int G = 8;
+  const int per_group = G * p.tiles_n;
+  const int g = tile / per_group;
+  const int first_m = g * G;
+  const int gsize = min(G, p.tiles_m - first_m);
+  const int rr = tile - g * per_group;
+  mb = first_m + rr % gsize;
+  nb = rr / gsize;
+}
+
+template <int S, typename TO>
+__global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__ I8Params p) {
+  using Cf = I8Cfg<S>;
+  constexpr int kBN = Cf::kBN;
+  constexpr int kStage = Cf::kStage;
+  const TO* Cp = (const TO*)p.C;
+  TO* Dp = (TO*)p.D;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages];
+  __shared__ __align__(8) uint64_t tfull_bar, tempty_bar, drain_bar;
+  __shared__ uint32_t s_tmem;
+  __shared__ volatile int s_abort;
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int nkb = p.K / kBK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&tfull_bar, 1);
+    mbar_init(&tempty_bar, 128);
+    mbar_init(&drain_bar, 1);
+    s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = s_tmem;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int t = 0; t < p.nterms; ++t)
+        for (int q = 0; q < S; ++q) {
+          prefetch_map(&p.map_a[t][q]);
+          prefetch_map(&p.map_b[t][q]);
+        }
+      uint32_t kit = 0;
+      bool ok = true;
+      int issued[kStages];
+      for (int s = 0; s < kStages; ++s) issued[s] = -1;
+      for (int tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x) {
+        int mb, nb;
+        tile_of(p, tile, mb, nb);
+        for (int t = 0; t < p.nterms && ok; ++t) {
+          for (int kb = 0; kb < nkb; ++kb, ++kit) {
+            const int s = kit % kStages;
+            const uint32_t ph = (kit / kStages) & 1;
+            if (!mbar_wait(&empty_bar[s], ph ^ 1, &s_abort, p.timeout_ns, p.err)) {
+              ok = false;
+              break;
+            }
+            uint8_t* st = smem + (size_t)s * kStage;
+            mbar_expect_tx(&full_bar[s], kStage);
+            for (int q = 0; q < S; ++q) {
+              tma_load_2d(st + q * Cf::kATile, &p.map_a[t][q], &full_bar[s], kb * kBK, mb * kBM);
+              tma_load_2d(st + S * Cf::kATile + q * Cf::kBTile, &p.map_b[t][q], &full_bar[s], kb * kBK,
+                          nb * kBN);
+            }
+            issued[s] = (int)(kit / kStages);
+          }
+        }
+      }
+      if (!ok) {
+        for (int s = 0; s < kStages; ++s) {
+          if (issued[s] < 0) continue;
+          const unsigned long long t0 = gtimer();
+          while (!mbar_try(&full_bar[s], (uint32_t)issued[s] & 1))
+            if (gtimer() - t0 > p.timeout_ns) break;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_i8(kBM, kBN);
+      uint32_t kit = 0;
+      int it = 0;
+      bool ok = true, issued_any = false;
+      for (int tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x, ++it) {
+        if (!mbar_wait(&tempty_bar, (it & 1) ^ 1, &s_abort, p.timeout_ns, p.err)) break;
+        tc_fence_after();
+        bool first[S];
+#pragma unroll
+        for (int l = 0; l < S; ++l) first[l] = true;
+        for (int t = 0; t < p.nterms && ok; ++t) {
+          for (int kb = 0; kb < nkb; ++kb, ++kit) {
+            const int s = kit % kStages;
+            const uint32_t ph = (kit / kStages) & 1;
+            if (!mbar_wait(&full_bar[s], ph, &s_abort, p.timeout_ns, p.err)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t st = smem_u32(smem + (size_t)s * kStage);
+#pragma unroll
+            for (int pa = 0; pa < S; ++pa) {
+#pragma unroll
+              for (int pb = 0; pb < S; ++pb) {
+                const int lvl = pa + pb;  // 0..S-1 <=> level l = 2..S+1
+                if (lvl > S - 1) continue;
+                const uint32_t a_addr = st + pa * Cf::kATile;
+                const uint32_t b_addr = st + S * Cf::kATile + pb * Cf::kBTile;
+                const uint32_t tmem_d = tmem_base + (uint32_t)(lvl * kBN);
+#pragma unroll
+                for (int k32 = 0; k32 < kBK / 32; ++k32) {
+                  umma_i8(tmem_d, desc_sw64(a_addr + k32 * 32), desc_sw64(b_addr + k32 * 32), idesc,
+                          first[lvl] ? 0u : 1u);
+                  first[lvl] = false;
+                  issued_any = true;
+                }
+              }
+            }
+            umma_commit(&empty_bar[s]);
+          }
+        }
+        if (ok) umma_commit(&tfull_bar);
+      }
+      if (issued_any) {
+        umma_commit(&drain_bar);
+        const unsigned long long t0 = gtimer();
+        while (!mbar_try(&drain_bar, 0)) {
+          if (gtimer() - t0 > p.timeout_ns) {
+            atomicOr(p.err, kDevTimeout);
+            break;
+          }
+        }
+      }
+    }
+  } else {
+    const int q = warp & 3;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++it) {
+      if (!mbar_wait(&tfull_bar, it & 1, &s_abort, p.timeout_ns, p.err)) break;
+      tc_fence_after();
+      int mb, nb;
+      tile_of(p, tile, mb, nb);
+      const int64_t row = (int64_t)mb * kBM + q * 32 + lane;
+      const bool row_ok = row < p.M;
+      const int ea = row_ok ? p.aexp[row] : 0;
+      for (int cc = 0; cc < kBN / 16; ++cc) {
+        int lv[S][16];
+        const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(cc * 16);
+#pragma unroll
+        for (int l = 0; l < S; ++l) tmem_ld16(ta + l * kBN, lv[l]);
+        tmem_wait_ld();
+        const int64_t col0 = (int64_t)nb * kBN + cc * 16;
+        if (!row_ok || col0 >= p.N) continue;
+        TO out[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int64_t col = col0 + i;
+          double v = (double)lv[S - 1][i];
+#pragma unroll
+          for (int l = S - 2; l >= 0; --l) v = v * 0x1p-7 + (double)lv[l][i];
+          v = ldexp(v, ea + p.bexp[col] - 14);
+          v *= p.alpha;
+          if (p.beta != 0.0) v += p.beta * (double)Cp[row * p.ldc + col];
+          if (col == row) v += p.gamma;
+          out[i] = (TO)v;
+        }
+        if (!p.sym) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) Dp[row * p.ldd + col0 + i] = out[i];
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int64_t col = col0 + i;
+            if (col >= row) Dp[row * p.ldd + col] = out[i];
+            if (col > row) Dp[col * p.ldd + row] = out[i];
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&tempty_bar);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(512));
+  }
+}
+
+// ---- slicing: warp per row; the row exponent is shared by the real and imaginary planes.
+template <typename TI>
+__global__ void k_slice_rows(const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K, int S,
+                             I8Slices out, bool want_neg) {
+  const int lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (row >= rows) return;
+  double mx = 0.0;
+  for (int64_t k = lane; k < K; k += 32) {
+    mx = fmax(mx, fabs((double)re[row * ld + k]));
+    if (im) mx = fmax(mx, fabs((double)im[row * ld + k]));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  // mx = m 2^e with m in [0.5, 1); bump e when 128 m would round to 128, so that the first
+  // slice rint(128 x) stays in [-127, 127].
+  int e = 0;
+  if (mx > 0.0) {
+    frexp(mx, &e);
+    if (ldexp(mx, 7 - e) > 127.5) e += 1;
+  }
+  if (lane == 0) out.exp[row] = e;
+  for (int64_t k0 = (int64_t)lane * 4; k0 < K; k0 += 128) {
+#pragma unroll
+    for (int plane = 0; plane < 2; ++plane) {
+      const TI* src = plane == 0 ? re : im;
+      if (!src) continue;
+      uint32_t packed[kMaxSlices] = {0, 0, 0, 0, 0}, packed_neg[kMaxSlices] = {0, 0, 0, 0, 0};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        // Exact in FP64 for FP32 and FP64 inputs: scaling by 2^-e, multiplying by 128 and
+        // subtracting the rounded integer never round.
+        double x = (k0 + j < K) ? ldexp((double)src[row * ld + k0 + j], -e) : 0.0;
+#pragma unroll
+        for (int q = 0; q < kMaxSlices; ++q) {
+          if (q < S) {
+            x *= 128.0;
+            const double r = rint(x);
+            x -= r;
+            const int v = (int)r;
+            packed[q] |= ((uint32_t)(uint8_t)(int8_t)v) << (8 * j);
+            packed_neg[q] |= ((uint32_t)(uint8_t)(int8_t)(-v)) << (8 * j);
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kMaxSlices; ++q) {
+        if (q >= S) continue;
+        int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
+        if (dst) *reinterpret_cast<uint32_t*>(dst + row * out.ld + k0) = packed[q];
+        if (plane == 1 && want_neg && out.neg_im[q])
+          *reinterpret_cast<uint32_t*>(out.neg_im[q] + row * out.ld + k0) = packed_neg[q];
+      }
+    }
+  }
+}
+
+void make_map_u8(CUtensorMap* m, const int8_t* base, int64_t rows, int64_t cols, int64_t ld, int box_rows);
+
+}  // namespace
+
+// Host-side tensor maps (int8 data via the UINT8 TMA type; only bytes are moved).
+namespace {
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(ptr);
+  }
+  return fn;
+}
+void make_map_u8(CUtensorMap* m, const int8_t* base, int64_t rows, int64_t cols, int64_t ld, int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) throw Error{FX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable"};
+  if (((uintptr_t)base & 15) != 0 || ld % 16 != 0) throw Error{FX_ERR_VALUE, "int8 TMA operand not 16-byte aligned"};
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld};
+  cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error{FX_ERR_CUDA, "cuTensorMapEncodeTiled (int8) failed"};
+}
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+}  // namespace
+
+template <typename TI>
+void launch_slice_rows(int S, const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K, I8Slices out,
+                       bool want_neg_im, cudaStream_t s) {
+  if (S < 4 || S > kMaxSlices) throw Error{FX_ERR_VALUE, "slice count must be 4 or 5"};
+  if (K % 4 != 0 || out.ld % 16 != 0) throw Error{FX_ERR_VALUE, "slice: K and ld must be multiples of 4/16"};
+  if (!im) {
+    for (int q = 0; q < kMaxSlices; ++q) out.im[q] = out.neg_im[q] = nullptr;
+  }
+  k_slice_rows<TI><<<cdiv(rows, 8), 256, 0, s>>>(re, im, ld, rows, K, S, out, want_neg_im && im != nullptr);
+  FX_LAUNCH_CHECK();
+}
+template void launch_slice_rows<float>(int, const float*, const float*, int64_t, int64_t, int64_t, I8Slices, bool,
+                                       cudaStream_t);
+template void launch_slice_rows<double>(int, const double*, const double*, int64_t, int64_t, int64_t, I8Slices,
+                                        bool, cudaStream_t);
+
+namespace {
+template <int S, typename TO>
+void launch_i8_cfg(I8Params& p, const I8Term* terms, int nterms, int64_t M, int64_t N, int64_t K, int64_t lda,
+                   int64_t ldb, cudaStream_t s) {
+  using Cf = I8Cfg<S>;
+  static bool attr = false;
+  if (!attr) {
+    FX_CUDA(cudaFuncSetAttribute(k_gemm_i8<S, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::kSmem));
+    attr = true;
+  }
+  for (int t = 0; t < nterms; ++t)
+    for (int q = 0; q < S; ++q) {
+      make_map_u8(&p.map_a[t][q], terms[t].a[q], M, K, lda, kBM);
+      make_map_u8(&p.map_b[t][q], terms[t].b[q], N, K, ldb, Cf::kBN);
+    }
+  p.tiles_m = (int)cdiv(M, kBM);
+  p.tiles_n = (int)cdiv(N, Cf::kBN);
+  p.bn = Cf::kBN;
+  if (p.sym) {
+    p.ntiles = 0;
+    for (int r = 0; r < p.tiles_m; ++r) p.ntiles += p.tiles_n - (r * kBM) / Cf::kBN;
+  } else {
+    p.ntiles = p.tiles_m * p.tiles_n;
+  }
+  const int grid = p.ntiles < sm_count() ? p.ntiles : sm_count();
+  k_gemm_i8<S, TO><<<grid, kThreads, Cf::kSmem, s>>>(p);
+  FX_LAUNCH_CHECK();
+}
+}  // namespace
+
+template <typename TO>
+void launch_gemm_i8(int S, int64_t M, int64_t N, int64_t K, const I8Term* terms, int nterms, int64_t lda,
+                    int64_t ldb, const int* aexp, const int* bexp, double alpha, double beta, const TO* C,
+                    int64_t ldc, double gamma, TO* D, int64_t ldd, bool sym, int* err, unsigned timeout_ms,
+                    cudaStream_t s) {
+  if (nterms < 1 || nterms > kMaxTerms) throw Error{FX_ERR_VALUE, "int8 product: 1 or 2 terms"};
+  if (M <= 0 || N <= 0) return;
+  if (M % 16 || N % 16 || K % kBK || K <= 0 || K > 32768)
+    throw Error{FX_ERR_VALUE, "int8 product: M, N multiples of 16, K multiple of 64 and <= 32768"};
+  if (sym && M != N) throw Error{FX_ERR_VALUE, "symmetric product needs M == N"};
+  if (beta != 0.0 && !C) throw Error{FX_ERR_VALUE, "int8 product: beta without C"};
+  I8Params p;
+  memset(&p, 0, sizeof(p));
+  p.nterms = nterms;
+  p.M = (int)M;
+  p.N = (int)N;
+  p.K = (int)K;
+  p.sym = sym ? 1 : 0;
+  p.aexp = aexp;
+  p.bexp = bexp;
+  p.alpha = alpha;
+  p.beta = beta;
+  p.gamma = gamma;
+  p.C = C;
+  p.ldc = ldc;
+  p.D = D;
+  p.ldd = ldd;
+  p.err = err;
+  p.timeout_ns = (unsigned long long)timeout_ms * 1000000ull;
+  if (S == 4)
+    launch_i8_cfg<4, TO>(p, terms, nterms, M, N, K, lda, ldb, s);
+  else if (S == 5)
+    launch_i8_cfg<5, TO>(p, terms, nterms, M, N, K, lda, ldb, s);
+  else
+    throw Error{FX_ERR_VALUE, "slice count must be 4 or 5"};
+}
+template void launch_gemm_i8<float>(int, int64_t, int64_t, int64_t, const I8Term*, int, int64_t, int64_t,
+                                    const int*, const int*, double, double, const float*, int64_t, double,
+                                    float*, int64_t, bool, int*, unsigned, cudaStream_t);
+template void launch_gemm_i8<double>(int, int64_t, int64_t, int64_t, const I8Term*, int, int64_t, int64_t,
+                                     const int*, const int*, double, double, const double*, int64_t, double,
+                                     double*, int64_t, bool, int*, unsigned, cudaStream_t);
+
+}  // namespace fx

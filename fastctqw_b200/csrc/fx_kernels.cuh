@@ -1,0 +1,167 @@
+// Launchers of the bandwidth-bound kernels, the LU kernels and the matrix-product
+// kernels (internal header).  All pointers are device pointers; all work is ordered on
+// the given stream.  Matrices are planar complex: separate real and imaginary planes,
+// row-major with leading dimension `ld`; an imaginary plane of nullptr means "zero".
+#pragma once
+#include "fx_common.cuh"
+
+namespace fx {
+
+// ---------------------------------------------------------------- input / structure
+// Line sums, trace and exact structure flags of the interleaved input (n x n, row-major,
+// element type given by dtype).  row/col: n doubles each (real,imag interleaved => 2n).
+struct InputStats {
+  double* rowsum;   // 2n (re, im)
+  double* colsum;   // 2n
+  double* diag;     // 2n (diagonal entries, re/im)
+  int* flags;       // [0] any Re != 0, [1] any Im != 0, [2] not symmetric,
+                    // [3] not skew-Hermitian, [4] non-finite seen
+};
+void launch_input_stats(const void* X, int dtype, int64_t n, InputStats st, cudaStream_t s);
+
+// Y = X - mu I - (nu/n) J on the n x n block, zero padding elsewhere, planar T.
+template <typename T>
+void launch_load_shifted(const void* X, int dtype, int64_t n, int64_t np, double mu_re,
+                         double mu_im, double nu_re, double nu_im, T* yre, T* yim,
+                         cudaStream_t s);
+
+// --------------------------------------------------------------------------- norms
+// colsum[j] += sum_i |M_ij| (double, 2 planes -> complex modulus), columns 0..np-1.
+template <typename T>
+void launch_col_abs_sums(const T* re, const T* im, int64_t np, int64_t ld, double* colsum,
+                         cudaStream_t s);
+// Block products for the 1-norm estimator: Y = M X, Z = M^H S with X, S: np x 2 complex
+// stored as (re, im) double arrays of length 2*np per column, column-major.
+template <typename T>
+void launch_matvec2(const T* re, const T* im, int64_t np, const double* X, double* Y,
+                    cudaStream_t s);
+template <typename T>
+void launch_matvec2_h(const T* re, const T* im, int64_t np, const double* S, double* Z,
+                      cudaStream_t s);
+// w = v |M| (row vector times the entrywise modulus), w zeroed by the launcher.
+template <typename T>
+void launch_vec_absmat(const T* re, const T* im, int64_t np, const double* v, double* w,
+                       cudaStream_t s);
+
+// --------------------------------------------------------------------- elementwise
+// D = c0 M0 + c1 M1 + c2 M2 + c3 M3 + g I   (one real plane; null Mk are skipped).
+template <typename T>
+void launch_combo(T* D, const T* M0, double c0, const T* M1, double c1, const T* M2,
+                  double c2, const T* M3, double c3, double g, int64_t np, cudaStream_t s);
+// Zero fill of a plane.
+template <typename T>
+void launch_zero(T* D, int64_t count, cudaStream_t s);
+// Out-of-place transpose of an rows x cols block (ld_in / ld_out).
+template <typename T>
+void launch_transpose(const T* in, int64_t ld_in, T* out, int64_t ld_out, int64_t rows,
+                      int64_t cols, cudaStream_t s);
+// BF16 split planes of an rows x cols FP32 block: out[p] gets part p (p < nparts); with
+// `transpose` the block is written transposed (cols x rows).
+void launch_split(const float* in, int64_t ld_in, __nv_bfloat16* const* out, int nparts,
+                  int64_t ld_out, int64_t rows, int64_t cols, bool transpose, cudaStream_t s);
+
+// ------------------------------------------------------------------------- output
+// U = e^mu (E + ipe*I + rank1 * (e^nu - 1)/n J) on the n x n block -> interleaved dtype.
+struct OutputMap {
+  double emu_re, emu_im;     // e^mu
+  double cj_re, cj_im;       // (e^nu - 1)/n, 0 when no rank-one shift
+  int ipe;                   // 1 if E stores R - I
+};
+template <typename T>
+void launch_output(const T* ere, const T* eim, int64_t n, int64_t np, OutputMap om,
+                   void* U, int dtype, cudaStream_t s);
+// psi = e^mu (E psi0 + ipe psi0 + rank1 * (e^nu-1)/n (1^T psi0) 1), psi0/psi interleaved
+// complex of the handle's dtype (complex64 for real handles is not used).
+template <typename T>
+void launch_apply(const T* ere, const T* eim, int64_t n, int64_t np, OutputMap om,
+                  const void* psi0, void* psi, int dtype, double* scratch2, cudaStream_t s);
+
+// ----------------------------------------------------------------------------- LU
+// Right-looking panel factorisation with partial pivoting of columns [k0, k0+nb) of the
+// planar complex np x np matrix, rows [k0, np).  ipiv[k] = pivot row of column k.
+template <typename T>
+void launch_lu_panel(T* re, T* im, int64_t np, int64_t k0, int nb, int* ipiv, int* err,
+                     cudaStream_t s);
+// Apply the row interchanges ipiv[k0..k0+nb) to columns [c0, c1) of a planar matrix.
+template <typename T>
+void launch_row_swaps(T* re, T* im, int64_t ld, int64_t c0, int64_t c1, const int* ipiv,
+                      int64_t k0, int nb, cudaStream_t s);
+// In place B <- L^-1 B (L unit lower, nb x nb at (r0, r0) of the factored matrix) for the
+// nb x cols block B at rows [r0, r0+nb), columns [c0, c0+cols) of (bre, bim, ldb).
+template <typename T>
+void launch_trsm_lower_unit(const T* lre, const T* lim, int64_t ldl, int64_t r0, int nb,
+                            T* bre, T* bim, int64_t ldb, int64_t c0, int64_t cols,
+                            cudaStream_t s);
+// In place B <- U^-1 B (U upper non-unit, nb x nb at (r0, r0)).
+template <typename T>
+void launch_trsm_upper(const T* ure, const T* uim, int64_t ldu, int64_t r0, int nb, T* bre,
+                       T* bim, int64_t ldb, int64_t c0, int64_t cols, int* err,
+                       cudaStream_t s);
+
+// ----------------------------------------------------------------- matrix products
+// D = alpha * sum_t sign_t * A_t * Bt_t^T + beta * C + gamma * I_diag
+// A_t: M x K row-major (lda), Bt_t: N x K row-major (ldb) -- i.e. the right factor is
+// given transposed, K contiguous, for both operands.  C may alias D.  `diag` adds gamma at
+// (i, i) of the M x N block.
+template <typename T>
+struct GemmTerm {
+  const T* a;
+  const T* b;
+  float sign;
+};
+template <typename T>
+void launch_gemm_simt(int64_t M, int64_t N, int64_t K, const GemmTerm<T>* terms, int nterms,
+                      int64_t lda, int64_t ldb, double alpha, double beta, const T* C,
+                      int64_t ldc, double gamma, T* D, int64_t ldd, cudaStream_t s);
+
+// tcgen05 (5th-gen tensor core) product on BF16 split planes with FP32 accumulation in
+// TMEM.  Each term carries `nplanes` split planes of A and of Bt; the products (i, j) with
+// i + j < nplanes are accumulated (3 for nplanes = 2, 6 for nplanes = 3).
+struct TcTerm {
+  const __nv_bfloat16* a[4];
+  const __nv_bfloat16* b[4];
+  int neg;
+};
+struct TcOut {
+  float* d;                       // FP32 result (may be null)
+  int64_t ldd;
+  __nv_bfloat16* split[4];        // optional BF16 split planes of the result
+  int nsplit;
+  int64_t lds;
+};
+void launch_gemm_tc(int64_t M, int64_t N, int64_t K, const TcTerm* terms, int nterms,
+                    int nplanes, int64_t lda, int64_t ldb, float alpha, float beta,
+                    const float* C, int64_t ldc, float gamma, TcOut out, int* err,
+                    unsigned timeout_ms, cudaStream_t s);
+bool tc_available();
+
+// Int8 slices (Ozaki splitting) of an operand: S = 4 or 5 slices per plane, row exponents
+// shared by the real and imaginary planes; optional negated imaginary slices.
+struct I8Slices {
+  int8_t* re[5];
+  int8_t* im[5];
+  int8_t* neg_im[5];
+  int* exp;
+  int64_t ld;   // bytes between rows of a slice
+};
+template <typename TI>
+void launch_slice_rows(int S, const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K,
+                       I8Slices out, bool want_neg_im, cudaStream_t s);
+struct I8Term {
+  const int8_t* a[5];
+  const int8_t* b[5];
+};
+// D = alpha * 2^(ea_i + eb_j) * sum_t A_t Bt_t^T + beta C + gamma I with exact int32 accumulation
+// of the slice products (S slices, products p + q <= S + 1); `sym`: the result is symmetric,
+// only tiles touching the upper triangle are computed and mirrored (M == N).
+template <typename TO>
+void launch_gemm_i8(int S, int64_t M, int64_t N, int64_t K, const I8Term* terms, int nterms,
+                    int64_t lda, int64_t ldb, const int* aexp, const int* bexp, double alpha,
+                    double beta, const TO* C, int64_t ldc, double gamma, TO* D, int64_t ldd, bool sym,
+                    int* err, unsigned timeout_ms, cudaStream_t s);
+// In place A <- (A + A^T) / 2 of an n x n plane (exact symmetry of a result known to be
+// symmetric in exact arithmetic).
+template <typename T>
+void launch_symmetrize(T* a, int64_t n, int64_t ld, cudaStream_t s);
+
+}  // namespace fx

@@ -1,0 +1,136 @@
+/*
+ * fastctqw_b200 — C ABI of the B200 expm(-iHt) engine.
+ *
+ * Plain C types only (pointers, sizes, ints).  Every entry point returns an fx_status;
+ * fx_last_error() gives the message of the last failure on a handle (or globally when the
+ * handle is NULL).  Matrices are dense, row-major ("C order", as numpy hands them over),
+ * interleaved complex (real, imag) in the dtype the handle was created with.  Because
+ * expm(A^T) = expm(A)^T, row- vs column-major storage does not change the result as long
+ * as input and output use the same order.
+ *
+ * Reference interfaces replaced (Crinton/FastCTQW):
+ *   fx_create  <- MatrixExpCalculator<T>::MatrixExpCalculator(size_t n)
+ *                 (include/MatrixExpCalculator.h:36, :64, :92; bound src/main.cu:14-15,
+ *                 :27-28, :40-41, :53-54 as ExpMatFloat32/Float64/Complex64/Complex128)
+ *   fx_run_host <- MatrixExpCalculator<T>::run(py::array_t<T>&)
+ *                 (include/MatrixExpCalculator.h:40, :68, :96; src/main.cu:17-19, :30-32,
+ *                 :43-45, :56-58)
+ *   fx_free    <- MatrixExpCalculator<T>::free()  (include/MatrixExpCalculator.h:42, :70, :98;
+ *                 src/main.cu:21-22)
+ *   fx_get_n   <- MatrixExpCalculator<T>::getN()  (include/MatrixExpCalculator.h:41, :69, :97)
+ *   fx_destroy <- ~MatrixExpCalculator()          (include/MatrixExpCalculator.h:37, :65, :93)
+ *   fx_walk_device / fx_walk_host <- Operator.buildExpmOperator(t) followed by the host
+ *                 GEMV U @ psi0 in Ctqw.runWalk (FastCTQW/Operator.py:70-78,
+ *                 FastCTQW/Ctqw.py:90-94), kept on the device.
+ *   fx_run_device: device-pointer variant of run (no counterpart: the reference always
+ *                 copies through host numpy arrays).
+ *   fx_gpu_memory_gb <- get_current_gpu_memory_gb() (include/MatrixExpCalculator.h:101)
+ */
+#ifndef FASTCTQW_B200_H
+#define FASTCTQW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fx_engine* fx_handle;
+
+/* Element types (ExpMatFloat32 / Float64 / Complex64 / Complex128). */
+enum fx_dtype { FX_F32 = 0, FX_F64 = 1, FX_C64 = 2, FX_C128 = 3 };
+
+enum fx_status {
+  FX_OK = 0,
+  FX_ERR_TYPE = 1,      /* bad dtype / handle kind          -> Python TypeError   */
+  FX_ERR_VALUE = 2,     /* bad size, shape, option value    -> Python ValueError  */
+  FX_ERR_NOMEM = 3,     /* device or host allocation failed -> Python MemoryError */
+  FX_ERR_CUDA = 4,      /* CUDA runtime / launch error      -> RuntimeError       */
+  FX_ERR_TIMEOUT = 5,   /* a bounded device wait ran out    -> RuntimeError       */
+  FX_ERR_NONFINITE = 6, /* NaN/Inf in the input or a norm   -> ValueError         */
+  FX_ERR_SINGULAR = 7,  /* exactly singular Pade denominator-> RuntimeError       */
+  FX_ERR_NODEV = 8,     /* no sm_100 device                 -> RuntimeError       */
+  FX_ERR_FREED = 9      /* handle used after fx_free        -> RuntimeError       */
+};
+
+/* Arithmetic forms for the matrix products (fx_set_option(FX_OPT_FORM, ...)). */
+enum fx_form {
+  FX_FORM_PLAIN = 0,  /* FP32-faithful: BF16 3-way split, 6 products, FP32 accumulate */
+  FX_FORM_MIXED = 1,  /* BF16 hi+lo split, 3 products (hi*hi, hi*lo, lo*hi)           */
+  FX_FORM_SIMT = 2,   /* CUDA-core FP32/FP64 FMA products (checker / FP64 engine)    */
+  FX_FORM_FP64 = 3    /* FP64 engine (complex128 / float64 handles)                   */
+};
+
+enum fx_option {
+  FX_OPT_FORM = 0,        /* fx_form                                                   */
+  FX_OPT_SHIFT = 1,       /* 0 none, 1 trace, 2 trace + rank-one (default 2)           */
+  FX_OPT_STRUCTURE = 2,   /* 1: exploit X = i*(real symmetric) structure (default 1)   */
+  FX_OPT_FORCE_S = 3,     /* >= 0: override the scaling s (with FX_OPT_FORCE_M)        */
+  FX_OPT_FORCE_M = 4,     /* 3, 5, 7, 9, 13 or -1 (automatic)                          */
+  FX_OPT_TIMEOUT_MS = 5,  /* bound of every device-side wait (default 2000)            */
+  FX_OPT_IPE = 6,         /* 1: square in I+E form (default 1)                         */
+  FX_OPT_REFINE = 7,      /* iterative-refinement steps of the Pade solve (default 0)  */
+  FX_OPT_DEBUG_STAGE = 8  /* diagnostics: k > 0 makes run write intermediate k instead of
+                             U (1 Y, 2-4 A2/A4/A6, 5 U_pade, 6 V_pade, 7 R, 8+j after j
+                             squarings) and stop                                       */
+};
+
+/* What the last run did. */
+typedef struct fx_stats {
+  int32_t m;            /* Pade degree                                   */
+  int32_t s;            /* number of squarings                           */
+  int32_t form;         /* fx_form used for the products                 */
+  int32_t structured;   /* 1 if the X = i*(real symmetric) path was used */
+  int32_t rank1_shift;  /* 1 if the rank-one commuting shift was applied */
+  int32_t symmetric;    /* 1 if X^T == X (no transposes needed)          */
+  int32_t gemm_launches;/* matrix-product kernel launches in the run     */
+  int32_t launches;     /* all kernel launches of the run                */
+  double norm1;         /* ||X - shifts||_1                              */
+  double d[5];          /* d4, d6, d8, d10, log2 ||(|A|)^27||_1          */
+  double ms_total;      /* device time of the last run (CUDA events)     */
+  double flops;         /* algorithmic real flops of the last run        */
+} fx_stats;
+
+int fx_create(size_t n, int dtype, fx_handle* out);
+int fx_destroy(fx_handle h);
+int fx_free(fx_handle h);
+int fx_get_n(fx_handle h, size_t* n);
+int fx_set_option(fx_handle h, int key, double value);
+int fx_get_stats(fx_handle h, fx_stats* out);
+const char* fx_last_error(fx_handle h);
+
+/* U = expm(A), both host buffers of n*n elements of the handle's dtype. */
+int fx_run_host(fx_handle h, const void* A, void* U);
+/* Same with device buffers; the work is ordered on `stream` (a cudaStream_t or NULL). */
+int fx_run_device(fx_handle h, const void* dA, void* dU, void* stream);
+/* psi = expm(A) psi0 (and U if dU != NULL); device buffers. */
+int fx_walk_device(fx_handle h, const void* dA, const void* dpsi0, void* dpsi, void* dU,
+                   void* stream);
+/* psi = expm(A) psi0 with host buffers.  U stays resident on the device (not copied back)
+ * until fx_fetch_u asks for it. */
+int fx_walk_host(fx_handle h, const void* A, const void* psi0, void* psi);
+/* Copy the U of the last fx_walk_host call to a host buffer of n*n elements
+ * (Operator.getOperator after Ctqw.runWalk, FastCTQW/Operator.py:165-166). */
+int fx_fetch_u(fx_handle h, void* U);
+
+/* Diagnostics (no counterpart in the reference): one real product through the engine's
+ * product kernels, D = alpha A Bt^T + beta C + gamma I, on device buffers (row-major;
+ * Bt is the right factor transposed, N x K).  form: FX_FORM_PLAIN / FX_FORM_MIXED
+ * (tcgen05, BF16 split) or FX_FORM_SIMT (CUDA cores).  Allocates its split scratch. */
+int fx_product_f32(int form, int64_t M, int64_t N, int64_t K, const float* A, int64_t lda,
+                   const float* Bt, int64_t ldb, float alpha, float beta, const float* C,
+                   int64_t ldc, float gamma, float* D, int64_t ldd, void* stream);
+const char* fx_product_error(void);
+
+/* Device memory currently in use on the current device, GB. */
+double fx_gpu_memory_gb(void);
+/* 1 if a device with compute capability 10.x is present. */
+int fx_device_ok(void);
+/* Library build string. */
+const char* fx_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FASTCTQW_B200_H */
