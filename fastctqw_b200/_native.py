@@ -21,7 +21,7 @@ CODE_DTYPE = {v: k for k, v in DTYPE_CODE.items()}
 
 FORM_PLAIN, FORM_MIXED, FORM_SIMT, FORM_FP64 = 0, 1, 2, 3
 FORMS = {"plain": FORM_PLAIN, "mixed": FORM_MIXED, "simt": FORM_SIMT, "fp64": FORM_FP64}
-OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE, OPT_DEBUG_STAGE = range(9)
+OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE, OPT_DEBUG_STAGE, OPT_PROFILE = range(10)
 
 OK, ERR_TYPE, ERR_VALUE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_NONFINITE, ERR_SINGULAR, ERR_NODEV, ERR_FREED = range(10)
 
@@ -30,12 +30,15 @@ class FxStats(ctypes.Structure):
     _fields_ = [("m", ctypes.c_int32), ("s", ctypes.c_int32), ("form", ctypes.c_int32),
                 ("structured", ctypes.c_int32), ("rank1_shift", ctypes.c_int32),
                 ("symmetric", ctypes.c_int32), ("gemm_launches", ctypes.c_int32),
-                ("launches", ctypes.c_int32), ("norm1", ctypes.c_double),
+                ("launches", ctypes.c_int32), ("solver", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("norm1", ctypes.c_double),
                 ("d", ctypes.c_double * 5), ("ms_total", ctypes.c_double),
-                ("flops", ctypes.c_double)]
+                ("flops", ctypes.c_double), ("prod_ms", ctypes.c_double),
+                ("prod_ops", ctypes.c_double), ("prod_flops", ctypes.c_double),
+                ("prod_launches", ctypes.c_int32), ("reserved2", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
-        out = {k: getattr(self, k) for k, _ in self._fields_ if k != "d"}
+        out = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("d", "reserved", "reserved2")}
         out["d4"], out["d6"], out["d8"], out["d10"], out["log2_abs27"] = list(self.d)
         return out
 
@@ -149,7 +152,8 @@ class Engine:
     def configure(self, form: str | None = None, shift: int | None = None,
                   structure: bool | None = None, force_m: int | None = None,
                   force_s: int | None = None, ipe: bool | None = None,
-                  timeout_ms: float | None = None, debug_stage: int | None = None) -> None:
+                  timeout_ms: float | None = None, debug_stage: int | None = None,
+                  profile: bool | None = None) -> None:
         if form is not None:
             if form not in FORMS:
                 raise ValueError(f"form must be one of {sorted(FORMS)}")
@@ -168,6 +172,8 @@ class Engine:
             self.set_option(OPT_TIMEOUT_MS, timeout_ms)
         if debug_stage is not None:
             self.set_option(OPT_DEBUG_STAGE, debug_stage)
+        if profile is not None:
+            self.set_option(OPT_PROFILE, int(bool(profile)))
 
     def stats(self) -> dict:
         st = FxStats()

@@ -86,6 +86,7 @@ struct RunOpts {
   unsigned timeout_ms;
   int ipe;
   int debug_stage;   // 0: normal output; k > 0: output an intermediate (diagnostics)
+  int profile;       // 1: time every int8 product launch with CUDA events
 };
 
 // Planar complex matrix view over owned storage; a missing plane is identically zero.
@@ -121,6 +122,7 @@ class Pipeline {
     err_.alloc(sizeof(int) * 8);
     const size_t tbytes = sizeof(T) * (size_t)np_ * kPanel;
     panel_t_.alloc(tbytes * 2);
+    chol_.alloc(sizeof(T) * (size_t)np_ * kCholNb * 6);
   }
   ~Pipeline() {
     mats_.release();
@@ -130,6 +132,7 @@ class Pipeline {
     ipiv_.release();
     err_.release();
     panel_t_.release();
+    chol_.release();
   }
 
   using Opts = RunOpts;
@@ -293,17 +296,41 @@ class Pipeline {
     }
 
     if (dump(5, U, dU) || dump(6, V, dU)) return;
-    // Q = V - U into the LU slot, P = V + U into the solution slot.
     CM<T>& Q = slot_[kQ];
     CM<T>& R = slot_[kR];
-    combo(Q, {{&V, 1.0}, {&U, -1.0}}, 0.0);
-    combo(R, {{&V, 1.0}, {&U, 1.0}}, 0.0);
-    // The solver works on full planes: materialise a zero imaginary plane if needed.
-    ensure_planes(Q, !real_in);
-    ensure_planes(R, !real_in);
-
-    // ---- 6. R = Q^-1 P
-    lu_solve(Q, R);
+    // FP64 masters only: in FP32 storage the kappa(Q)^2 of the normal equations costs accuracy.
+    const bool chol = std::is_same<T, double>::value && structured_ && normal_ && V.hr && !V.hi && U.hi && !U.hr;
+    st.solver = chol ? 1 : 0;
+    if (chol) {
+      // ---- 6'. X = i*(real symmetric): P = conj(Q) = Q^H, so R = Q^-1 P = G^-1 (Q^H)^2 with
+      // G = Q^H Q = V^2 + W^2 real SPD (V even part, U = iW odd part; V and W commute).
+      CM<T>& VV = slot_[kT1];
+      CM<T>& WW = slot_[kT2];
+      CM<T>& VW = slot_[kTmp];
+      cproduct(np_, np_, np_, V.rb, nullptr, np_, V.rb, nullptr, np_, 1.0, nullptr, nullptr, np_, 0.0, 0.0,
+               VV.rb, nullptr, np_, true);
+      cproduct(np_, np_, np_, U.ib, nullptr, np_, U.ib, nullptr, np_, 1.0, nullptr, nullptr, np_, 0.0, 0.0,
+               WW.rb, nullptr, np_, true);
+      cproduct(np_, np_, np_, V.rb, nullptr, np_, U.ib, nullptr, np_, 1.0, nullptr, nullptr, np_, 0.0, 0.0,
+               VW.rb, nullptr, np_, true);
+      launch_combo<T>(Q.rb, VV.rb, 1.0, WW.rb, 1.0, nullptr, 0, nullptr, 0, 0.0, np_, s);
+      launch_combo<T>(R.rb, VV.rb, 1.0, WW.rb, -1.0, nullptr, 0, nullptr, 0, 0.0, np_, s);
+      launch_combo<T>(R.ib, VW.rb, 2.0, nullptr, 0, nullptr, 0, nullptr, 0, 0.0, np_, s);
+      launches_ += 3;
+      Q.hr = true;
+      Q.hi = false;
+      R.hr = R.hi = true;
+      chol_solve(Q.rb, R.rb, R.ib);
+    } else {
+      // Q = V - U into the LU slot, P = V + U into the solution slot.
+      combo(Q, {{&V, 1.0}, {&U, -1.0}}, 0.0);
+      combo(R, {{&V, 1.0}, {&U, 1.0}}, 0.0);
+      // The solver works on full planes: materialise a zero imaginary plane if needed.
+      ensure_planes(Q, !real_in);
+      ensure_planes(R, !real_in);
+      // ---- 6. R = Q^-1 P
+      lu_solve(Q, R);
+    }
     if (sym_) {
       // R = Q^-1 P is symmetric in exact arithmetic (P, Q commute and are symmetric); the
       // solve leaves an antisymmetric rounding part that the squarings would amplify.
@@ -347,6 +374,7 @@ class Pipeline {
     FX_CUDA(cudaStreamSynchronize(s));
     if (h_err[0] & kDevTimeout) throw Error{FX_ERR_TIMEOUT, "a device-side wait timed out"};
     if (h_err[0] & kDevSingular) throw Error{FX_ERR_SINGULAR, "Pade denominator is singular"};
+    prof_collect(st);
     st.form = form_;
     st.gemm_launches = gemm_count_;
     st.launches = launches_;
@@ -371,10 +399,11 @@ class Pipeline {
   static constexpr int kSplitPlanes = 16;
   static constexpr int kSlicePlanes = 25;
   static constexpr int kPanel = 128;
+  static constexpr int kCholNb = 128;
 
   int64_t n_, np_;
   int dtype_;
-  DevBuf mats_, split_, slices_, small_, ipiv_, err_, panel_t_;
+  DevBuf mats_, split_, slices_, small_, ipiv_, err_, panel_t_, chol_;
   CM<T> slot_[kNumMats];
   Opts opts_{};
   cudaStream_t stream_ = nullptr;
@@ -383,6 +412,53 @@ class Pipeline {
   int gemm_count_ = 0, launches_ = 0;
 
   int* derr() const { return (int*)err_.p; }
+
+  // ---- live timing of the int8 product launches (CUDA events on the launch stream)
+  std::vector<cudaEvent_t> ev_pool_;
+  std::vector<std::pair<double, double>> ev_work_;   // (issued int8 ops, useful real flops)
+  size_t ev_used_ = 0;
+  void prof_begin() {
+    if (!opts_.profile) return;
+    if (ev_used_ + 2 > ev_pool_.size()) {
+      for (int i = 0; i < 64; ++i) {
+        cudaEvent_t e;
+        FX_CUDA(cudaEventCreate(&e));
+        ev_pool_.push_back(e);
+      }
+    }
+    FX_CUDA(cudaEventRecord(ev_pool_[ev_used_], stream_));
+  }
+  void prof_end(double ops, double flops) {
+    if (!opts_.profile) return;
+    FX_CUDA(cudaEventRecord(ev_pool_[ev_used_ + 1], stream_));
+    ev_work_.push_back({ops, flops});
+    ev_used_ += 2;
+  }
+  void prof_collect(fx_stats& st) {
+    if (!opts_.profile) return;
+    FX_CUDA(cudaStreamSynchronize(stream_));
+    double ms = 0, ops = 0, fl = 0;
+    for (size_t i = 0; i < ev_work_.size(); ++i) {
+      float t = 0;
+      FX_CUDA(cudaEventElapsedTime(&t, ev_pool_[2 * i], ev_pool_[2 * i + 1]));
+      ms += t;
+      ops += ev_work_[i].first;
+      fl += ev_work_[i].second;
+    }
+    st.prod_ms = ms;
+    st.prod_ops = ops;
+    st.prod_flops = fl;
+    st.prod_launches = (int)ev_work_.size();
+    ev_work_.clear();
+    ev_used_ = 0;
+  }
+  static double sym_tile_fraction(int64_t n, int S) {
+    const int bn = S == 4 ? 128 : 96;
+    const int64_t tm = (n + 127) / 128, tn = (n + bn - 1) / bn;
+    int64_t cnt = 0;
+    for (int64_t r = 0; r < tm; ++r) cnt += tn - (r * 128) / bn;
+    return (double)cnt / (double)(tm * tn);
+  }
   __nv_bfloat16* split_plane(int i, int64_t elems) const {
     if (elems > np_ * np_) throw Error{FX_ERR_VALUE, "split plane overflow"};
     return (__nv_bfloat16*)split_.p + (size_t)i * np_ * np_;
@@ -476,8 +552,8 @@ class Pipeline {
     if (ai && bti) tr.push_back({1, 1, 1});
     if (ar && bti) ti.push_back({0, 1, 0});
     if (ai && btr) ti.push_back({1, 0, 0});
-    const bool want_r = !tr.empty() || (cr && beta != 0.0) || gamma != 0.0;
-    const bool want_i = !ti.empty() || (ci && beta != 0.0);
+    const bool want_r = dr && (!tr.empty() || (cr && beta != 0.0) || gamma != 0.0);
+    const bool want_i = di && (!ti.empty() || (ci && beta != 0.0));
     const T* A2[2] = {ar, ai};
     const T* B2[2] = {btr, bti};
     auto plain_combo = [&](T* d, const T* c, double bt, double g) {
@@ -563,11 +639,25 @@ class Pipeline {
       sb.exp = slice_exp(1);
       sa.ld = sb.ld = K;
       const bool need_a = ar || ai, need_b = btr || bti;
-      if (need_a) {
+      if (need_a && !(need_b && ar == btr && ai == bti && lda == ldb && M == N)) {
         launch_slice_rows<T>(S, ar ? ar : ai, ar ? ai : nullptr, lda, M, K, sa, false, stream_);
         ++launches_;
       }
-      if (need_b) {
+      // The same matrix on both sides (squarings, powers): slice it once.
+      const bool same = need_a && need_b && ar == btr && ai == bti && lda == ldb && M == N;
+      if (same) {
+        sb.re[0] = nullptr;  // marker: B side uses the A slices
+        I8Slices sab = sa;
+        for (int q = 0; q < S; ++q) sab.neg_im[q] = sb.neg_im[q];
+        launch_slice_rows<T>(S, ar ? ar : ai, ar ? ai : nullptr, lda, M, K, sab, ai != nullptr && ar != nullptr,
+                             stream_);
+        ++launches_;
+        for (int q = 0; q < S; ++q) {
+          sb.re[q] = sa.re[q];
+          sb.im[q] = sa.im[q];
+        }
+        sb.exp = sa.exp;
+      } else if (need_b) {
         launch_slice_rows<T>(S, btr ? btr : bti, btr ? bti : nullptr, ldb, N, K, sb,
                              bti != nullptr && btr != nullptr, stream_);
         ++launches_;
@@ -588,8 +678,14 @@ class Pipeline {
           if (t.neg && (btr == nullptr)) sgn = -1.0;
           tt.push_back(x);
         }
+        prof_begin();
         launch_gemm_i8<T>(S, M, N, K, tt.data(), (int)tt.size(), K, K, sa.exp, sb.exp, alpha * sgn,
                           c ? beta : 0.0, c, ldc, g, d, ldd, sym, derr(), opts_.timeout_ms, stream_);
+        // Issued int8 MMA work: 2 M N K ops per slice product and term; a symmetric product
+        // computes only the tiles touching the upper triangle.
+        const double frac = sym ? sym_tile_fraction(M, S) : 1.0;
+        prof_end(2.0 * (double)M * (double)N * (double)K * (S * (S + 1) / 2) * tt.size() * frac,
+                 2.0 * (double)M * (double)N * (double)K * tt.size() * frac);
         ++gemm_count_;
         ++launches_;
       };
@@ -770,6 +866,62 @@ class Pipeline {
     return out;
   }
 
+  // ---- blocked Cholesky G = L L^T (real SPD, in place) and R <- G^-1 R for the two planes of R.
+  void chol_solve(T* G, T* rr, T* ri) {
+    const int nb = kCholNb;
+    const int64_t np = np_;
+    T* Linv = (T*)chol_.p;               // block k at rows [k0, k0+nb), ld nb
+    T* LinvT = Linv + (size_t)np * nb;
+    T* P21 = LinvT + (size_t)np * nb;    // np x nb
+    T* At = P21 + (size_t)np * nb;       // np x nb
+    T* Btr = At + (size_t)np * nb;       // np x nb (two planes)
+    T* Bti = Btr + (size_t)np * nb;
+    for (int64_t k0 = 0; k0 < np; k0 += nb) {
+      launch_potrf_inv<T>(G, np, k0, nb, Linv + k0 * nb, LinvT + k0 * nb, derr(), stream_);
+      ++launches_;
+      const int64_t rest = np - k0 - nb;
+      if (rest <= 0) continue;
+      T* G21 = G + (k0 + nb) * np + k0;
+      // L21 = G21 L11^-T  (A = G21, Bt = L11^-1)
+      cproduct(rest, nb, nb, G21, nullptr, np, Linv + k0 * nb, nullptr, nb, 1.0, nullptr, nullptr, nb, 0.0, 0.0,
+               P21, nullptr, nb, false);
+      FX_CUDA(cudaMemcpy2DAsync(G21, sizeof(T) * np, P21, sizeof(T) * nb, sizeof(T) * nb, rest,
+                                cudaMemcpyDeviceToDevice, stream_));
+      // G22 -= L21 L21^T  (symmetric result)
+      T* G22 = G + (k0 + nb) * np + (k0 + nb);
+      cproduct(rest, rest, nb, P21, nullptr, nb, P21, nullptr, nb, -1.0, G22, nullptr, np, 1.0, 0.0, G22, nullptr,
+               np, true);
+    }
+    auto transpose_rows = [&](int64_t r0) {   // rows [r0, r0+nb) of R -> Bt (np x nb)
+      launch_transpose<T>(rr + r0 * np, np, Btr, nb, nb, np, stream_);
+      launch_transpose<T>(ri + r0 * np, np, Bti, nb, nb, np, stream_);
+      launches_ += 2;
+    };
+    // forward: L Z = R
+    for (int64_t k0 = 0; k0 < np; k0 += nb) {
+      transpose_rows(k0);
+      cproduct(nb, np, nb, Linv + k0 * nb, nullptr, nb, Btr, Bti, nb, 1.0, nullptr, nullptr, np, 0.0, 0.0,
+               rr + k0 * np, ri + k0 * np, np, false);
+      const int64_t rest = np - k0 - nb;
+      if (rest <= 0) continue;
+      transpose_rows(k0);
+      cproduct(rest, np, nb, G + (k0 + nb) * np + k0, nullptr, np, Btr, Bti, nb, -1.0, rr + (k0 + nb) * np,
+               ri + (k0 + nb) * np, np, 1.0, 0.0, rr + (k0 + nb) * np, ri + (k0 + nb) * np, np, false);
+    }
+    // backward: L^T R = Z
+    for (int64_t k0 = np - nb; k0 >= 0; k0 -= nb) {
+      transpose_rows(k0);
+      cproduct(nb, np, nb, LinvT + k0 * nb, nullptr, nb, Btr, Bti, nb, 1.0, nullptr, nullptr, np, 0.0, 0.0,
+               rr + k0 * np, ri + k0 * np, np, false);
+      if (k0 == 0) continue;
+      // Z_{<k} -= L_{k,<k}^T R_k
+      launch_transpose<T>(G + k0 * np, np, At, nb, nb, k0, stream_);
+      ++launches_;
+      transpose_rows(k0);
+      cproduct(k0, np, nb, At, nullptr, nb, Btr, Bti, nb, -1.0, rr, ri, np, 1.0, 0.0, rr, ri, np, false);
+    }
+  }
+
   // ---- blocked LU with partial pivoting and the two triangular solves (in place).
   void lu_solve(CM<T>& Q, CM<T>& P) {
     const int nb = 64;
@@ -846,7 +998,7 @@ struct fx_engine {
   void* h_psi = nullptr;
   bool u_valid = false;   // h_out holds the U of the last fx_walk_host
   size_t elem = 8;
-  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0};
+  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0};
   fx_stats stats{};
   std::string last_error;
 };
@@ -1030,6 +1182,7 @@ int fx_set_option(fx_handle h, int key, double value) {
     case FX_OPT_IPE: h->opts.ipe = v != 0; return FX_OK;
     case FX_OPT_REFINE: return v == 0 ? FX_OK : fail(h, fx::Error{FX_ERR_VALUE, "refinement not available"});
     case FX_OPT_DEBUG_STAGE: h->opts.debug_stage = v; return FX_OK;
+    case FX_OPT_PROFILE: h->opts.profile = v != 0; return FX_OK;
   }
   return fail(h, fx::Error{FX_ERR_VALUE, "unknown option"});
 }

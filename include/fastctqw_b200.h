@@ -56,10 +56,12 @@ enum fx_status {
 
 /* Arithmetic forms for the matrix products (fx_set_option(FX_OPT_FORM, ...)). */
 enum fx_form {
-  FX_FORM_PLAIN = 0,  /* FP32-faithful: BF16 3-way split, 6 products, FP32 accumulate */
-  FX_FORM_MIXED = 1,  /* BF16 hi+lo split, 3 products (hi*hi, hi*lo, lo*hi)           */
-  FX_FORM_SIMT = 2,   /* CUDA-core FP32/FP64 FMA products (checker / FP64 engine)    */
-  FX_FORM_FP64 = 3    /* FP64 engine (complex128 / float64 handles)                   */
+  FX_FORM_PLAIN = 0,  /* int8 tensor-core products of 5 (FP64 masters) or 4 (FP32)
+                         Ozaki slices, exact int32 accumulation; default for complex64 */
+  FX_FORM_MIXED = 1,  /* BF16 hi+lo split, 3 products (hi*hi, hi*lo, lo*hi), FP32
+                         accumulate, FP32 masters (complex64 / float32 handles)       */
+  FX_FORM_SIMT = 2,   /* CUDA-core FP32 FMA products, FP32 masters (checker)          */
+  FX_FORM_FP64 = 3    /* CUDA-core FP64 products (default for complex128 / float64)   */
 };
 
 enum fx_option {
@@ -71,9 +73,11 @@ enum fx_option {
   FX_OPT_TIMEOUT_MS = 5,  /* bound of every device-side wait (default 2000)            */
   FX_OPT_IPE = 6,         /* 1: square in I+E form (default 1)                         */
   FX_OPT_REFINE = 7,      /* iterative-refinement steps of the Pade solve (default 0)  */
-  FX_OPT_DEBUG_STAGE = 8  /* diagnostics: k > 0 makes run write intermediate k instead of
+  FX_OPT_DEBUG_STAGE = 8, /* diagnostics: k > 0 makes run write intermediate k instead of
                              U (1 Y, 2-4 A2/A4/A6, 5 U_pade, 6 V_pade, 7 R, 8+j after j
                              squarings) and stop                                       */
+  FX_OPT_PROFILE = 9      /* 1: CUDA-event timing of every tensor-core product launch
+                             (fx_stats.prod_*)                                         */
 };
 
 /* What the last run did. */
@@ -86,10 +90,17 @@ typedef struct fx_stats {
   int32_t symmetric;    /* 1 if X^T == X (no transposes needed)          */
   int32_t gemm_launches;/* matrix-product kernel launches in the run     */
   int32_t launches;     /* all kernel launches of the run                */
+  int32_t solver;       /* 0 pivoted LU, 1 Cholesky of Q^H Q (normal Q)  */
+  int32_t reserved;
   double norm1;         /* ||X - shifts||_1                              */
   double d[5];          /* d4, d6, d8, d10, log2 ||(|A|)^27||_1          */
   double ms_total;      /* device time of the last run (CUDA events)     */
   double flops;         /* algorithmic real flops of the last run        */
+  double prod_ms;       /* summed duration of the int8 product launches  */
+  double prod_ops;      /* int8 tensor ops they issued                   */
+  double prod_flops;    /* real-arithmetic flops they computed           */
+  int32_t prod_launches;
+  int32_t reserved2;
 } fx_stats;
 
 int fx_create(size_t n, int dtype, fx_handle* out);

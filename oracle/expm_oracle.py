@@ -353,6 +353,14 @@ def expm(A: np.ndarray, shift: str = "none", return_selection: bool = False,
     return (R, sel) if return_selection else R
 
 
+def reference_cpu_expm(X: np.ndarray) -> np.ndarray:
+    """The reference's CPU path itself: ``scipy.linalg.expm(X)`` exactly as
+    ``Operator.buildExpmOperator`` calls it for device="cpu" (FastCTQW/Operator.py:74-76).
+    Used as the timed CPU baseline; it runs in X's precision on all host BLAS threads."""
+    import scipy.linalg
+    return scipy.linalg.expm(X)
+
+
 # ---------------------------------------------------------------- walk-level helpers
 
 def build_hamiltonian(A: np.ndarray, gamma: float = 1.0, laplacian: bool = False,
