@@ -161,7 +161,7 @@ class Engine:
         if shift is not None:
             self.set_option(OPT_SHIFT, shift)
         if structure is not None:
-            self.set_option(OPT_STRUCTURE, int(bool(structure)))
+            self.set_option(OPT_STRUCTURE, int(structure))
         if force_m is not None:
             self.set_option(OPT_FORCE_M, force_m)
         if force_s is not None:

@@ -117,7 +117,7 @@ class Pipeline {
     }
     // int8 slices (plain form): A (re, im) and Bt (re, im, -im), up to 5 slices each, + exponents.
     slices_.alloc((size_t)np_ * (size_t)np_ * kSlicePlanes + sizeof(int) * 2 * (size_t)np_ + 4096);
-    small_.alloc(sizeof(double) * (size_t)np_ * 16 + 4096);
+    small_.alloc(sizeof(double) * (size_t)np_ * 48 + 4096);
     ipiv_.alloc(sizeof(int) * (size_t)np_);
     err_.alloc(sizeof(int) * 8);
     const size_t tbytes = sizeof(T) * (size_t)np_ * kPanel;
@@ -343,9 +343,22 @@ class Pipeline {
     // ---- 7. squarings in I+E form
     const bool ipe = o.ipe != 0;
     if (ipe) add_identity(R, -1.0);
+    // With the rank-one shift, Y 1 = 0 = 1^T Y, hence E 1 = 0 = 1^T E exactly (E = R - I):
+    // restore that invariant after the solve and after every squaring (an exact identity of
+    // the iterates, O(N^2); rounding otherwise accumulates along the all-ones direction).
+    const bool project = rank1 && ipe;
+    auto proj = [&]() {
+      if (!project) return;
+      double* scr = (double*)small_.p + 8 * np_;
+      if (R.hr) launch_project_ones<T>(R.rb, n_, np_, scr, s);
+      if (R.hi) launch_project_ones<T>(R.ib, n_, np_, scr, s);
+      launches_ += 5 * ((int)R.hr + (int)R.hi);
+    };
+    proj();
     for (int k = 0; k < sq; ++k) {
       if (dump(8 + k, R, dU)) return;
       square(R, ipe);
+      proj();
     }
     if (dump(8 + sq, R, dU)) return;
 
@@ -721,7 +734,7 @@ class Pipeline {
   void square(CM<T>& R, bool ipe) {
     CM<T>& Tmp = slot_[kTmp];
     const double beta = ipe ? 2.0 : 0.0;
-    if (structured_ && R.hr && R.hi && form_ != FX_FORM_PLAIN) {
+    if (structured_ && R.hr && R.hi && (form_ != FX_FORM_PLAIN || opts_.structure >= 2)) {
       // Re and Im of R commute (both are functions of the same real symmetric matrix), so
       // Re' = (Re + Im)(Re - Im) and Im' = 2 Re Im.  The computed parts commute only up to
       // rounding; the forms that symmetrise by averaging, (M + M^T)/2, remove that commutator
@@ -892,34 +905,60 @@ class Pipeline {
       cproduct(rest, rest, nb, P21, nullptr, nb, P21, nullptr, nb, -1.0, G22, nullptr, np, 1.0, 0.0, G22, nullptr,
                np, true);
     }
-    auto transpose_rows = [&](int64_t r0) {   // rows [r0, r0+nb) of R -> Bt (np x nb)
-      launch_transpose<T>(rr + r0 * np, np, Btr, nb, nb, np, stream_);
-      launch_transpose<T>(ri + r0 * np, np, Bti, nb, nb, np, stream_);
+    // Triangular solves by recursive halving: the off-diagonal updates are large-K
+    // products, the leaves apply the inverted 128 x 128 diagonal blocks.
+    CM<T>& Sc = slot_[kBt];   // transposed right-hand-side blocks (two planes, np x np)
+    CM<T>& Sa = slot_[kS1];   // transposed L blocks
+    fwd_solve(G, Linv, rr, ri, 0, np, Sc);
+    bwd_solve(G, LinvT, rr, ri, 0, np, Sc, Sa);
+  }
+
+  // Rows [r0, r1) of R hold T; solve L[r0:r1, r0:r1] Z = T in place.
+  void fwd_solve(const T* G, const T* Linv, T* rr, T* ri, int64_t r0, int64_t r1, CM<T>& Sc) {
+    const int nb = kCholNb;
+    const int64_t np = np_;
+    if (r1 - r0 <= nb) {
+      launch_transpose<T>(rr + r0 * np, np, Sc.rb, nb, nb, np, stream_);
+      launch_transpose<T>(ri + r0 * np, np, Sc.ib, nb, nb, np, stream_);
       launches_ += 2;
-    };
-    // forward: L Z = R
-    for (int64_t k0 = 0; k0 < np; k0 += nb) {
-      transpose_rows(k0);
-      cproduct(nb, np, nb, Linv + k0 * nb, nullptr, nb, Btr, Bti, nb, 1.0, nullptr, nullptr, np, 0.0, 0.0,
-               rr + k0 * np, ri + k0 * np, np, false);
-      const int64_t rest = np - k0 - nb;
-      if (rest <= 0) continue;
-      transpose_rows(k0);
-      cproduct(rest, np, nb, G + (k0 + nb) * np + k0, nullptr, np, Btr, Bti, nb, -1.0, rr + (k0 + nb) * np,
-               ri + (k0 + nb) * np, np, 1.0, 0.0, rr + (k0 + nb) * np, ri + (k0 + nb) * np, np, false);
+      cproduct(nb, np, nb, Linv + r0 * nb, nullptr, nb, Sc.rb, Sc.ib, nb, 1.0, nullptr, nullptr, np, 0.0, 0.0,
+               rr + r0 * np, ri + r0 * np, np, false);
+      return;
     }
-    // backward: L^T R = Z
-    for (int64_t k0 = np - nb; k0 >= 0; k0 -= nb) {
-      transpose_rows(k0);
-      cproduct(nb, np, nb, LinvT + k0 * nb, nullptr, nb, Btr, Bti, nb, 1.0, nullptr, nullptr, np, 0.0, 0.0,
-               rr + k0 * np, ri + k0 * np, np, false);
-      if (k0 == 0) continue;
-      // Z_{<k} -= L_{k,<k}^T R_k
-      launch_transpose<T>(G + k0 * np, np, At, nb, nb, k0, stream_);
-      ++launches_;
-      transpose_rows(k0);
-      cproduct(k0, np, nb, At, nullptr, nb, Btr, Bti, nb, -1.0, rr, ri, np, 1.0, 0.0, rr, ri, np, false);
+    const int64_t mid = r0 + ((r1 - r0) / nb / 2) * nb;
+    fwd_solve(G, Linv, rr, ri, r0, mid, Sc);
+    const int64_t K = mid - r0, M = r1 - mid;
+    launch_transpose<T>(rr + r0 * np, np, Sc.rb, K, K, np, stream_);
+    launch_transpose<T>(ri + r0 * np, np, Sc.ib, K, K, np, stream_);
+    launches_ += 2;
+    cproduct(M, np, K, G + mid * np + r0, nullptr, np, Sc.rb, Sc.ib, K, -1.0, rr + mid * np, ri + mid * np, np, 1.0,
+             0.0, rr + mid * np, ri + mid * np, np, false);
+    fwd_solve(G, Linv, rr, ri, mid, r1, Sc);
+  }
+
+  // Rows [r0, r1) of R hold Z; solve L^T[r0:r1, r0:r1] R = Z in place.
+  void bwd_solve(const T* G, const T* LinvT, T* rr, T* ri, int64_t r0, int64_t r1, CM<T>& Sc, CM<T>& Sa) {
+    const int nb = kCholNb;
+    const int64_t np = np_;
+    if (r1 - r0 <= nb) {
+      launch_transpose<T>(rr + r0 * np, np, Sc.rb, nb, nb, np, stream_);
+      launch_transpose<T>(ri + r0 * np, np, Sc.ib, nb, nb, np, stream_);
+      launches_ += 2;
+      cproduct(nb, np, nb, LinvT + r0 * nb, nullptr, nb, Sc.rb, Sc.ib, nb, 1.0, nullptr, nullptr, np, 0.0, 0.0,
+               rr + r0 * np, ri + r0 * np, np, false);
+      return;
     }
+    const int64_t mid = r0 + ((r1 - r0) / nb / 2) * nb;
+    bwd_solve(G, LinvT, rr, ri, mid, r1, Sc, Sa);
+    // Z[r0:mid] -= L[mid:r1, r0:mid]^T R[mid:r1]
+    const int64_t M = mid - r0, K = r1 - mid;
+    launch_transpose<T>(G + mid * np + r0, np, Sa.rb, K, K, M, stream_);   // (M x K) = L block^T
+    launch_transpose<T>(rr + mid * np, np, Sc.rb, K, K, np, stream_);
+    launch_transpose<T>(ri + mid * np, np, Sc.ib, K, K, np, stream_);
+    launches_ += 3;
+    cproduct(M, np, K, Sa.rb, nullptr, K, Sc.rb, Sc.ib, K, -1.0, rr + r0 * np, ri + r0 * np, np, 1.0, 0.0,
+             rr + r0 * np, ri + r0 * np, np, false);
+    bwd_solve(G, LinvT, rr, ri, r0, mid, Sc, Sa);
   }
 
   // ---- blocked LU with partial pivoting and the two triangular solves (in place).
@@ -1168,7 +1207,10 @@ int fx_set_option(fx_handle h, int key, double value) {
       if (v < 0 || v > 2) return fail(h, fx::Error{FX_ERR_VALUE, "shift must be 0, 1 or 2"});
       h->opts.shift = v;
       return FX_OK;
-    case FX_OPT_STRUCTURE: h->opts.structure = v != 0; return FX_OK;
+    case FX_OPT_STRUCTURE:
+      if (v < 0 || v > 2) return fail(h, fx::Error{FX_ERR_VALUE, "structure must be 0, 1 or 2"});
+      h->opts.structure = v;
+      return FX_OK;
     case FX_OPT_FORCE_S: h->opts.force_s = v; return FX_OK;
     case FX_OPT_FORCE_M:
       if (v != -1 && v != 3 && v != 5 && v != 7 && v != 9 && v != 13)

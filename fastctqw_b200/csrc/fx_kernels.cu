@@ -726,3 +726,76 @@ void launch_symmetrize(T* a, int64_t n, int64_t ld, cudaStream_t s) {
 template void launch_symmetrize<float>(float*, int64_t, int64_t, cudaStream_t);
 template void launch_symmetrize<double>(double*, int64_t, int64_t, cudaStream_t);
 }  // namespace fx
+
+namespace fx {
+namespace {
+// Signed row sums (warp per row) and column sums (row-chunked, ordered) of the n x n block.
+template <typename T>
+__global__ void k_row_sums(const T* a, int64_t n, int64_t ld, double* rs) {
+  const int lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (row >= n) return;
+  double s = 0.0;
+  for (int64_t j = lane; j < n; j += 32) s += (double)a[row * ld + j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) rs[row] = s;
+}
+template <typename T>
+__global__ void k_col_sum_partials(const T* a, int64_t n, int64_t ld, int64_t rows_per_chunk, double* part) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int64_t r0 = (int64_t)blockIdx.y * rows_per_chunk;
+  const int64_t r1 = min(n, r0 + rows_per_chunk);
+  double s = 0.0;
+  for (int64_t i = r0; i < r1; ++i) s += (double)a[i * ld + j];
+  part[(int64_t)blockIdx.y * n + j] = s;
+}
+__global__ void k_vec_total(const double* v, int64_t n, double* out) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s += v[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = sh[0];
+}
+template <typename T>
+__global__ void k_apply_proj(T* a, int64_t n, int64_t ld, const double* rs, const double* cs, const double* tot) {
+  const int64_t total = n * n;
+  const double inv = 1.0 / (double)n, sig = tot[0] * inv * inv;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx / n, j = idx - (idx / n) * n;
+    a[i * ld + j] = (T)((double)a[i * ld + j] - rs[i] * inv - cs[j] * inv + sig);
+  }
+}
+}  // namespace
+
+template <typename T>
+void launch_project_ones(T* a, int64_t n, int64_t ld, double* scratch, cudaStream_t s) {
+  // scratch: rs (n), cs (n), tot (1), partials (32 n)
+  double* rs = scratch;
+  double* cs = rs + n;
+  double* tot = cs + n;
+  double* part = tot + 8;
+  k_row_sums<T><<<cdiv(n, 8), 256, 0, s>>>(a, n, ld, rs);
+  FX_LAUNCH_CHECK();
+  const int chunks = 32;
+  const int64_t rpc = (n + chunks - 1) / chunks;
+  k_col_sum_partials<T><<<dim3(cdiv(n, 128), chunks), 128, 0, s>>>(a, n, ld, rpc, part);
+  FX_LAUNCH_CHECK();
+  k_col_finish1<<<cdiv(n, 256), 256, 0, s>>>(part, chunks, n, cs);
+  FX_LAUNCH_CHECK();
+  k_vec_total<<<1, 256, 0, s>>>(rs, n, tot);
+  FX_LAUNCH_CHECK();
+  unsigned g = (unsigned)std::min<int64_t>((n * n + 255) / 256, 148 * 16);
+  k_apply_proj<T><<<g, 256, 0, s>>>(a, n, ld, rs, cs, tot);
+  FX_LAUNCH_CHECK();
+}
+template void launch_project_ones<float>(float*, int64_t, int64_t, double*, cudaStream_t);
+template void launch_project_ones<double>(double*, int64_t, int64_t, double*, cudaStream_t);
+}  // namespace fx

@@ -98,6 +98,11 @@ void launch_trsm_upper(const T* ure, const T* uim, int64_t ldu, int64_t r0, int 
                        T* bim, int64_t ldb, int64_t c0, int64_t cols, int* err,
                        cudaStream_t s);
 
+// A <- P A P with P = I - J/n on the n x n block (removes the components along the all-ones
+// vector on both sides).  scratch: at least 34 n + 8 doubles.
+template <typename T>
+void launch_project_ones(T* a, int64_t n, int64_t ld, double* scratch, cudaStream_t s);
+
 // Cholesky diagonal block: G_kk -> L_kk in place, Linv = L_kk^-1, LinvT = L_kk^-T (nb x nb).
 template <typename T>
 void launch_potrf_inv(T* G, int64_t ld, int64_t k0, int nb, T* Linv, T* LinvT, int* err,

@@ -71,9 +71,16 @@ def test_reference_walk_fixtures(golden):
             inf = eo.infidelity(psi, c[f"psi_eig_{kind}"])
             assert inf <= INFID, (name, kind, inf)
             if "U_eig" in c:
+                # U is compared with the oracle on the same (rounded) input X: for complex64
+                # data the rounding of X itself moves expm(X) away from the FP64 truth by up
+                # to ||dX||_2 (about 1e-5 for the t = 100 weighted case), which is not an
+                # error of the engine.
                 U = w.getOperator().getOperator()
+                dt = np.complex64 if A.dtype == np.float32 else np.complex128
+                H = eo.build_hamiltonian(A, float(c["gamma"]), bool(c["laplacian"]), dtype=dt)
+                Uo = eo.expm(eo.walk_generator(H, float(c["t"]), dt).astype(np.complex128))
                 tol = C64_REL if A.dtype == np.float32 else C128_REL
-                assert eo.rel_error(U, c["U_eig"]) < tol, (name, eo.rel_error(U, c["U_eig"]))
+                assert eo.rel_error(U, Uo) < tol, (name, eo.rel_error(U, Uo))
             w.free()
 
 
