@@ -180,6 +180,7 @@ def main():
     ap.add_argument("--ref-sample-n", type=int, default=1024)
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 infidelity check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) leg")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -279,7 +280,7 @@ def main():
 
     # ---- end to end through the drop-in API (host ndarray in, host ndarray out)
     e2e = None
-    if rank == 0:
+    if rank == 0 and not args.no_e2e:
         X_pinned = torch.from_numpy(X).pin_memory().numpy()
         em = fastexpm.ExpMatComplex64(n)
         em.configure(form=args.form)

@@ -64,21 +64,26 @@ def test_reference_walk_fixtures(golden):
         if "psi_ref_e0" not in c:
             continue
         A = c["A"]
+        # The oracle runs on the same (rounded) input X as the engine: for complex64 data the
+        # rounding of X itself moves expm(X) away from the FP64 truth of the exact H by up to
+        # ||dX||_2 (about 1e-5 for the t = 100 weighted case, where even the exact expm of the
+        # rounded X has infidelity 4.3e-10 against the exact H), which is not an error of the
+        # engine.  Against the exact H the engine must do no worse than the reference's own
+        # result (psi_ref, scipy.linalg.expm in the input precision).
+        dt = np.complex64 if A.dtype == np.float32 else np.complex128
+        H = eo.build_hamiltonian(A, float(c["gamma"]), bool(c["laplacian"]), dtype=dt)
+        Uo = eo.expm(eo.walk_generator(H, float(c["t"]), dt).astype(np.complex128))
         for kind in ("uniform", "e0", "random"):
             w = Ctqw(A, State(c[f"psi0_{kind}"]), float(c["gamma"]), bool(c["laplacian"]))
             w.runWalk(float(c["t"]))
             psi = w.getFinalState().getState()
-            inf = eo.infidelity(psi, c[f"psi_eig_{kind}"])
+            inf = eo.infidelity(psi, Uo @ c[f"psi0_{kind}"].astype(np.complex128))
             assert inf <= INFID, (name, kind, inf)
+            inf_truth = eo.infidelity(psi, c[f"psi_eig_{kind}"])
+            inf_ref = eo.infidelity(c[f"psi_ref_{kind}"], c[f"psi_eig_{kind}"])
+            assert inf_truth <= max(INFID, inf_ref), (name, kind, inf_truth, inf_ref)
             if "U_eig" in c:
-                # U is compared with the oracle on the same (rounded) input X: for complex64
-                # data the rounding of X itself moves expm(X) away from the FP64 truth by up
-                # to ||dX||_2 (about 1e-5 for the t = 100 weighted case), which is not an
-                # error of the engine.
                 U = w.getOperator().getOperator()
-                dt = np.complex64 if A.dtype == np.float32 else np.complex128
-                H = eo.build_hamiltonian(A, float(c["gamma"]), bool(c["laplacian"]), dtype=dt)
-                Uo = eo.expm(eo.walk_generator(H, float(c["t"]), dt).astype(np.complex128))
                 tol = C64_REL if A.dtype == np.float32 else C128_REL
                 assert eo.rel_error(U, Uo) < tol, (name, eo.rel_error(U, Uo))
             w.free()
