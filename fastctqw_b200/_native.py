@@ -66,6 +66,10 @@ SIGNATURES = {
                        ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int64,
                        ctypes.c_float, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
     "fx_product_error": [],
+    "fx_product_f32_noalloc": [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                               ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                               ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int64,
+                               ctypes.c_float, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
     "fx_gpu_memory_gb": [],
     "fx_device_ok": [],
     "fx_version": [],

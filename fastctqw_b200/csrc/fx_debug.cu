@@ -13,6 +13,11 @@ namespace {
 std::string g_dbg_err;
 }
 
+namespace fx {
+// Message of the last failed diagnostic product call (read back by fx_product_error).
+void set_product_error(const std::string& msg) { g_dbg_err = msg; }
+}  // namespace fx
+
 extern "C" {
 
 int fx_product_f32(int form, int64_t M, int64_t N, int64_t K, const float* A, int64_t lda,

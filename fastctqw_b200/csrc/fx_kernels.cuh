@@ -169,6 +169,8 @@ void launch_gemm_i8(int S, int64_t M, int64_t N, int64_t K, const I8Term* terms,
                     int64_t lda, int64_t ldb, const int* aexp, const int* bexp, double alpha,
                     double beta, const TO* C, int64_t ldc, double gamma, TO* D, int64_t ldd, bool sym,
                     int* err, unsigned timeout_ms, cudaStream_t s);
+// Records the message returned by fx_product_error (fx_debug.cu).
+void set_product_error(const std::string& msg);
 // In place A <- (A + A^T) / 2 of an n x n plane (exact symmetry of a result known to be
 // symmetric in exact arithmetic).
 template <typename T>

@@ -134,6 +134,20 @@ int fx_product_f32(int form, int64_t M, int64_t N, int64_t K, const float* A, in
                    int64_t ldc, float gamma, float* D, int64_t ldd, void* stream);
 const char* fx_product_error(void);
 
+/* Allocation-free form of fx_product_f32 with FX_FORM_PLAIN (4 int8 slices, exact int32
+ * accumulation on the tensor cores); no counterpart in the reference.  For callers that must
+ * not allocate device memory once they are running (a pool that owns the device, an
+ * allocator callback, a host that sizes all GPU memory at start-up): the slice scratch lives
+ * in one fixed 16 MiB array of device memory inside the library, present on every GPU that
+ * loads it until the process exits.  Needs 4 (M + N) K + 4 (M + N) + 512 bytes of it (M, N
+ * multiples of 16, K of 64) and returns FX_ERR_VALUE beyond that.  The first call on a device
+ * looks the array's device address up (make it before any stream capture).  All calls share
+ * the array: calls that overlap on the GPU race; order them on one stream.  Messages through
+ * fx_product_error. */
+int fx_product_f32_noalloc(int64_t M, int64_t N, int64_t K, const float* A, int64_t lda,
+                           const float* Bt, int64_t ldb, float alpha, float beta, const float* C,
+                           int64_t ldc, float gamma, float* D, int64_t ldd, void* stream);
+
 /* Device memory currently in use on the current device, GB. */
 double fx_gpu_memory_gb(void);
 /* 1 if a device with compute capability 10.x is present. */
