@@ -167,6 +167,89 @@ def full_size_selection(n_full, n_sample, sel_sample):
     return (13, sel_sample[1] + int(round(math.log2(n_full / n_sample))))
 
 
+def batch_workload(count: int, seed: int, nmin: int, nmax: int):
+    """The uneven batch: `count` walks, N ~ U{nmin..nmax}, alternating random d-regular
+    (d ~ U{3..16}) and G(N, p) (p ~ U[0.05, 0.5]) adjacency graphs, t log-uniform in [0.5, 50],
+    X = -1j*H*t with H = -A (FastCTQW/Operator.py:49-56) in complex64, psi0 uniform."""
+    from fastctqw_b200 import graphs
+    specs = graphs.uneven_batch(count, seed=seed, nmin=nmin, nmax=nmax)
+    As, Xs, P0 = [], [], []
+    for sp in specs:
+        A = sp.adjacency(np.float32)
+        As.append(A)
+        Xs.append(np.asarray(1j * A * np.float32(sp.t), dtype=np.complex64))
+        P0.append(graphs.uniform_state(sp.n))
+    return specs, As, Xs, P0
+
+
+def bench_batch(args, dev):
+    """Grouped batch (one CUDA graph of grouped launches) vs a loop of the per-walk plain form,
+    both with the inputs resident in HBM and timed with CUDA events."""
+    import torch
+    from fastctqw_b200._native import Engine
+    from fastctqw_b200.batch import WalkBatch
+    specs, As, Xs, P0 = batch_workload(args.batch_count, args.seed, args.batch_nmin, args.batch_nmax)
+    ns = [X.shape[0] for X in Xs]
+    dX = [torch.from_numpy(X).to(dev) for X in Xs]
+    dP0 = [torch.from_numpy(p).to(dev) for p in P0]
+    dP = [torch.empty_like(p) for p in dP0]
+    stream = torch.cuda.current_stream(dev)
+    b = WalkBatch(ns)
+    for _ in range(max(1, args.warmup)):
+        b.run_device(dX, dP0, dP, stream)
+    torch.cuda.synchronize()
+    reps = max(1, min(args.steps, 3))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(reps):
+        b.run_device(dX, dP0, dP, stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    batch_ms = ev0.elapsed_time(ev1) / reps
+    info = b.info()
+    m, s = b.selection()
+    # accuracy on the largest walks: FP64 eigendecomposition of A on the device
+    worst = 0.0
+    for k in sorted(range(len(ns)), key=lambda k: -ns[k])[:4]:
+        A = torch.from_numpy(As[k]).to(dev, torch.float64)
+        lam, V = torch.linalg.eigh(A)
+        t32 = float(np.float32(specs[k].t))
+        p0 = dP0[k].to(torch.complex128)
+        ref = V.to(torch.complex128) @ (torch.exp(1j * lam * t32) * (V.T.to(torch.complex128) @ p0))
+        psi = dP[k].to(torch.complex128)
+        ov = torch.vdot(ref, psi).abs() ** 2 / (torch.vdot(ref, ref).real * torch.vdot(psi, psi).real)
+        worst = max(worst, float(1.0 - ov))
+    b.close()
+    del dP
+    # per-walk loop of the plain form (compute only: engines are created outside the timing)
+    loop_ms = 0.0
+    if not args.no_batch_loop:
+        outs = [torch.empty_like(p) for p in dP0]
+        for k in range(len(ns)):
+            e = Engine(ns[k], np.complex64)
+            e.walk_device(dX[k], dP0[k], outs[k], None, stream)   # warm-up of this size
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            e.walk_device(dX[k], dP0[k], outs[k], None, stream)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            loop_ms += ev0.elapsed_time(ev1)
+            e.close()
+    walks = len(ns)
+    return {
+        "workload": f"{walks} walks, N ~ U{{{args.batch_nmin}..{args.batch_nmax}}}, alternating d-regular "
+                    f"(d 3..16) / G(N, p 0.05..0.5) adjacency, t log-uniform [0.5, 50], complex64, psi0 uniform",
+        "walks_per_s": round(walks / (batch_ms * 1e-3), 1), "ms": round(batch_ms, 2),
+        "loop_walks_per_s": round(walks / (loop_ms * 1e-3), 1) if loop_ms else None,
+        "loop_ms": round(loop_ms, 1) if loop_ms else None,
+        "speedup_vs_loop": round(loop_ms / batch_ms, 2) if loop_ms else None,
+        "launches_per_batch": info["launches"], "algorithmic_tflops": round(info["flops"] / (batch_ms * 1e-3) / 1e12, 1),
+        "m_hist": {int(k): int(v) for k, v in zip(*np.unique(m, return_counts=True))},
+        "s_max": int(s.max()), "s_mean": round(float(s.mean()), 2),
+        "worst_infidelity_4_largest": worst,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -181,6 +264,12 @@ def main():
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 infidelity check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")
+    ap.add_argument("--no-batch-loop", action="store_true", help="skip the per-walk loop of the batch leg")
+    ap.add_argument("--batch-only", action="store_true", help="run only the uneven-batch leg")
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--batch-nmin", type=int, default=64)
+    ap.add_argument("--batch-nmax", type=int, default=2048)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -199,6 +288,11 @@ def main():
 
     from fastctqw_b200 import fastexpm
     from fastctqw_b200._native import Engine
+
+    if args.batch_only:
+        if rank == 0:
+            print(json.dumps({"batch": bench_batch(args, torch.device("cuda", local))}), flush=True)
+        return
 
     n = args.n
     A, H, X = workload(n, args.seed, args.t)
@@ -303,6 +397,13 @@ def main():
                "sample": f"scipy.linalg.expm at N={args.ref_sample_n} (m={sel_s[0]}, s={sel_s[1]}), best of 2, "
                          f"scaled to N={n} (m={sel_full[0]}, s={sel_full[1]}) by 8N^3(pi_m+s)+(8/3)N^3+8N^3"}
 
+    batch = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        eng.close()
+        del dX, dU, dpsi0, dpsi
+        torch.cuda.empty_cache()
+        batch = bench_batch(args, dev)
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
@@ -315,7 +416,7 @@ def main():
                        "l2": "working set ~25 GB >> 126 MB L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
             "clocks": clk, "e2e": e2e, "gpu_launches": int(st["launches"]) * args.steps,
-            "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy,
+            "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "batch": batch,
             "algorithmic_tflops": round(st["flops"] / (ms_per_step * 1e-3) / 1e12, 2),
         }
         print(json.dumps(out), flush=True)

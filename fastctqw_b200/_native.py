@@ -70,11 +70,26 @@ SIGNATURES = {
                                ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
                                ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int64,
                                ctypes.c_float, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
+    "fx_batch_create": [ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64), ctypes.c_int,
+                        ctypes.POINTER(ctypes.c_void_p)],
+    "fx_batch_destroy": [ctypes.c_void_p],
+    "fx_batch_set_option": [ctypes.c_void_p, ctypes.c_int, ctypes.c_double],
+    "fx_batch_walk_device": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                             ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                             ctypes.c_void_p],
+    "fx_batch_walk_host": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                           ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)],
+    "fx_batch_selection": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                           ctypes.POINTER(ctypes.c_int32)],
+    "fx_batch_info": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)],
+    "fx_batch_last_error": [ctypes.c_void_p],
     "fx_gpu_memory_gb": [],
     "fx_device_ok": [],
     "fx_version": [],
 }
 RESTYPES = {"fx_last_error": ctypes.c_char_p, "fx_version": ctypes.c_char_p,
+            "fx_batch_last_error": ctypes.c_char_p,
             "fx_product_error": ctypes.c_char_p,
             "fx_gpu_memory_gb": ctypes.c_double}
 

@@ -1,0 +1,123 @@
+"""Batched walks: many independent walks of uneven sizes through grouped device launches.
+
+The reference runs one walk at a time (``Ctqw.runWalk``, FastCTQW/Ctqw.py:90-94, one
+``MatrixExpCalculator`` per matrix size, include/MatrixExpCalculator.h:17-103).
+:class:`WalkBatch` runs ``psi_w = expm(X_w) psi0_w`` for a whole list of walks at once through
+the C ABI's ``fx_batch_*`` entry points: every phase of the scaling-and-squaring pipeline is
+one grouped launch over all walks, and everything after the (m, s) selection is replayed as
+one CUDA graph.  The generators must be walk generators ``X = -1j * H * t`` with a real
+symmetric H (``ValueError`` otherwise); the dtype is complex64 or complex128.
+
+    >>> b = WalkBatch([A.shape[0] for A in adjs])
+    >>> psis = b.run([walk_generator(A, t) for A, t in zip(adjs, ts)], psi0s)
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native
+from ._native import check, lib
+
+OPT_GRAPH, OPT_TIMEOUT_MS, OPT_FORCE_M = 0, 1, 2
+
+
+def _check(rc: int, h) -> None:
+    if rc == _native.OK:
+        return
+    msg = lib().fx_batch_last_error(h)
+    msg = msg.decode() if msg else f"error code {rc}"
+    try:
+        check(rc)
+    except Exception as e:  # noqa: BLE001 - re-raise the mapped type with the batch message
+        raise type(e)(msg) from None
+
+
+def walk_generator(A: np.ndarray, t: float, gamma: float = 1.0, laplacian: bool = False,
+                   dtype=np.complex64) -> np.ndarray:
+    """X = -1j * H * t with H = -gamma A or -gamma (D - A) (FastCTQW/Operator.py:49-56)."""
+    A = np.asarray(A, dtype=np.float64)
+    H = -gamma * ((np.diag(A.sum(axis=1)) - A) if laplacian else A)
+    return np.asarray(-1j * H * t, dtype=dtype)
+
+
+class WalkBatch:
+    """Owner of one ``fx_batch`` handle: device workspace for walks of sizes ``ns``."""
+
+    def __init__(self, ns, dtype=np.complex64, graph: bool = True) -> None:
+        self.ns = [int(n) for n in ns]
+        self.dtype = np.dtype(dtype)
+        if self.dtype not in (np.dtype(np.complex64), np.dtype(np.complex128)):
+            raise TypeError("batched walks are complex64 or complex128")
+        arr = (ctypes.c_int64 * len(self.ns))(*self.ns)
+        h = ctypes.c_void_p()
+        _check(lib().fx_batch_create(len(self.ns), arr, _native.DTYPE_CODE[self.dtype], ctypes.byref(h)), None)
+        self._h = h
+        if not graph:
+            self.set_option(OPT_GRAPH, 0)
+
+    def set_option(self, key: int, value: float) -> None:
+        _check(lib().fx_batch_set_option(self._h, int(key), float(value)), self._h)
+
+    def _ptrs(self, xs):
+        return (ctypes.c_void_p * len(xs))(*[ctypes.c_void_p(x) for x in xs])
+
+    def run(self, Xs, psi0s) -> list[np.ndarray]:
+        """psi_w = expm(X_w) psi0_w for host ndarrays; returns a list of new arrays."""
+        if len(Xs) != len(self.ns) or len(psi0s) != len(self.ns):
+            raise ValueError(f"expected {len(self.ns)} generators and states")
+        xs, p0, p1 = [], [], []
+        for X, p, n in zip(Xs, psi0s, self.ns):
+            X = np.ascontiguousarray(X, dtype=self.dtype)
+            if X.shape != (n, n):
+                raise ValueError(f"Input matrix must have shape ({n}, {n}).")
+            p = np.ascontiguousarray(p, dtype=self.dtype).reshape(-1)
+            if p.shape != (n,):
+                raise ValueError(f"state must have length {n}")
+            xs.append(X)
+            p0.append(p)
+            p1.append(np.empty(n, dtype=self.dtype))
+        _check(lib().fx_batch_walk_host(self._h, self._ptrs([x.ctypes.data for x in xs]),
+                                        self._ptrs([p.ctypes.data for p in p0]),
+                                        self._ptrs([p.ctypes.data for p in p1])), self._h)
+        return p1
+
+    def run_device(self, dXs, dpsi0s, dpsis, stream=None) -> None:
+        """The same on device buffers (torch CUDA tensors or raw pointers)."""
+        P = _native.Engine._ptr
+        s = _native.Engine._stream(stream)
+        _check(lib().fx_batch_walk_device(self._h, self._ptrs([P(x) for x in dXs]),
+                                          self._ptrs([P(x) for x in dpsi0s]),
+                                          self._ptrs([P(x) for x in dpsis]), s), self._h)
+
+    def selection(self) -> tuple[np.ndarray, np.ndarray]:
+        """(m, s) of every walk in the last run."""
+        m = (ctypes.c_int32 * len(self.ns))()
+        s = (ctypes.c_int32 * len(self.ns))()
+        _check(lib().fx_batch_selection(self._h, m, s), self._h)
+        return np.array(m[:], dtype=np.int32), np.array(s[:], dtype=np.int32)
+
+    def info(self) -> dict:
+        """Device time (ms), algorithmic flops and kernel launches of the last run."""
+        ms, fl, nl = ctypes.c_double(), ctypes.c_double(), ctypes.c_int32()
+        _check(lib().fx_batch_info(self._h, ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(nl)), self._h)
+        return {"ms": ms.value, "flops": fl.value, "launches": nl.value}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().fx_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

@@ -1,0 +1,1779 @@
+// Batched walks: many independent expm(X_w) psi0_w of uneven sizes in grouped launches.
+//
+// The per-walk engine (fx_engine.cu) issues a few hundred launches and several host
+// round trips per walk; for hundreds of small and medium walks that is launch- and
+// latency-bound.  Here every phase of the pipeline is one grouped launch over all walks that
+// take part in it:
+//   * grouped int8 Ozaki-slice products (one tile list over all walks' problems, see
+//     k_gemm_i8<.., true> in fx_gemm_i8.cu), with the slices of all walks stacked in common
+//     slice planes,
+//   * grouped elementwise / reduction kernels (this file): grid.y runs over a list of walks,
+//   * a device-side block 1-norm estimator (one CTA per walk) so that the selection of (m, s)
+//     needs a single host round trip for the whole batch,
+//   * the Pade solve for X = i*(real symmetric) as G = Q^H Q = L L^T (blocked Cholesky, one
+//     CTA per walk for the diagonal blocks), the explicit inverse X = L^-1 (blocked, backward),
+//     and two large triangle-aware products Z = P2 X^T, R^T = Z X (R = G^-1 P2 is symmetric).
+// Everything after the selection is recorded once and replayed as one CUDA graph.
+//
+// Scope: walk generators X = i*(real symmetric) (the walk family X = -iHt with a real
+// symmetric H), complex64 or complex128 storage, FP64 masters and 5 int8 slices (the plain
+// form of the per-walk engine).  The selection follows the per-walk engine (Al-Mohy & Higham
+// 2009, Algorithm 6.1; normal input, so l(A, m) = 0).
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fx_kernels.cuh"
+
+namespace fx {
+namespace {
+
+constexpr int kS = 5;          // int8 slices (FP64 masters)
+constexpr int kNb = 128;       // Cholesky / inverse block
+constexpr int kEstScratch = 8; // doubles per row of a walk in the estimator scratch
+
+struct BWalk {
+  int n, np;
+  int64_t off;    // element offset of the walk's np x np block in every master arena
+  int64_t row0;   // first row of the walk in stacked per-row arrays (sum of np of earlier walks)
+};
+
+// ------------------------------------------------------------------ grouped elementwise
+struct Planes4 {
+  const double* m[4];
+};
+
+// D = sum_k c_k M_k + g I on the np x np block of every listed walk; coef[w] = (c0..c3, g).
+__global__ void kb_combo(double* D, Planes4 M, const int* list, const BWalk* wk, const double* coef) {
+  const int w = list[blockIdx.y];
+  const BWalk b = wk[w];
+  const int64_t n2 = (int64_t)b.np * b.np;
+  const double* c = coef + 5 * w;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (M.m[k]) v += c[k] * M.m[k][b.off + idx];
+    const int64_t i = idx / b.np;
+    if (idx - i * b.np == i) v += c[4];
+    D[b.off + idx] = v;
+  }
+}
+
+// Statistics of the interleaved input of each walk, warp per row i < n:
+// rowstat[kRS * (row0 + i)] = (Re row sum, Im row sum, Re X_ii, Im X_ii, sum |Re| + |Im|);
+// flags[w] |= 1 (Re != 0), 2 (not symmetric), 4 (non-finite).
+constexpr int kRS = 6;
+template <typename C>
+__global__ void kb_stats(const void* const* X, const int* list, const BWalk* wk, double* rowstat, int* flags) {
+  const int w = list[blockIdx.y];
+  const BWalk b = wk[w];
+  const C* x = (const C*)X[w];
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x / 32;
+  int f = 0;
+  for (int64_t i = (int64_t)blockIdx.x * wpb + threadIdx.x / 32; i < b.n; i += (int64_t)gridDim.x * wpb) {
+    double sr = 0, si = 0, sa = 0;
+    for (int64_t j = lane; j < b.n; j += 32) {
+      const C v = x[i * b.n + j];
+      const double vr = (double)v.x, vi = (double)v.y;
+      sr += vr;
+      si += vi;
+      sa += fabs(vr) + fabs(vi);
+      if (vr != 0.0) f |= 1;
+      if (!isfinite(vr) || !isfinite(vi)) f |= 4;
+      if (j > i) {
+        const C u = x[j * b.n + i];
+        if (u.x != v.x || u.y != v.y) f |= 2;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, o);
+      si += __shfl_xor_sync(0xffffffffu, si, o);
+      sa += __shfl_xor_sync(0xffffffffu, sa, o);
+    }
+    if (lane == 0) {
+      const C d = x[i * b.n + i];
+      double* r = rowstat + kRS * (b.row0 + i);
+      r[0] = sr;
+      r[1] = si;
+      r[2] = (double)d.x;
+      r[3] = (double)d.y;
+      r[4] = sa;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) f |= __shfl_xor_sync(0xffffffffu, f, o);
+  if (lane == 0 && f) atomicOr(flags + w, f);
+}
+
+// One CTA per walk: the shifts.  mu = trace / n (ordered sum of the diagonal); the rank-one
+// shift applies when every row sum equals row 0's within the rounding of a sum,
+// 4 n 2^-53 max_i sum_j |X_ij| (the input is exactly symmetric, so the column sums are the
+// same numbers); then nu = c0 - mu.  out[8 w ..] = (mu re, mu im, nu re, nu im, rank1, mu_im,
+// nu_im / n, 0); the last two are the load parameters of kb_load_imag.
+__global__ void kb_walk_reduce(const int* list, const BWalk* wk, const double* rowstat, double* out) {
+  const int w = list[blockIdx.x];
+  const BWalk b = wk[w];
+  const double* r = rowstat + kRS * b.row0;
+  __shared__ double s_max[256];
+  __shared__ double s_dev[256];
+  const double c0r = r[0], c0i = r[1];
+  double mx = 0.0, dev = 0.0;
+  for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
+    mx = fmax(mx, r[kRS * i + 4]);
+    dev = fmax(dev, fmax(fabs(r[kRS * i] - c0r), fabs(r[kRS * i + 1] - c0i)));
+  }
+  s_max[threadIdx.x] = mx;
+  s_dev[threadIdx.x] = dev;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s_max[threadIdx.x] = fmax(s_max[threadIdx.x], s_max[threadIdx.x + o]);
+      s_dev[threadIdx.x] = fmax(s_dev[threadIdx.x], s_dev[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double tr = 0, ti = 0;
+    for (int i = 0; i < b.n; ++i) {
+      tr += r[kRS * i + 2];
+      ti += r[kRS * i + 3];
+    }
+    const double n = b.n;
+    const double mur = tr / n, mui = ti / n;
+    const bool rank1 = b.n > 1 && s_dev[0] <= 4.0 * n * 0x1p-53 * s_max[0];
+    const double nur = rank1 ? c0r - mur : 0.0, nui = rank1 ? c0i - mui : 0.0;
+    double* o = out + 8 * w;
+    o[0] = mur;
+    o[1] = mui;
+    o[2] = nur;
+    o[3] = nui;
+    o[4] = rank1 ? 1.0 : 0.0;
+    o[5] = mui;
+    o[6] = nui / n;
+    o[7] = 0.0;
+  }
+}
+
+// Y = Im(X) - mu_im I - nu_im/n J on the n x n block, 0 in the padding (imaginary plane of the
+// shifted generator; its real plane is zero for X = i*(real symmetric)).  sh[8 w + 5, 6] =
+// (mu_im, nu_im/n) as written by kb_walk_reduce.
+template <typename C>
+__global__ void kb_load_imag(const void* const* X, const int* list, const BWalk* wk, const double* sh, double* Y) {
+  const int w = list[blockIdx.y];
+  const BWalk b = wk[w];
+  const C* x = (const C*)X[w];
+  const double mu = sh[8 * w + 5], nun = sh[8 * w + 6];
+  const int64_t n2 = (int64_t)b.np * b.np;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx / b.np, j = idx - i * b.np;
+    double v = 0.0;
+    if (i < b.n && j < b.n) v = (double)x[i * b.n + j].y - (i == j ? mu : 0.0) - nun;
+    Y[b.off + idx] = v;
+  }
+}
+
+// Absolute row sums of a symmetric plane (= column sums), warp per row -> rs[row0 + i].
+__global__ void kb_abs_rowsums(const double* P, const int* list, const BWalk* wk, double* rs) {
+  const int w = list[blockIdx.y];
+  const BWalk b = wk[w];
+  const int lane = threadIdx.x & 31, wpb = blockDim.x / 32;
+  for (int64_t i = (int64_t)blockIdx.x * wpb + threadIdx.x / 32; i < b.np; i += (int64_t)gridDim.x * wpb) {
+    const double* row = P + b.off + i * b.np;
+    double s = 0;
+    for (int64_t j = lane; j < b.np; j += 32) s += fabs(row[j]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) rs[b.row0 + i] = s;
+  }
+}
+// Signed row sums over the n x n block (the projection along the all-ones vector).
+__global__ void kb_rowsums(const double* P, const int* list, const BWalk* wk, double* rs) {
+  const int w = list[blockIdx.y];
+  const BWalk b = wk[w];
+  const int lane = threadIdx.x & 31, wpb = blockDim.x / 32;
+  for (int64_t i = (int64_t)blockIdx.x * wpb + threadIdx.x / 32; i < b.n; i += (int64_t)gridDim.x * wpb) {
+    const double* row = P + b.off + i * b.np;
+    double s = 0;
+    for (int64_t j = lane; j < b.n; j += 32) s += row[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) rs[b.row0 + i] = s;
+  }
+}
+// One CTA per walk: out[w * stride + slot] = max (mode 0) or sum (mode 1) of v[row0 .. row0 + len).
+__global__ void kb_walk_vec_reduce(const double* v, const int* list, const BWalk* wk, int use_np, int mode,
+                                   double* out, int stride, int slot) {
+  const int w = list[blockIdx.x];
+  const BWalk b = wk[w];
+  const int len = use_np ? b.np : b.n;
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < len; i += blockDim.x) {
+    const double x = v[b.row0 + i];
+    acc = mode == 0 ? fmax(acc, x) : acc + x;
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] = mode == 0 ? fmax(sh[threadIdx.x], sh[threadIdx.x + o]) : sh[threadIdx.x] + sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[(int64_t)w * stride + slot] = sh[0];
+}
+// E <- E - (r_i + r_j)/n + T/n^2 on the n x n block (E symmetric, r its row sums, T = sum r).
+__global__ void kb_apply_proj(double* E, const int* list, const BWalk* wk, const double* rs, const double* tot) {
+  const int w = list[blockIdx.y];
+  const BWalk b = wk[w];
+  const int64_t n2 = (int64_t)b.n * b.n;
+  const double inv = 1.0 / b.n, sig = tot[w] * inv * inv;
+  const double* r = rs + b.row0;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx / b.n, j = idx - i * b.n;
+    double& e = E[b.off + i * b.np + j];
+    e = e - r[i] * inv - r[j] * inv + sig;
+  }
+}
+
+// Out-of-place transpose of every listed walk's np x np block (32 x 32 tiles).
+__global__ void kb_transpose(const double* in, double* out, const int* list, const BWalk* wk, int tiles_max) {
+  const int w = list[blockIdx.z];
+  const BWalk b = wk[w];
+  const int nt = b.np / 32;
+  __shared__ double tile[32][33];
+  for (int t = blockIdx.x; t < nt * nt; t += gridDim.x) {
+    const int64_t r0 = (int64_t)(t / nt) * 32, c0 = (int64_t)(t % nt) * 32;
+    for (int r = threadIdx.y; r < 32; r += 8) tile[r][threadIdx.x] = in[b.off + (r0 + r) * b.np + c0 + threadIdx.x];
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) out[b.off + (c0 + r) * b.np + r0 + threadIdx.x] = tile[threadIdx.x][r];
+    __syncthreads();
+  }
+  (void)tiles_max;
+}
+// A <- (A + A^T)/2 in place for every listed walk (32 x 32 tile pairs, upper tiles drive).
+__global__ void kb_symmetrize(double* A, const int* list, const BWalk* wk) {
+  const int w = list[blockIdx.z];
+  const BWalk b = wk[w];
+  const int nt = b.np / 32;
+  __shared__ double t1[32][33], t2[32][33];
+  for (int t = blockIdx.x; t < nt * nt; t += gridDim.x) {
+    const int bi = t / nt, bj = t % nt;
+    if (bi > bj) continue;   // uniform per block
+    double* a = A + b.off;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+      t1[r][threadIdx.x] = a[((int64_t)bi * 32 + r) * b.np + bj * 32 + threadIdx.x];
+      t2[r][threadIdx.x] = a[((int64_t)bj * 32 + r) * b.np + bi * 32 + threadIdx.x];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+      a[((int64_t)bi * 32 + r) * b.np + bj * 32 + threadIdx.x] = (t1[r][threadIdx.x] + t2[threadIdx.x][r]) * 0.5;
+      a[((int64_t)bj * 32 + r) * b.np + bi * 32 + threadIdx.x] = (t2[r][threadIdx.x] + t1[threadIdx.x][r]) * 0.5;
+    }
+    __syncthreads();
+  }
+}
+// Zero every listed walk's block, then copy the diagonal 128 x 128 blocks of L^-1 (stored
+// per walk as np x 128, block j at rows [128 j, 128 j + 128)) into X.
+__global__ void kb_init_inverse(double* X, const double* Linv, const int* list, const BWalk* wk, const int64_t* loff) {
+  const int w = list[blockIdx.y];
+  const BWalk b = wk[w];
+  const int64_t n2 = (int64_t)b.np * b.np;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx / b.np, j = idx - i * b.np;
+    double v = 0.0;
+    if (i / kNb == j / kNb) v = Linv[loff[w] + i * kNb + (j - (i / kNb) * kNb)];
+    X[b.off + idx] = v;
+  }
+}
+
+// psi = e^mu (E psi0 + psi0 + cj (1^T psi0) 1), warp per row; om[w] = (emu re, im, cj re, im);
+// E planes per walk (the squaring chain leaves E in one of two arena pairs).
+template <typename C>
+__global__ void kb_apply(const double* const* Ere, const double* const* Eim, const void* const* psi0,
+                         void* const* psi, const int* list, const BWalk* wk, const double* om, const double* psum) {
+  const int w = list[blockIdx.y];
+  const BWalk b = wk[w];
+  const C* p0 = (const C*)psi0[w];
+  C* p1 = (C*)psi[w];
+  if (!p0 || !p1) return;
+  const double* er = Ere[w] + b.off;
+  const double* ei = Eim[w] + b.off;
+  const int lane = threadIdx.x & 31, wpb = blockDim.x / 32;
+  const double* o = om + 4 * w;
+  for (int64_t i = (int64_t)blockIdx.x * wpb + threadIdx.x / 32; i < b.n; i += (int64_t)gridDim.x * wpb) {
+    double yr = 0, yi = 0;
+    for (int64_t j = lane; j < b.n; j += 32) {
+      const double a = er[i * b.np + j], c = ei[i * b.np + j];
+      const double x = (double)p0[j].x, y = (double)p0[j].y;
+      yr += a * x - c * y;
+      yi += a * y + c * x;
+    }
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) {
+      yr += __shfl_xor_sync(0xffffffffu, yr, k);
+      yi += __shfl_xor_sync(0xffffffffu, yi, k);
+    }
+    if (lane == 0) {
+      yr += (double)p0[i].x;
+      yi += (double)p0[i].y;
+      const double sr = psum[2 * w], si = psum[2 * w + 1];
+      yr += o[2] * sr - o[3] * si;
+      yi += o[2] * si + o[3] * sr;
+      C out;
+      out.x = (decltype(out.x))(o[0] * yr - o[1] * yi);
+      out.y = (decltype(out.y))(o[0] * yi + o[1] * yr);
+      p1[i] = out;
+    }
+  }
+}
+// psum[w] = sum_j psi0_w[j] (ordered, one thread).
+template <typename C>
+__global__ void kb_psi_sum(const void* const* psi0, const int* list, const BWalk* wk, double* psum) {
+  const int w = list[blockIdx.x];
+  if (threadIdx.x != 0) return;
+  const C* p = (const C*)psi0[w];
+  if (!p) return;
+  double sr = 0, si = 0;
+  for (int j = 0; j < wk[w].n; ++j) {
+    sr += (double)p[j].x;
+    si += (double)p[j].y;
+  }
+  psum[2 * w] = sr;
+  psum[2 * w + 1] = si;
+}
+
+// ------------------------------------------------------------------ block 1-norm estimator
+// Deterministic Higham-Tisseur estimate (t = 2) of ||M0 M1||_1 for real symmetric M0, M1 (so
+// M^H = M) of every listed walk: start columns 1/n and a fixed +-1/n pattern, at most 5
+// iterations, sign vectors, and the two largest unvisited entries of |Z| (ties to the lower
+// index) as the next unit columns -- the iteration of the oracle's normest1.  The products
+// are grid-wide grouped mat-vecs; the decisions run in one CTA per walk; a per-walk `done`
+// flag in device memory makes the fixed launch sequence (5 rounds) graph-capturable.
+// Per walk, scr holds kEstScratch vectors of np doubles: X0 X1 T0 T1 Y0 Y1 H VIS, and est
+// holds 4 doubles: (estimate, best index, done, unused).
+__device__ __forceinline__ double probe_sign_d(int64_t i) {
+  const uint32_t h = (uint32_t)((uint64_t)i * 0x9E3779B1ull);
+  return (h >> 31) & 1 ? -1.0 : 1.0;
+}
+__device__ __forceinline__ double* est_vec(double* scr, const BWalk& b, int k) {
+  return scr + (int64_t)kEstScratch * b.row0 + (int64_t)k * b.np;
+}
+enum { kEX0, kEX1, kET0, kET1, kEY0, kEY1, kEH, kEVIS };
+
+__global__ void kb_est_init(const int* list, const BWalk* wk, double* scr, double* est) {
+  const int w = list[blockIdx.x];
+  const BWalk b = wk[w];
+  double* X0 = est_vec(scr, b, kEX0);
+  double* X1 = est_vec(scr, b, kEX1);
+  double* VIS = est_vec(scr, b, kEVIS);
+  for (int i = threadIdx.x; i < b.np; i += blockDim.x) {
+    X0[i] = i < b.n ? 1.0 / b.n : 0.0;
+    X1[i] = (i < b.n && b.n > 1) ? probe_sign_d(i) / b.n : 0.0;
+    VIS[i] = 0.0;
+  }
+  if (threadIdx.x == 0) {
+    est[4 * w] = 0.0;
+    est[4 * w + 1] = 0.0;
+    est[4 * w + 2] = 0.0;
+  }
+}
+// (out0, out1) = M (in0, in1) for every listed walk that is not done; warp per row.
+__global__ void kb_est_matvec(const double* M, const int* list, const BWalk* wk, double* scr, const double* est,
+                              int in0, int out0) {
+  const int w = list[blockIdx.y];
+  if (est[4 * w + 2] != 0.0) return;
+  const BWalk b = wk[w];
+  const double* x0 = est_vec(scr, b, in0);
+  const double* x1 = est_vec(scr, b, in0 + 1);
+  double* y0 = est_vec(scr, b, out0);
+  double* y1 = est_vec(scr, b, out0 + 1);
+  const double* A = M + b.off;
+  const int lane = threadIdx.x & 31, wpb = blockDim.x / 32;
+  for (int64_t i = (int64_t)blockIdx.x * wpb + threadIdx.x / 32; i < b.np; i += (int64_t)gridDim.x * wpb) {
+    const double* row = A + i * b.np;
+    double a = 0, c = 0;
+    for (int64_t j = lane; j < b.np; j += 32) {
+      const double m = row[j];
+      a += m * x0[j];
+      c += m * x1[j];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0) {
+      y0[i] = a;
+      y1[i] = c;
+    }
+  }
+}
+__device__ double block_reduce(double v, double* sh, bool take_max) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] = take_max ? fmax(sh[threadIdx.x], sh[threadIdx.x + o]) : sh[threadIdx.x] + sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+// argmax of val over i < n with skip[i] == 0 and i != excl (ties to the lower index); -1 if none.
+__device__ int block_argmax(const double* val, const double* skip, int n, int excl, double* shv, int* shi) {
+  double best = -1.0;
+  int bi = -1;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (skip[i] != 0.0 || i == excl) continue;
+    const double v = val[i];
+    if (bi < 0 || v > best) {
+      best = v;
+      bi = i;
+    }
+  }
+  shv[threadIdx.x] = best;
+  shi[threadIdx.x] = bi;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      const int j = threadIdx.x + o;
+      const int ia = shi[threadIdx.x], ib = shi[j];
+      const double va = shv[threadIdx.x], vb = shv[j];
+      bool take_b = false;
+      if (ib >= 0) {
+        if (ia < 0) take_b = true;
+        else if (vb > va) take_b = true;
+        else if (vb == va && ib < ia) take_b = true;
+      }
+      if (take_b) {
+        shv[threadIdx.x] = vb;
+        shi[threadIdx.x] = ib;
+      }
+    }
+    __syncthreads();
+  }
+  const int r = shi[0];
+  __syncthreads();
+  return r;
+}
+// After Y = M0 M1 X: the estimate of round k; stop, or S = sign(Y) -> X.
+__global__ void kb_est_step1(const int* list, const BWalk* wk, double* scr, double* est, int k) {
+  const int w = list[blockIdx.x];
+  if (est[4 * w + 2] != 0.0) return;
+  const BWalk b = wk[w];
+  __shared__ double sh[256];
+  const double* Y0 = est_vec(scr, b, kEY0);
+  const double* Y1 = est_vec(scr, b, kEY1);
+  double* X0 = est_vec(scr, b, kEX0);
+  double* X1 = est_vec(scr, b, kEX1);
+  const int t = b.n > 1 ? 2 : 1;
+  const double old = est[4 * w];   // read before any thread can write it below
+  double c0 = 0, c1 = 0;
+  for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
+    c0 += fabs(Y0[i]);
+    c1 += fabs(Y1[i]);
+  }
+  c0 = block_reduce(c0, sh, false);
+  c1 = block_reduce(c1, sh, false);
+  const double e = (t == 2 && c1 > c0) ? c1 : c0;
+  if ((k >= 2 && e <= old) || k == 5) {
+    if (threadIdx.x == 0) {
+      if (!(k >= 2 && e <= old)) est[4 * w] = e;
+      est[4 * w + 2] = 1.0;
+    }
+    return;
+  }
+  for (int i = threadIdx.x; i < b.np; i += blockDim.x) {
+    X0[i] = i < b.n ? (Y0[i] != 0.0 ? (Y0[i] > 0 ? 1.0 : -1.0) : 1.0) : 0.0;
+    X1[i] = (i < b.n && t == 2) ? (Y1[i] != 0.0 ? (Y1[i] > 0 ? 1.0 : -1.0) : 1.0) : 0.0;
+  }
+  if (threadIdx.x == 0) est[4 * w] = e;
+}
+// After Z = M1 M0 S (in Y): stop, or the next two unit columns.
+__global__ void kb_est_step2(const int* list, const BWalk* wk, double* scr, double* est, int k) {
+  const int w = list[blockIdx.x];
+  if (est[4 * w + 2] != 0.0) return;
+  const BWalk b = wk[w];
+  __shared__ double shv[256];
+  __shared__ int shi[256];
+  const double* Y0 = est_vec(scr, b, kEY0);
+  const double* Y1 = est_vec(scr, b, kEY1);
+  double* X0 = est_vec(scr, b, kEX0);
+  double* X1 = est_vec(scr, b, kEX1);
+  double* H = est_vec(scr, b, kEH);
+  double* VIS = est_vec(scr, b, kEVIS);
+  const int t = b.n > 1 ? 2 : 1;
+  double hm = 0.0;
+  for (int i = threadIdx.x; i < b.np; i += blockDim.x) {
+    const double h = i < b.n ? (t == 2 ? fmax(fabs(Y0[i]), fabs(Y1[i])) : fabs(Y0[i])) : 0.0;
+    H[i] = h;
+    hm = fmax(hm, h);
+  }
+  hm = block_reduce(hm, shv, true);   // also orders the H writes before the reads below
+  const int best = (int)est[4 * w + 1];   // written (by thread 0) only after the last barrier
+  if (k >= 2 && hm <= H[best]) {
+    if (threadIdx.x == 0) est[4 * w + 2] = 1.0;
+    return;
+  }
+  const int p0 = block_argmax(H, VIS, b.n, -1, shv, shi);
+  const int p1 = t == 2 ? block_argmax(H, VIS, b.n, p0, shv, shi) : -1;
+  if (p0 < 0 || (t == 2 && p1 < 0)) {
+    if (threadIdx.x == 0) est[4 * w + 2] = 1.0;
+    return;
+  }
+  for (int i = threadIdx.x; i < b.np; i += blockDim.x) {
+    X0[i] = i == p0 ? 1.0 : 0.0;
+    X1[i] = (t == 2 && i == p1) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    VIS[p0] = 1.0;
+    if (p1 >= 0) VIS[p1] = 1.0;
+    est[4 * w + 1] = p0;
+  }
+}
+__global__ void kb_est_final(const int* list, int nlist, const double* est, double* out, int stride, int slot) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nlist) return;
+  const int w = list[i];
+  out[(int64_t)w * stride + slot] = est[4 * w];
+}
+
+// U = e^mu (I + E + cj J) on the n x n block, written to the walk's interleaved output.
+template <typename C>
+__global__ void kb_output(const double* const* Ere, const double* const* Eim, void* const* U, const int* list,
+                          const BWalk* wk, const double* om) {
+  const int w = list[blockIdx.y];
+  C* u = (C*)U[w];
+  if (!u) return;
+  const BWalk b = wk[w];
+  const double* er = Ere[w] + b.off;
+  const double* ei = Eim[w] + b.off;
+  const double* o = om + 4 * w;
+  const int64_t n2 = (int64_t)b.n * b.n;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx / b.n, j = idx - i * b.n;
+    double a = er[i * b.np + j] + o[2] + (i == j ? 1.0 : 0.0);
+    double c = ei[i * b.np + j] + o[3];
+    C v;
+    v.x = (decltype(v.x))(o[0] * a - o[1] * c);
+    v.y = (decltype(v.y))(o[0] * c + o[1] * a);
+    u[idx] = v;
+  }
+}
+
+unsigned grid_x_for(int64_t max_elems, int nlist) {
+  // enough CTAs per walk to cover the largest block with ~8 elements per thread, and enough
+  // in total to fill the GPU a few times over
+  int64_t per = (max_elems + 2047) / 2048;
+  int64_t want = std::max<int64_t>(1, (148 * 16 + nlist - 1) / std::max(1, nlist));
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(per, std::max<int64_t>(want, 1)));
+}
+
+// Al-Mohy & Higham (2009), Table 3.1 (theta_13 = 4.25 of their Algorithm 6.1).
+const double kTheta3 = 1.495585217958292e-2, kTheta5 = 2.539398330063230e-1,
+             kTheta7 = 9.504178996162932e-1, kTheta9 = 2.097847961257068e0, kTheta13 = 4.25;
+double factorial(int k) {
+  double f = 1;
+  for (int i = 2; i <= k; ++i) f *= i;
+  return f;
+}
+std::vector<double> pade_coeffs(int m) {
+  std::vector<double> b(m + 1);
+  for (int j = 0; j <= m; ++j) b[j] = factorial(2 * m - j) / (factorial(j) * factorial(m - j));
+  return b;
+}
+int pade_products(int m) { return m == 3 ? 2 : m == 5 ? 3 : m == 7 ? 4 : m == 9 ? 5 : 6; }
+
+struct DevArena {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void alloc(size_t b) {
+    release();
+    if (b == 0) return;
+    if (cudaMalloc(&p, b) != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      throw Error{FX_ERR_NOMEM, "device allocation of " + std::to_string(b) + " bytes failed"};
+    }
+    bytes = b;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  ~DevArena() { release(); }
+};
+
+// Host staging of the small device descriptors of a launch sequence, uploaded in one copy.
+struct Staging {
+  std::vector<unsigned char> buf;
+  template <typename T>
+  size_t put(const T* data, size_t count) {
+    size_t off = (buf.size() + 255) & ~(size_t)255;
+    buf.resize(off + sizeof(T) * count);
+    if (count) std::memcpy(buf.data() + off, data, sizeof(T) * count);
+    return off;
+  }
+  template <typename T>
+  size_t put(const std::vector<T>& v) {
+    return put(v.data(), v.size());
+  }
+};
+
+}  // namespace
+
+// ================================================================== batch pipeline
+class BatchPipeline {
+ public:
+  BatchPipeline(const std::vector<int64_t>& ns, int dtype) : dtype_(dtype) {
+    const int W = (int)ns.size();
+    walks_.resize(W);
+    int64_t off = 0, row = 0;
+    maxnp_ = kNb;
+    for (int w = 0; w < W; ++w) {
+      const int64_t n = ns[w];
+      if (n <= 0 || n > 32768) throw Error{FX_ERR_VALUE, "batched walk sizes must be 1..32768"};
+      const int64_t np = pad_n(n);
+      walks_[w] = BWalk{(int)n, (int)np, off, row};
+      off += np * np;
+      row += np;
+      maxnp_ = std::max<int64_t>(maxnp_, np);
+    }
+    elems_ = off;
+    rows_ = row;
+    pitch_ = maxnp_;
+    for (int a = 0; a < kArenas; ++a) arena_[a].alloc(sizeof(double) * (size_t)std::max<int64_t>(elems_, 1));
+    // int8 slice planes: A re (2 rows per walk row: the two planes of a complex left factor
+    // side by side), A im, A -im, B re; 5 slices each.
+    a_rows_ = 2 * rows_;
+    const size_t sl = (size_t)pitch_ * (size_t)(a_rows_ + 3 * rows_) * kS;
+    slices_.alloc(sl);
+    exps_.alloc(sizeof(int) * (size_t)(a_rows_ + rows_ + 64));
+    linv_.alloc(sizeof(double) * (size_t)rows_ * kNb * 2);
+    // small: rowstat (kRS per row), estimator vectors (kEstScratch per row), row sums (1 per
+    // row), per-walk records (8 + 8 + 4 + 8 + W ints)
+    small_.alloc(sizeof(double) * (size_t)(rows_ * (kRS + kEstScratch + 1) + 32 * W + 64));
+    err_.alloc(sizeof(int) * 8);
+    d_walks_.alloc(sizeof(BWalk) * W);
+    FX_CUDA(cudaMemcpy(d_walks_.p, walks_.data(), sizeof(BWalk) * W, cudaMemcpyHostToDevice));
+    ptrs_.alloc(sizeof(void*) * 4 * W);
+    sel_m_.assign(W, 13);
+    sel_s_.assign(W, 0);
+    rank1_.assign(W, 0);
+    mu_.assign(W, {0, 0});
+    nu_.assign(W, {0, 0});
+    norms_.assign(8 * W, 0.0);
+    record_phase1();
+  }
+  ~BatchPipeline() {
+    if (graph1_) cudaGraphExecDestroy(graph1_);
+    if (graph2_) cudaGraphExecDestroy(graph2_);
+  }
+
+  int count() const { return (int)walks_.size(); }
+  int64_t n_of(int w) const { return walks_[w].n; }
+  void selection(int w, int* m, int* s) const {
+    *m = sel_m_[w];
+    *s = sel_s_[w];
+  }
+  int launches() const { return launches_; }
+  double flops() const { return flops_; }
+  void set_graph(bool g) { use_graph_ = g; }
+  void set_timeout(unsigned ms) { timeout_ms_ = ms; }
+  void set_profile(bool p) { profile_ = p; }
+  // Per walk: ||Y||_1, d4, d6, d8, d10 and the shift flags of the last run.
+  void walk_stats(int w, fx_stats* st) const {
+    st->m = sel_m_[w];
+    st->s = sel_s_[w];
+    st->structured = 1;
+    st->rank1_shift = rank1_[w];
+    st->symmetric = 1;
+    st->solver = 1;
+    st->norm1 = norms_[8 * w];
+    st->d[0] = std::pow(norms_[8 * w + 1], 0.25);
+    st->d[1] = std::pow(norms_[8 * w + 2], 1.0 / 6);
+    st->d[2] = std::pow(norms_[8 * w + 3], 0.125);
+    st->d[3] = std::pow(norms_[8 * w + 4], 0.1);
+    st->d[4] = -1.0;
+    st->prod_ms = prod_ms_;
+    st->prod_ops = prod_ops_;
+    st->prod_flops = prod_flops_;
+    st->prod_launches = prod_launches_;
+  }
+  int gemm_launches() const { return gemm_launches_; }
+
+  // psi_w = expm(X_w) psi0_w and/or U_w = expm(X_w); any of dpsi0 / dpsi / dU may be null (a
+  // null table, or a null entry, skips that output for that walk).
+  void run(const void* const* dX, const void* const* dpsi0, void* const* dpsi, void* const* dU, cudaStream_t s) {
+    const int W = count();
+    stream_ = s;
+    launches_ = 0;
+    gemm_launches_ = 0;
+    prof_reset();
+    std::vector<const void*> tab(4 * W, nullptr);
+    for (int w = 0; w < W; ++w) {
+      tab[w] = dX[w];
+      tab[W + w] = dpsi0 ? dpsi0[w] : nullptr;
+      tab[2 * W + w] = dpsi ? dpsi[w] : nullptr;
+      tab[3 * W + w] = dU ? dU[w] : nullptr;
+    }
+    FX_CUDA(cudaMemcpyAsync(ptrs_.p, tab.data(), sizeof(void*) * 4 * W, cudaMemcpyHostToDevice, s));
+    FX_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int) * 8, s));
+    FX_CUDA(cudaMemsetAsync(flags(), 0, sizeof(int) * W, s));
+
+    // ---- phase 1: statistics and shifts, powers, exact norms, estimates (one host round trip)
+    run_recorded(desc1_, st1_, r1_, graph1_, use_graph_ && !profile_);
+    std::vector<double> h_wo(8 * W);
+    std::vector<int> h_flags(W);
+    FX_CUDA(cudaMemcpyAsync(h_wo.data(), walkout(), sizeof(double) * 8 * W, cudaMemcpyDeviceToHost, s));
+    FX_CUDA(cudaMemcpyAsync(h_flags.data(), flags(), sizeof(int) * W, cudaMemcpyDeviceToHost, s));
+    FX_CUDA(cudaMemcpyAsync(norms_.data(), norms(), sizeof(double) * 8 * W, cudaMemcpyDeviceToHost, s));
+    FX_CUDA(cudaStreamSynchronize(s));
+    check_err();
+    for (int w = 0; w < W; ++w) {
+      if (h_flags[w] & 4) throw Error{FX_ERR_NONFINITE, "input " + std::to_string(w) + " contains NaN or Inf"};
+      if (h_flags[w] & 3)
+        throw Error{FX_ERR_VALUE, "batched walks need generators X = i*(real symmetric); input " +
+                                      std::to_string(w) + " is not"};
+      mu_[w] = std::complex<double>(h_wo[8 * w], h_wo[8 * w + 1]);
+      nu_[w] = std::complex<double>(h_wo[8 * w + 2], h_wo[8 * w + 3]);
+      rank1_[w] = h_wo[8 * w + 4] != 0.0;
+    }
+
+    // ---- selection (m, s) per walk: Al-Mohy & Higham (2009) Alg. 6.1, normal input (l = 0)
+    flops_ = 0;
+    for (int w = 0; w < W; ++w) {
+      const double* nw = norms_.data() + 8 * w;
+      const double anorm = nw[0], d4 = std::pow(nw[1], 0.25), d6 = std::pow(nw[2], 1.0 / 6);
+      if (!std::isfinite(anorm) || !std::isfinite(d4) || !std::isfinite(d6))
+        throw Error{FX_ERR_NONFINITE, "non-finite norm in walk " + std::to_string(w)};
+      int m = 13, sq = 0;
+      if (std::max(d4, d6) < kTheta3) {
+        m = 3;
+      } else if (std::max(d4, d6) < kTheta5) {
+        m = 5;
+      } else {
+        const double d8 = std::pow(nw[3], 0.125);
+        const double eta3 = std::max(d6, d8);
+        if (eta3 < kTheta7) {
+          m = 7;
+        } else if (eta3 < kTheta9) {
+          m = 9;
+        } else {
+          const double d10 = std::pow(nw[4], 0.1);
+          const double eta5 = std::min(eta3, std::max(d8, d10));
+          sq = eta5 == 0.0 ? 0 : std::max((int)std::ceil(std::log2(eta5 / kTheta13)), 0);
+        }
+      }
+      if (force_m_ > 0) m = force_m_;
+      if (force_s_ >= 0 && m == 13) sq = force_s_;
+      if (m != 13) sq = 0;
+      sel_m_[w] = m;
+      sel_s_[w] = sq;
+      const double N3 = (double)walks_[w].n * walks_[w].n * walks_[w].n;
+      flops_ += 8.0 * N3 * (pade_products(m) + sq) + (8.0 / 3.0) * N3 + 8.0 * N3;
+    }
+
+    // ---- phase 2: Pade, solve, squarings, outputs.  The recorded launch sequence (and its
+    // CUDA graph) depends only on the sizes, (m, s), the shifts and which outputs are wanted;
+    // it is rebuilt only when one of those changed since the last run.
+    std::vector<double> key;
+    for (int w = 0; w < W; ++w) {
+      key.insert(key.end(), {(double)sel_m_[w], (double)sel_s_[w], (double)rank1_[w], mu_[w].real(),
+                             mu_[w].imag(), nu_[w].real(), nu_[w].imag(), tab[W + w] ? 1.0 : 0.0,
+                             tab[2 * W + w] ? 1.0 : 0.0, tab[3 * W + w] ? 1.0 : 0.0});
+    }
+    if (key != key2_ || profile_) {
+      st2_ = Staging();
+      r2_ = Rec();
+      if (graph2_) {
+        cudaGraphExecDestroy(graph2_);
+        graph2_ = nullptr;
+      }
+      record_rest(st2_, r2_);
+      desc2_.alloc(std::max<size_t>(st2_.buf.size(), 256));
+      FX_CUDA(cudaMemcpyAsync(desc2_.p, st2_.buf.data(), st2_.buf.size(), cudaMemcpyHostToDevice, s));
+      key2_ = profile_ ? std::vector<double>() : key;
+    }
+    run_recorded(desc2_, st2_, r2_, graph2_, use_graph_ && !profile_, false);
+    FX_CUDA(cudaStreamSynchronize(s));
+    check_err();
+    prof_collect();
+  }
+
+ private:
+  enum { kY, kA2, kA4, kA6, kT1, kT2, kW, kV, kArenas };
+  struct Rec {
+    std::vector<std::function<void()>> ops;
+    int launches = 0, gemms = 0;
+  };
+
+  int dtype_;
+  std::vector<BWalk> walks_;
+  int64_t elems_ = 0, rows_ = 0, maxnp_ = 0, pitch_ = 0, a_rows_ = 0;
+  DevArena arena_[kArenas];
+  DevArena slices_, exps_, linv_, small_, err_, d_walks_, ptrs_, desc1_, desc2_;
+  Staging st1_, st2_;
+  Rec r1_, r2_;
+  std::vector<double> key2_;
+  std::vector<int> sel_m_, sel_s_, rank1_;
+  std::vector<std::complex<double>> mu_, nu_;
+  std::vector<double> norms_;
+  cudaStream_t stream_ = nullptr;
+  unsigned timeout_ms_ = 2000;
+  bool use_graph_ = true, profile_ = false;
+  int force_m_ = -1, force_s_ = -1;
+  int launches_ = 0, gemm_launches_ = 0;
+  double flops_ = 0;
+  cudaGraphExec_t graph1_ = nullptr, graph2_ = nullptr;
+  unsigned char* desc_base_ = nullptr;
+  // product-launch timing (profile mode)
+  std::vector<cudaEvent_t> ev_pool_;
+  std::vector<std::pair<double, double>> ev_work_;
+  double prod_ms_ = 0, prod_ops_ = 0, prod_flops_ = 0;
+  int prod_launches_ = 0;
+
+ public:
+  void force(int m, int s) {
+    force_m_ = m;
+    force_s_ = s;
+  }
+
+ private:
+  double* A(int a) const { return (double*)arena_[a].p; }
+  // layout of small_
+  double* rowstat() const { return (double*)small_.p; }
+  double* est_scr() const { return rowstat() + kRS * rows_; }
+  double* rsum() const { return est_scr() + kEstScratch * rows_; }
+  double* walkout() const { return rsum() + rows_; }
+  double* norms() const { return walkout() + 8 * count(); }
+  double* estst() const { return norms() + 8 * count(); }
+  double* misc() const { return estst() + 4 * count(); }   // 8 per walk: psum, projection totals
+  int* flags() const { return (int*)(misc() + 8 * count()); }
+  const void* const* dX() const { return (const void* const*)ptrs_.p; }
+  const void* const* dP0() const { return dX() + count(); }
+  void* const* dP1() const { return (void* const*)(dX() + 2 * count()); }
+  void* const* dUo() const { return (void* const*)(dX() + 3 * count()); }
+
+  int8_t* slice_plane(int which, int q) const {
+    // which: 0 A re (a_rows_), 1 A im, 2 A -im, 3 B re (rows_ each)
+    const size_t plane_a = (size_t)pitch_ * a_rows_, plane_r = (size_t)pitch_ * rows_;
+    int8_t* base = (int8_t*)slices_.p;
+    if (which == 0) return base + q * plane_a;
+    return base + kS * plane_a + (size_t)((which - 1) * kS + q) * plane_r;
+  }
+  int* aexp() const { return (int*)exps_.p; }
+  int* bexp() const { return (int*)exps_.p + a_rows_ + 32; }
+  double* linv(int w) const { return (double*)linv_.p + (size_t)walks_[w].row0 * kNb; }
+  double* linvT(int w) const { return (double*)linv_.p + (size_t)rows_ * kNb + (size_t)walks_[w].row0 * kNb; }
+  template <typename T>
+  T* dev(size_t off) const {
+    return (T*)(desc_base_ + off);
+  }
+
+  void check_err() {
+    int h = 0;
+    FX_CUDA(cudaMemcpy(&h, err_.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h & kDevTimeout) throw Error{FX_ERR_TIMEOUT, "a device-side wait timed out"};
+    if (h & kDevSingular) throw Error{FX_ERR_SINGULAR, "Pade denominator is not positive definite"};
+  }
+
+  void prof_reset() {
+    ev_work_.clear();
+    prod_ms_ = prod_ops_ = prod_flops_ = 0;
+    prod_launches_ = 0;
+  }
+  // Events around a product launch (profile mode, eager replay only).
+  size_t prof_begin() {
+    if (!profile_) return 0;
+    const size_t i = ev_work_.size();
+    while (ev_pool_.size() < 2 * (i + 1)) {
+      cudaEvent_t e;
+      FX_CUDA(cudaEventCreate(&e));
+      ev_pool_.push_back(e);
+    }
+    FX_CUDA(cudaEventRecord(ev_pool_[2 * i], stream_));
+    return i;
+  }
+  void prof_end(size_t i, double ops, double fl) {
+    if (!profile_) return;
+    FX_CUDA(cudaEventRecord(ev_pool_[2 * i + 1], stream_));
+    ev_work_.push_back({ops, fl});
+  }
+  void prof_collect() {
+    if (!profile_) return;
+    for (size_t i = 0; i < ev_work_.size(); ++i) {
+      float t = 0;
+      FX_CUDA(cudaEventElapsedTime(&t, ev_pool_[2 * i], ev_pool_[2 * i + 1]));
+      prod_ms_ += t;
+      prod_ops_ += ev_work_[i].first;
+      prod_flops_ += ev_work_[i].second;
+    }
+    prod_launches_ = (int)ev_work_.size();
+  }
+
+  // Replay a recorded launch sequence: eagerly, or through its (cached) CUDA graph.
+  void run_recorded(DevArena& desc, Staging& st, Rec& r, cudaGraphExec_t& gexec, bool graph, bool upload = true) {
+    if (upload && desc.bytes == 0) {
+      desc.alloc(std::max<size_t>(st.buf.size(), 256));
+      FX_CUDA(cudaMemcpy(desc.p, st.buf.data(), st.buf.size(), cudaMemcpyHostToDevice));
+    }
+    desc_base_ = (unsigned char*)desc.p;
+    launches_ += r.launches;
+    gemm_launches_ += r.gemms;
+    if (!graph) {
+      for (auto& op : r.ops) op();
+      return;
+    }
+    if (!gexec) {
+      warm_attributes();
+      cudaGraph_t g = nullptr;
+      FX_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      try {
+        for (auto& op : r.ops) op();
+      } catch (...) {
+        cudaStreamEndCapture(stream_, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      FX_CUDA(cudaStreamEndCapture(stream_, &g));
+      const cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        gexec = nullptr;
+        throw Error{FX_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+      }
+    }
+    FX_CUDA(cudaGraphLaunch(gexec, stream_));
+  }
+  // Kernel attributes (dynamic shared memory) are set outside any stream capture.
+  void warm_attributes() {
+    prepare_gemm_i8_grouped(kS);
+    prepare_potrf_inv_grouped();
+  }
+
+  // Phase 1, recorded once: statistics and shifts, Y, A2 = Y^2, A4, A6, exact norms of Y, A4,
+  // A6 and the estimates of ||A4 A4||_1 and ||A4 A6||_1.
+  void record_phase1() {
+    const int W = count();
+    Staging& st = st1_;
+    Rec& r = r1_;
+    std::vector<int> all(W);
+    for (int w = 0; w < W; ++w) all[w] = w;
+    const size_t o_all = st.put(all);
+    const dim3 g_rows(grid_x_for(maxnp_ * 32, W), W), g_el(grid_x_for(maxnp_ * maxnp_, W), W);
+    const int dt = dtype_;
+    r.ops.push_back([=]() {
+      const BWalk* wk = (const BWalk*)d_walks_.p;
+      if (dt == FX_C64)
+        kb_stats<float2><<<g_rows, 256, 0, stream_>>>(dX(), dev<int>(o_all), wk, rowstat(), flags());
+      else
+        kb_stats<double2><<<g_rows, 256, 0, stream_>>>(dX(), dev<int>(o_all), wk, rowstat(), flags());
+      FX_LAUNCH_CHECK();
+      kb_walk_reduce<<<W, 256, 0, stream_>>>(dev<int>(o_all), wk, rowstat(), walkout());
+      FX_LAUNCH_CHECK();
+      if (dt == FX_C64)
+        kb_load_imag<float2><<<g_el, 256, 0, stream_>>>(dX(), dev<int>(o_all), wk, walkout(), A(kY));
+      else
+        kb_load_imag<double2><<<g_el, 256, 0, stream_>>>(dX(), dev<int>(o_all), wk, walkout(), A(kY));
+      FX_LAUNCH_CHECK();
+    });
+    r.launches += 3;
+    product(st, r, all, kY, kY, -1.0, -1, 0.0, 0.0, kA2, true);
+    product(st, r, all, kA2, kA2, 1.0, -1, 0.0, 0.0, kA4, true);
+    product(st, r, all, kA4, kA2, 1.0, -1, 0.0, 0.0, kA6, true);
+    const int arenas[3] = {kY, kA4, kA6};
+    r.ops.push_back([=]() {
+      const BWalk* wk = (const BWalk*)d_walks_.p;
+      for (int k = 0; k < 3; ++k) {
+        kb_abs_rowsums<<<g_rows, 256, 0, stream_>>>(A(arenas[k]), dev<int>(o_all), wk, rsum());
+        FX_LAUNCH_CHECK();
+        kb_walk_vec_reduce<<<W, 256, 0, stream_>>>(rsum(), dev<int>(o_all), wk, 1, 0, norms(), 8, k);
+        FX_LAUNCH_CHECK();
+      }
+    });
+    r.launches += 6;
+    estimate(st, r, all, kA4, kA4, 3);
+    estimate(st, r, all, kA4, kA6, 4);
+  }
+
+  // Block 1-norm estimate of ||M0 M1||_1 for the listed walks into norms()[8 w + slot].
+  void estimate(Staging& st, Rec& r, const std::vector<int>& list, int m0, int m1, int slot) {
+    const size_t o_l = st.put(list);
+    const int nl = (int)list.size();
+    const dim3 g_rows(grid_x_for(maxnp_ * 32, nl), nl);
+    r.ops.push_back([=]() {
+      const BWalk* wk = (const BWalk*)d_walks_.p;
+      const int* l = dev<int>(o_l);
+      kb_est_init<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), estst());
+      FX_LAUNCH_CHECK();
+      for (int k = 1; k <= 5; ++k) {
+        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m1), l, wk, est_scr(), estst(), kEX0, kET0);
+        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m0), l, wk, est_scr(), estst(), kET0, kEY0);
+        kb_est_step1<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), estst(), k);
+        FX_LAUNCH_CHECK();
+        if (k == 5) break;
+        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m0), l, wk, est_scr(), estst(), kEX0, kET0);
+        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m1), l, wk, est_scr(), estst(), kET0, kEY0);
+        kb_est_step2<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), estst(), k);
+        FX_LAUNCH_CHECK();
+      }
+      kb_est_final<<<(nl + 255) / 256, 256, 0, stream_>>>(l, nl, estst(), norms(), 8, slot);
+      FX_LAUNCH_CHECK();
+    });
+    r.launches += 1 + 5 * 3 + 4 * 3 + 1;
+  }
+
+  // ---- recorded grouped operations --------------------------------------------------
+  // Real multiply-adds x 2 that the listed tiles compute (tile-level: 128 x BN x 64 per K step
+  // and term); the int8 MMA operations issued are S(S+1)/2 times that.
+  static double tile_ops(const std::vector<GTile>& tiles, int nterms) {
+    double steps = 0;
+    for (const GTile& t : tiles) steps += t.kb1 - t.kb0;
+    return steps * 2.0 * 128.0 * i8_tile_bn(kS) * 64.0 * nterms;
+  }
+  // Real product D_w = alpha_w A_w B_w + beta_w C_w + gamma_w I on np x np blocks of the listed
+  // walks (arenas; B symmetric so Bt = B); c_arena < 0: no C.
+  void product(Staging& st, Rec& r, const std::vector<int>& list, int a, int b, double alpha, int c_arena,
+               double beta, double gamma, int d_arena, bool sym, const std::vector<double>* alpha_w = nullptr,
+               const std::vector<double>* gamma_w = nullptr) {
+    std::vector<GSlab> sa, sb;
+    std::vector<GProblem> pr;
+    const bool same = a == b;
+    for (int w : list) {
+      const BWalk& bw = walks_[w];
+      sa.push_back(GSlab{A(a) + bw.off, nullptr, bw.np, bw.np, bw.np, (int)bw.row0, 0});
+      if (!same) sb.push_back(GSlab{A(b) + bw.off, nullptr, bw.np, bw.np, bw.np, (int)bw.row0, 0});
+      GProblem p{};
+      p.a_row0 = p.b_row0 = (int)bw.row0;
+      p.M = p.N = p.K = bw.np;
+      p.sym = sym ? 1 : 0;
+      p.alpha = alpha_w ? (*alpha_w)[w] : alpha;
+      p.beta = c_arena >= 0 ? beta : 0.0;
+      p.gamma = gamma_w ? (*gamma_w)[w] : gamma;
+      p.C = c_arena >= 0 ? A(c_arena) + bw.off : nullptr;
+      p.ldc = bw.np;
+      p.D = A(d_arena) + bw.off;
+      p.ldd = bw.np;
+      pr.push_back(p);
+    }
+    grouped(st, r, sa, same ? nullptr : &sb, pr, same, 0);
+  }
+
+  // Generic grouped product over explicit slabs and problems (one real term; A slabs into
+  // the A re planes, B slabs into the B re planes, or B = A when `same`).  tri: 0 none;
+  // 1: Bt rows are lower-triangular rows (Bt[c][k] = 0 for k > c); 2: Bt[c][k] = 0 for k < c;
+  // 3: A[r][k] = 0 for k > r.
+  void grouped(Staging& st, Rec& r, const std::vector<GSlab>& sa, const std::vector<GSlab>* sb,
+               const std::vector<GProblem>& pr, bool same, int tri) {
+    if (pr.empty()) return;
+    const int bn = i8_tile_bn(kS);
+    std::vector<GTile> tiles;
+    for (int i = 0; i < (int)pr.size(); ++i) {
+      const GProblem& p = pr[i];
+      const int tm = (p.M + 127) / 128, tn = (p.N + bn - 1) / bn, kbs = p.K / 64;
+      for (int mb = 0; mb < tm; ++mb)
+        for (int nb = 0; nb < tn; ++nb) {
+          if (p.sym && !((long long)nb * bn + bn - 1 >= (long long)mb * 128)) continue;
+          int kb0 = 0, kb1 = kbs;
+          if (tri == 1) kb1 = std::min(kbs, (nb * bn + bn + 63) / 64);
+          if (tri == 2) kb0 = std::min(kbs, (nb * bn) / 64);
+          if (tri == 3) kb1 = std::min(kbs, (mb * 128 + 128 + 63) / 64);
+          tiles.push_back(GTile{i, mb, nb, kb0, kb1, 0});
+        }
+    }
+    // Largest K ranges first: the persistent CTAs then finish close together.
+    std::stable_sort(tiles.begin(), tiles.end(),
+                     [](const GTile& x, const GTile& y) { return (x.kb1 - x.kb0) > (y.kb1 - y.kb0); });
+    std::vector<GSlab> a_sorted = sa, b_sorted = sb ? *sb : std::vector<GSlab>();
+    auto by_row = [](const GSlab& x, const GSlab& y) { return x.row0 < y.row0; };
+    std::sort(a_sorted.begin(), a_sorted.end(), by_row);
+    std::sort(b_sorted.begin(), b_sorted.end(), by_row);
+    const size_t o_sa = st.put(a_sorted), o_sb = st.put(b_sorted), o_pr = st.put(pr), o_t = st.put(tiles);
+    const int nsa = (int)a_sorted.size(), nsb = (int)b_sorted.size(), nt = (int)tiles.size();
+    const double ops = tile_ops(tiles, 1);
+    r.launches += same ? 2 : 3;
+    r.gemms += 1;
+    r.ops.push_back([=]() {
+      I8Slices outa{}, outb{};
+      for (int q = 0; q < kS; ++q) {
+        outa.re[q] = slice_plane(0, q);
+        outb.re[q] = slice_plane(3, q);
+      }
+      outa.exp = aexp();
+      outb.exp = bexp();
+      outa.ld = outb.ld = pitch_;
+      launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, a_rows_, outa, false, stream_);
+      I8Term t{};
+      for (int q = 0; q < kS; ++q) t.a[q] = outa.re[q];
+      if (!same) {
+        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sb), nsb, rows_, outb, false, stream_);
+        for (int q = 0; q < kS; ++q) t.b[q] = outb.re[q];
+      } else {
+        for (int q = 0; q < kS; ++q) t.b[q] = outa.re[q];
+      }
+      const size_t pi = prof_begin();
+      launch_gemm_i8_grouped<double>(kS, &t, 1, pitch_, a_rows_, same ? a_rows_ : rows_, aexp(),
+                                     same ? aexp() : bexp(), dev<GProblem>(o_pr), dev<GTile>(o_t), nt,
+                                     (int*)err_.p, timeout_ms_, stream_);
+      prof_end(pi, ops * kS * (kS + 1) / 2, ops);
+    });
+  }
+
+  void combo(Staging& st, Rec& r, const std::vector<int>& list, int d_arena, const int m_arena[4],
+             const std::vector<std::array<double, 5>>& coef) {
+    if (list.empty()) return;
+    std::vector<double> c(5 * count(), 0.0);
+    for (int w : list)
+      for (int k = 0; k < 5; ++k) c[5 * w + k] = coef[w][k];
+    const size_t o_l = st.put(list), o_c = st.put(c);
+    Planes4 M{};
+    for (int k = 0; k < 4; ++k) M.m[k] = m_arena[k] >= 0 ? A(m_arena[k]) : nullptr;
+    double* D = A(d_arena);
+    const int nl = (int)list.size();
+    int64_t mx = 0;
+    for (int w : list) mx = std::max<int64_t>(mx, (int64_t)walks_[w].np * walks_[w].np);
+    const dim3 g(grid_x_for(mx, nl), nl);
+    r.launches += 1;
+    r.ops.push_back([=]() {
+      kb_combo<<<g, 256, 0, stream_>>>(D, M, dev<int>(o_l), (const BWalk*)d_walks_.p, dev<double>(o_c));
+      FX_LAUNCH_CHECK();
+    });
+  }
+
+  void transpose(Staging& st, Rec& r, const std::vector<int>& list, int in, int out) {
+    if (list.empty()) return;
+    const size_t o_l = st.put(list);
+    const int nl = (int)list.size();
+    const double* src = A(in);
+    double* dst = A(out);
+    const unsigned gx = (unsigned)std::min(1024, std::max(8, 148 * 8 / nl));
+    r.launches += 1;
+    r.ops.push_back([=]() {
+      kb_transpose<<<dim3(gx, 1, nl), dim3(32, 8), 0, stream_>>>(src, dst, dev<int>(o_l), (const BWalk*)d_walks_.p, 0);
+      FX_LAUNCH_CHECK();
+    });
+  }
+
+  void symmetrize(Staging& st, Rec& r, const std::vector<int>& list, int a) {
+    if (list.empty()) return;
+    const size_t o_l = st.put(list);
+    const int nl = (int)list.size();
+    double* p = A(a);
+    const unsigned gx = (unsigned)std::min(1024, std::max(8, 148 * 8 / nl));
+    r.launches += 1;
+    r.ops.push_back([=]() {
+      kb_symmetrize<<<dim3(gx, 1, nl), dim3(32, 8), 0, stream_>>>(p, dev<int>(o_l), (const BWalk*)d_walks_.p);
+      FX_LAUNCH_CHECK();
+    });
+  }
+
+  // Exact projection E 1 = 0 = 1^T E of the symmetric iterates of rank-one-shifted walks.
+  void project(Staging& st, Rec& r, const std::vector<int>& list, int a) {
+    if (list.empty()) return;
+    const size_t o_l = st.put(list);
+    const int nl = (int)list.size();
+    double* p = A(a);
+    double* rs = rsum();
+    double* tot = misc();   // W doubles
+    int64_t mx = 0;
+    for (int w : list) mx = std::max<int64_t>(mx, (int64_t)walks_[w].np * walks_[w].np);
+    const dim3 g_el(grid_x_for(mx, nl), nl), g_rows(grid_x_for(maxnp_ * 32, nl), nl);
+    r.ops.push_back([=]() {
+      const BWalk* wk = (const BWalk*)d_walks_.p;
+      kb_rowsums<<<g_rows, 256, 0, stream_>>>(p, dev<int>(o_l), wk, rs);
+      FX_LAUNCH_CHECK();
+      kb_walk_vec_reduce<<<nl, 256, 0, stream_>>>(rs, dev<int>(o_l), wk, 0, 1, tot, 1, 0);
+      FX_LAUNCH_CHECK();
+      kb_apply_proj<<<g_el, 256, 0, stream_>>>(p, dev<int>(o_l), wk, rs, tot);
+      FX_LAUNCH_CHECK();
+    });
+    r.launches += 3;
+  }
+
+  // Everything after the selection.
+  void record_rest(Staging& st, Rec& r) {
+    const int W = count();
+    std::vector<int> all, m13, m9, mlt13, rank1;
+    for (int w = 0; w < W; ++w) {
+      all.push_back(w);
+      if (sel_m_[w] == 13) m13.push_back(w);
+      else mlt13.push_back(w);
+      if (sel_m_[w] == 9) m9.push_back(w);
+      if (rank1_[w]) rank1.push_back(w);
+    }
+    // ---- Pade numerator / denominator (powers scaled by 2^-s folded into the coefficients)
+    std::vector<std::array<double, 5>> cf(W), cg(W);
+    std::vector<double> al(W, 1.0), ga(W, 0.0);
+    auto cs = [&](int w, int p) { return std::ldexp(1.0, -p * sel_s_[w]); };
+    // m = 9: A8 = A4 A4 -> T2
+    product(st, r, m9, kA4, kA4, 1.0, -1, 0.0, 0.0, kT2, true);
+    // m = 13: T1 = b13 A6 + b11 A4 + b9 A2 (scaled), T2 = A6 T1 (scaled)
+    for (int w : m13) {
+      const auto b = pade_coeffs(13);
+      cf[w] = {b[13] * cs(w, 6), b[11] * cs(w, 4), b[9] * cs(w, 2), 0.0, 0.0};
+      al[w] = cs(w, 6);
+    }
+    const int m_642[4] = {kA6, kA4, kA2, -1};
+    combo(st, r, m13, kT1, m_642, cf);
+    product(st, r, m13, kA6, kT1, 1.0, -1, 0.0, 0.0, kT2, true, &al);
+    // odd part: T1 = [T2] + b7 A6 + b5 A4 + b3 A2 + b1 I  (T2 = W1 for m = 13, A8 for m = 9)
+    const int m_t2642[4] = {kT2, kA6, kA4, kA2};
+    for (int w = 0; w < W; ++w) {
+      const int m = sel_m_[w];
+      const auto b = pade_coeffs(m);
+      if (m == 13) cf[w] = {1.0, b[7] * cs(w, 6), b[5] * cs(w, 4), b[3] * cs(w, 2), b[1]};
+      else if (m == 9) cf[w] = {b[9], b[7], b[5], b[3], b[1]};
+      else if (m == 7) cf[w] = {0.0, b[7], b[5], b[3], b[1]};
+      else if (m == 5) cf[w] = {0.0, 0.0, b[5], b[3], b[1]};
+      else cf[w] = {0.0, 0.0, 0.0, b[3], b[1]};
+      al[w] = cs(w, 1);
+    }
+    combo(st, r, all, kT1, m_t2642, cf);
+    // U = i W with W = c Yim T1
+    product(st, r, all, kY, kT1, 1.0, -1, 0.0, 0.0, kW, true, &al);
+    // even part.  m = 13: T1 = b12 A6 + b10 A4 + b8 A2, T2 = b6 A6 + b4 A4 + b2 A2,
+    // V = A6 T1 + T2 + b0 I.  m < 13: V = [b8 A8] + b6 A6 + b4 A4 + b2 A2 + b0 I.
+    for (int w : m13) {
+      const auto b = pade_coeffs(13);
+      cf[w] = {b[12] * cs(w, 6), b[10] * cs(w, 4), b[8] * cs(w, 2), 0.0, 0.0};
+      cg[w] = {b[6] * cs(w, 6), b[4] * cs(w, 4), b[2] * cs(w, 2), 0.0, 0.0};
+      al[w] = cs(w, 6);
+      ga[w] = b[0];
+    }
+    combo(st, r, m13, kT1, m_642, cf);
+    combo(st, r, m13, kT2, m_642, cg);
+    for (int w : mlt13) {
+      const int m = sel_m_[w];
+      const auto b = pade_coeffs(m);
+      if (m == 9) cf[w] = {b[8], b[6], b[4], b[2], b[0]};
+      else if (m == 7) cf[w] = {0.0, b[6], b[4], b[2], b[0]};
+      else if (m == 5) cf[w] = {0.0, 0.0, b[4], b[2], b[0]};
+      else cf[w] = {0.0, 0.0, 0.0, b[2], b[0]};
+    }
+    combo(st, r, mlt13, kV, m_t2642, cf);
+    product(st, r, m13, kA6, kT1, 1.0, kT2, 1.0, 0.0, kV, true, &al, &ga);
+
+    // ---- solve: G = V^2 + W^2 = L L^T, P2 = (V + iW)^2, R = G^-1 P2
+    product(st, r, all, kV, kV, 1.0, -1, 0.0, 0.0, kT1, true);    // VV
+    product(st, r, all, kW, kW, 1.0, -1, 0.0, 0.0, kT2, true);    // WW
+    product(st, r, all, kV, kW, 1.0, -1, 0.0, 0.0, kA2, true);    // VW
+    const int m_12[4] = {kT1, kT2, -1, -1};
+    const int m_a2[4] = {kA2, -1, -1, -1};
+    for (int w = 0; w < W; ++w) cf[w] = {1.0, 1.0, 0.0, 0.0, 0.0};
+    combo(st, r, all, kA4, m_12, cf);                             // G -> A4
+    for (int w = 0; w < W; ++w) cf[w] = {1.0, -1.0, 0.0, 0.0, 0.0};
+    combo(st, r, all, kA6, m_12, cf);                             // P2 re -> A6
+    for (int w = 0; w < W; ++w) cf[w] = {2.0, 0.0, 0.0, 0.0, 0.0};
+    combo(st, r, all, kY, m_a2, cf);                              // P2 im -> Y
+    cholesky(st, r, kA4);
+    transpose(st, r, all, kA4, kT1);                              // L^T -> T1
+    inverse(st, r, kA4, kT1, kT2, kA2);                           // X = L^-1 -> T2 (scratch A2)
+    transpose(st, r, all, kT2, kW);                               // X^T -> W
+    // Z = P2 X^T (re -> V, im -> T1); R^T = Z X (re -> A4, im -> A2)
+    complex_by_real(st, r, all, kA6, kY, kT2, kV, kT1, 1);
+    complex_by_real(st, r, all, kV, kT1, kW, kA4, kA2, 2);
+    symmetrize(st, r, all, kA4);
+    symmetrize(st, r, all, kA2);
+
+    // ---- squarings in I + E form: E = R - I, E <- 2E + E^2
+    for (int w = 0; w < W; ++w) cf[w] = {1.0, 0.0, 0.0, 0.0, -1.0};
+    const int m_a4[4] = {kA4, -1, -1, -1};
+    combo(st, r, all, kA4, m_a4, cf);
+    std::vector<int> er(W, kA4), ei(W, kA2), tr(W, kT1), ti(W, kT2);
+    project_pair(st, r, rank1, er, ei);
+    int smax = 0;
+    for (int w = 0; w < W; ++w) smax = std::max(smax, sel_s_[w]);
+    for (int k = 0; k < smax; ++k) {
+      std::vector<int> act;
+      for (int w = 0; w < W; ++w)
+        if (sel_s_[w] > k) act.push_back(w);
+      square(st, r, act, er, ei, tr, ti);
+      for (int w : act) {
+        std::swap(er[w], tr[w]);
+        std::swap(ei[w], ti[w]);
+      }
+      std::vector<int> pj;
+      for (int w : act)
+        if (rank1_[w]) pj.push_back(w);
+      project_pair(st, r, pj, er, ei);
+    }
+
+    // ---- outputs: psi = e^mu (E psi0 + psi0 + cj (1^T psi0) 1) and U = e^mu (I + E + cj J)
+    std::vector<const double*> pre(W), pim(W);
+    std::vector<double> om(4 * W);
+    for (int w = 0; w < W; ++w) {
+      pre[w] = A(er[w]);
+      pim[w] = A(ei[w]);
+      const std::complex<double> e = std::exp(mu_[w]);
+      om[4 * w] = e.real();
+      om[4 * w + 1] = e.imag();
+      if (rank1_[w]) {
+        const std::complex<double> cj = (std::exp(nu_[w]) - 1.0) / (double)walks_[w].n;
+        om[4 * w + 2] = cj.real();
+        om[4 * w + 3] = cj.imag();
+      }
+    }
+    const size_t o_pre = st.put(pre), o_pim = st.put(pim), o_om = st.put(om), o_all = st.put(all);
+    double* psum = misc() + 2 * W;
+    const dim3 g_rows(grid_x_for(maxnp_ * 32, W), W);
+    const dim3 g_el(grid_x_for(maxnp_ * maxnp_, W), W);
+    const int dt = dtype_;
+    r.launches += 3;
+    r.ops.push_back([=]() {
+      const BWalk* wk = (const BWalk*)d_walks_.p;
+      const int* l = dev<int>(o_all);
+      const double* const* er_ = dev<const double*>(o_pre);
+      const double* const* ei_ = dev<const double*>(o_pim);
+      if (dt == FX_C64) {
+        kb_psi_sum<float2><<<W, 32, 0, stream_>>>(dP0(), l, wk, psum);
+        FX_LAUNCH_CHECK();
+        kb_apply<float2><<<g_rows, 256, 0, stream_>>>(er_, ei_, dP0(), dP1(), l, wk, dev<double>(o_om), psum);
+        FX_LAUNCH_CHECK();
+        kb_output<float2><<<g_el, 256, 0, stream_>>>(er_, ei_, dUo(), l, wk, dev<double>(o_om));
+      } else {
+        kb_psi_sum<double2><<<W, 32, 0, stream_>>>(dP0(), l, wk, psum);
+        FX_LAUNCH_CHECK();
+        kb_apply<double2><<<g_rows, 256, 0, stream_>>>(er_, ei_, dP0(), dP1(), l, wk, dev<double>(o_om), psum);
+        FX_LAUNCH_CHECK();
+        kb_output<double2><<<g_el, 256, 0, stream_>>>(er_, ei_, dUo(), l, wk, dev<double>(o_om));
+      }
+      FX_LAUNCH_CHECK();
+    });
+  }
+
+  void project_pair(Staging& st, Rec& r, const std::vector<int>& list, const std::vector<int>& er,
+                    const std::vector<int>& ei) {
+    // group the walks by the arena their iterate lives in
+    for (int pa : {kA4, kT1}) {
+      std::vector<int> l1;
+      for (int w : list)
+        if (er[w] == pa) l1.push_back(w);
+      project(st, r, l1, pa);
+    }
+    for (int pa : {kA2, kT2}) {
+      std::vector<int> l2;
+      for (int w : list)
+        if (ei[w] == pa) l2.push_back(w);
+      project(st, r, l2, pa);
+    }
+  }
+
+  // One squaring E <- 2E + E^2 of the listed walks (E symmetric complex, planes er/ei; result in
+  // tr/ti).  Walks whose iterates sit in different arena pairs go in separate launches.
+  void square(Staging& st, Rec& r, const std::vector<int>& act, const std::vector<int>& er,
+              const std::vector<int>& ei, const std::vector<int>& tr, const std::vector<int>& ti) {
+    for (int pa : {kA4, kT1}) {
+      std::vector<int> l;
+      for (int w : act)
+        if (er[w] == pa) l.push_back(w);
+      if (l.empty()) continue;
+      const int re = er[l[0]], im = ei[l[0]], ore = tr[l[0]], oim = ti[l[0]];
+      std::vector<GSlab> sa;
+      std::vector<GProblem> prr, pri;
+      for (int w : l) {
+        const BWalk& b = walks_[w];
+        sa.push_back(GSlab{A(re) + b.off, A(im) + b.off, b.np, b.np, b.np, (int)b.row0, 0});
+        GProblem p{};
+        p.a_row0 = p.b_row0 = (int)b.row0;
+        p.M = p.N = p.K = b.np;
+        p.sym = 1;
+        p.alpha = 1.0;
+        p.beta = 2.0;
+        p.ldc = p.ldd = b.np;
+        p.C = A(re) + b.off;
+        p.D = A(ore) + b.off;
+        prr.push_back(p);
+        p.C = A(im) + b.off;
+        p.D = A(oim) + b.off;
+        pri.push_back(p);
+      }
+      const int bn = i8_tile_bn(kS);
+      std::vector<GTile> tiles;
+      for (int i = 0; i < (int)prr.size(); ++i) {
+        const int tm = (prr[i].M + 127) / 128, tn = (prr[i].N + bn - 1) / bn;
+        for (int mb = 0; mb < tm; ++mb)
+          for (int nb = 0; nb < tn; ++nb)
+            if ((long long)nb * bn + bn - 1 >= (long long)mb * 128) tiles.push_back(GTile{i, mb, nb, 0, prr[i].K / 64, 0});
+      }
+      std::stable_sort(tiles.begin(), tiles.end(),
+                       [](const GTile& x, const GTile& y) { return (x.kb1 - x.kb0) > (y.kb1 - y.kb0); });
+      std::sort(sa.begin(), sa.end(), [](const GSlab& x, const GSlab& y) { return x.row0 < y.row0; });
+      const size_t o_sa = st.put(sa), o_r = st.put(prr), o_i = st.put(pri), o_t = st.put(tiles);
+      const int nsa = (int)sa.size(), nt = (int)tiles.size();
+      const double ops = tile_ops(tiles, 2);
+      r.launches += 3;
+      r.gemms += 2;
+      r.ops.push_back([=]() {
+        I8Slices out{};
+        for (int q = 0; q < kS; ++q) {
+          out.re[q] = slice_plane(0, q);
+          out.im[q] = slice_plane(1, q);
+          out.neg_im[q] = slice_plane(2, q);
+        }
+        out.exp = aexp();
+        out.ld = pitch_;
+        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, rows_, out, true, stream_);
+        I8Term t[2];
+        // real: Re Re + Im (-Im)
+        for (int q = 0; q < kS; ++q) {
+          t[0].a[q] = out.re[q];
+          t[0].b[q] = out.re[q];
+          t[1].a[q] = out.im[q];
+          t[1].b[q] = out.neg_im[q];
+        }
+        size_t pi = prof_begin();
+        launch_gemm_i8_grouped<double>(kS, t, 2, pitch_, rows_, rows_, aexp(), aexp(), dev<GProblem>(o_r),
+                                       dev<GTile>(o_t), nt, (int*)err_.p, timeout_ms_, stream_);
+        prof_end(pi, ops * kS * (kS + 1) / 2, ops);
+        // imaginary: Re Im + Im Re
+        for (int q = 0; q < kS; ++q) {
+          t[0].a[q] = out.re[q];
+          t[0].b[q] = out.im[q];
+          t[1].a[q] = out.im[q];
+          t[1].b[q] = out.re[q];
+        }
+        pi = prof_begin();
+        launch_gemm_i8_grouped<double>(kS, t, 2, pitch_, rows_, rows_, aexp(), aexp(), dev<GProblem>(o_i),
+                                       dev<GTile>(o_t), nt, (int*)err_.p, timeout_ms_, stream_);
+        prof_end(pi, ops * kS * (kS + 1) / 2, ops);
+      });
+    }
+  }
+
+  // D_re / D_im = (P_re, P_im) B^T per walk (two problems per walk, A rows side by side).
+  void complex_by_real(Staging& st, Rec& r, const std::vector<int>& list, int pre, int pim, int bt, int dre,
+                       int dim, int tri) {
+    std::vector<GSlab> sa, sb;
+    std::vector<GProblem> pr;
+    for (int w : list) {
+      const BWalk& b = walks_[w];
+      sa.push_back(GSlab{A(pre) + b.off, nullptr, b.np, b.np, b.np, (int)(2 * b.row0), 0});
+      sa.push_back(GSlab{A(pim) + b.off, nullptr, b.np, b.np, b.np, (int)(2 * b.row0 + b.np), 0});
+      sb.push_back(GSlab{A(bt) + b.off, nullptr, b.np, b.np, b.np, (int)b.row0, 0});
+      GProblem p{};
+      p.b_row0 = (int)b.row0;
+      p.M = p.N = p.K = b.np;
+      p.alpha = 1.0;
+      p.ldc = p.ldd = b.np;
+      p.a_row0 = (int)(2 * b.row0);
+      p.D = A(dre) + b.off;
+      pr.push_back(p);
+      p.a_row0 = (int)(2 * b.row0 + b.np);
+      p.D = A(dim) + b.off;
+      pr.push_back(p);
+    }
+    grouped(st, r, sa, &sb, pr, false, tri);
+  }
+
+  // Blocked right-looking Cholesky of the listed walks' G (in arena g), 128-wide steps.
+  void cholesky(Staging& st, Rec& r, int g) {
+    const int W = count();
+    int jmax = 0;
+    for (int w = 0; w < W; ++w) jmax = std::max(jmax, walks_[w].np / kNb);
+    for (int j = 0; j < jmax; ++j) {
+      std::vector<GChol> jobs;
+      std::vector<GSlab> sa21, sb_l;
+      std::vector<GProblem> p21, p22;
+      for (int w = 0; w < W; ++w) {
+        const BWalk& b = walks_[w];
+        if (b.np <= j * kNb) continue;
+        double* G = A(g) + b.off;
+        const int64_t k0 = (int64_t)j * kNb;
+        jobs.push_back(GChol{G, b.np, k0, kNb, 0, linv(w) + k0 * kNb, linvT(w) + k0 * kNb});
+        const int rest = b.np - (j + 1) * kNb;
+        if (rest <= 0) continue;
+        double* G21 = G + (k0 + kNb) * b.np + k0;
+        // L21 = G21 Linv^T: A = G21 (rest x 128), Bt = Linv (128 x 128)
+        sa21.push_back(GSlab{G21, nullptr, b.np, rest, kNb, (int)b.row0, 0});
+        sb_l.push_back(GSlab{linv(w) + k0 * kNb, nullptr, kNb, kNb, kNb, (int)b.row0, 0});
+        GProblem p{};
+        p.a_row0 = p.b_row0 = (int)b.row0;
+        p.M = rest;
+        p.N = kNb;
+        p.K = kNb;
+        p.alpha = 1.0;
+        p.D = G21;
+        p.ldd = b.np;
+        p21.push_back(p);
+        // G22 -= L21 L21^T (symmetric)
+        GProblem q{};
+        q.a_row0 = q.b_row0 = (int)b.row0;
+        q.M = q.N = rest;
+        q.K = kNb;
+        q.sym = 1;
+        q.alpha = -1.0;
+        q.beta = 1.0;
+        q.C = G21 + kNb;
+        q.ldc = b.np;
+        q.D = G21 + kNb;
+        q.ldd = b.np;
+        p22.push_back(q);
+      }
+      const size_t o_j = st.put(jobs);
+      const int nj = (int)jobs.size();
+      r.launches += 1;
+      r.ops.push_back([=]() { launch_potrf_inv_grouped<double>(dev<GChol>(o_j), nj, (int*)err_.p, stream_); });
+      if (p21.empty()) continue;
+      grouped(st, r, sa21, &sb_l, p21, false, 0);
+      // the updated G21 (= L21) is both factors of the trailing update
+      std::vector<GSlab> sl;
+      for (size_t i = 0; i < p21.size(); ++i) sl.push_back(GSlab{p21[i].D, nullptr, p21[i].ldd, p21[i].M, kNb, p21[i].a_row0, 0});
+      grouped(st, r, sl, nullptr, p22, true, 0);
+    }
+  }
+
+  // X = L^-1 (arena x) from L (arena l, lower), L^T (arena lt) and the diagonal-block inverses;
+  // blocked, backward over block columns: X[>j, j] = -(X[>j, >j] L[>j, j]) Linv_jj.
+  void inverse(Staging& st, Rec& r, int l, int lt, int x, int scratch) {
+    const int W = count();
+    (void)l;
+    std::vector<int64_t> loff(W);
+    std::vector<int> all(W);
+    for (int w = 0; w < W; ++w) {
+      loff[w] = (int64_t)walks_[w].row0 * kNb;
+      all[w] = w;
+    }
+    const size_t o_lo = st.put(loff), o_all = st.put(all);
+    double* X = A(x);
+    const double* Li = (const double*)linv_.p;
+    const dim3 g(grid_x_for(maxnp_ * maxnp_, W), W);
+    r.launches += 1;
+    r.ops.push_back([=]() {
+      kb_init_inverse<<<g, 256, 0, stream_>>>(X, Li, dev<int>(o_all), (const BWalk*)d_walks_.p, dev<int64_t>(o_lo));
+      FX_LAUNCH_CHECK();
+    });
+    int jmax = 0;
+    for (int w = 0; w < W; ++w) jmax = std::max(jmax, walks_[w].np / kNb);
+    for (int j = jmax - 2; j >= 0; --j) {
+      std::vector<GSlab> sa, sb, sa2, sb2;
+      std::vector<GProblem> pa, pb;
+      for (int w = 0; w < W; ++w) {
+        const BWalk& b = walks_[w];
+        const int rest = b.np - (j + 1) * kNb;
+        if (rest <= 0) continue;
+        const int64_t k1 = (int64_t)(j + 1) * kNb, k0 = (int64_t)j * kNb;
+        double* T = A(scratch) + b.off;   // rest x 128, ld 128
+        // T = X[>j, >j] L[>j, j]: A = X rows k1.., cols k1.. (lower triangular), Bt = L^T rows j-block, cols k1..
+        sa.push_back(GSlab{X + b.off + k1 * b.np + k1, nullptr, b.np, rest, rest, (int)b.row0, 0});
+        sb.push_back(GSlab{A(lt) + b.off + k0 * b.np + k1, nullptr, b.np, kNb, rest, (int)b.row0, 0});
+        GProblem p{};
+        p.a_row0 = p.b_row0 = (int)b.row0;
+        p.M = rest;
+        p.N = kNb;
+        p.K = rest;
+        p.alpha = 1.0;
+        p.D = T;
+        p.ldd = kNb;
+        pa.push_back(p);
+        // X[>j, j] = -T Linv_jj: A = T, Bt = Linv_jj^T
+        sa2.push_back(GSlab{T, nullptr, kNb, rest, kNb, (int)b.row0, 0});
+        sb2.push_back(GSlab{linvT(w) + k0 * kNb, nullptr, kNb, kNb, kNb, (int)b.row0, 0});
+        GProblem q{};
+        q.a_row0 = q.b_row0 = (int)b.row0;
+        q.M = rest;
+        q.N = kNb;
+        q.K = kNb;
+        q.alpha = -1.0;
+        q.D = X + b.off + k1 * b.np + k0;
+        q.ldd = b.np;
+        pb.push_back(q);
+      }
+      grouped(st, r, sa, &sb, pa, false, 3);
+      grouped(st, r, sa2, &sb2, pb, false, 0);
+    }
+  }
+};
+
+// ---- interface used by the per-walk engine (fx_engine.cu) for structured walks
+BatchPipeline* batch_pipeline_create(int64_t n, int dtype) { return new BatchPipeline({n}, dtype); }
+void batch_pipeline_destroy(BatchPipeline* p) { delete p; }
+void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU, bool profile,
+                        unsigned timeout_ms, cudaStream_t s) {
+  const void* x[1] = {dX};
+  const void* p0[1] = {dpsi0};
+  void* p1[1] = {dpsi};
+  void* u[1] = {dU};
+  p->set_profile(profile);
+  p->set_timeout(timeout_ms);
+  p->run(x, p0, p1, u, s);
+}
+void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st) {
+  p->walk_stats(0, st);
+  st->gemm_launches = p->gemm_launches();
+  st->launches = p->launches();
+  st->flops = p->flops();
+}
+
+}  // namespace fx
+
+// ================================================================== C ABI
+struct fx_batch {
+  std::unique_ptr<fx::BatchPipeline> p;
+  int dtype = FX_C64;
+  std::vector<int64_t> ns;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double ms = 0;
+  std::vector<void*> h_in;   // device staging of host runs (X, psi0, psi per walk)
+  std::string last_error;
+};
+
+namespace {
+std::mutex g_batch_mu;
+std::string g_batch_err;
+int bfail(fx_batch_handle b, const fx::Error& e) {
+  if (b) b->last_error = e.msg;
+  std::lock_guard<std::mutex> lk(g_batch_mu);
+  g_batch_err = e.msg;
+  return e.code;
+}
+template <typename F>
+int bguard(fx_batch_handle b, F&& f) {
+  try {
+    f();
+    return FX_OK;
+  } catch (const fx::Error& e) {
+    return bfail(b, e);
+  } catch (const std::bad_alloc&) {
+    return bfail(b, fx::Error{FX_ERR_NOMEM, "host allocation failed"});
+  } catch (const std::exception& e) {
+    return bfail(b, fx::Error{FX_ERR_CUDA, e.what()});
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int fx_batch_create(size_t count, const int64_t* n, int dtype, fx_batch_handle* out) {
+  if (!out || (!n && count)) return bfail(nullptr, fx::Error{FX_ERR_VALUE, "null argument"});
+  *out = nullptr;
+  if (dtype != FX_C64 && dtype != FX_C128)
+    return bfail(nullptr, fx::Error{FX_ERR_TYPE, "batched walks are complex64 or complex128"});
+  if (count == 0 || count > 65536) return bfail(nullptr, fx::Error{FX_ERR_VALUE, "batch size must be 1..65536"});
+  if (!fx_device_ok()) return bfail(nullptr, fx::Error{FX_ERR_NODEV, "no sm_100 CUDA device"});
+  fx_batch_handle b = new (std::nothrow) fx_batch();
+  if (!b) return bfail(nullptr, fx::Error{FX_ERR_NOMEM, "host allocation failed"});
+  const int rc = bguard(b, [&] {
+    b->dtype = dtype;
+    b->ns.assign(n, n + count);
+    FX_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    FX_CUDA(cudaEventCreate(&b->ev0));
+    FX_CUDA(cudaEventCreate(&b->ev1));
+    b->p.reset(new fx::BatchPipeline(b->ns, dtype));
+  });
+  if (rc != FX_OK) {
+    fx_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  (void)0;
+  return FX_OK;
+}
+
+int fx_batch_destroy(fx_batch_handle b) {
+  if (!b) return FX_OK;
+  b->p.reset();
+  for (void* p : b->h_in)
+    if (p) cudaFree(p);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return FX_OK;
+}
+
+int fx_batch_set_option(fx_batch_handle b, int key, double value) {
+  if (!b) return bfail(nullptr, fx::Error{FX_ERR_VALUE, "null handle"});
+  switch (key) {
+    case FX_BATCH_OPT_GRAPH: b->p->set_graph(value != 0.0); return FX_OK;
+    case FX_BATCH_OPT_TIMEOUT_MS:
+      if (value < 1) return bfail(b, fx::Error{FX_ERR_VALUE, "timeout must be >= 1 ms"});
+      b->p->set_timeout((unsigned)value);
+      return FX_OK;
+    case FX_BATCH_OPT_FORCE_M: b->p->force((int)value, -1); return FX_OK;
+  }
+  return bfail(b, fx::Error{FX_ERR_VALUE, "unknown batch option"});
+}
+
+int fx_batch_walk_device(fx_batch_handle b, const void* const* dX, const void* const* dpsi0, void* const* dpsi,
+                         void* stream) {
+  if (!b || !dX || !dpsi0 || !dpsi) return FX_ERR_VALUE;
+  return bguard(b, [&] {
+    cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
+    FX_CUDA(cudaEventRecord(b->ev0, s));
+    b->p->run(dX, dpsi0, dpsi, nullptr, s);
+    FX_CUDA(cudaEventRecord(b->ev1, s));
+    FX_CUDA(cudaEventSynchronize(b->ev1));
+    float ms = 0;
+    FX_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    b->ms = ms;
+  });
+}
+
+int fx_batch_walk_host(fx_batch_handle b, const void* const* X, const void* const* psi0, void* const* psi) {
+  if (!b || !X || !psi0 || !psi) return FX_ERR_VALUE;
+  return bguard(b, [&] {
+    const size_t W = b->ns.size();
+    const size_t es = b->dtype == FX_C64 ? 8 : 16;
+    if (b->h_in.empty()) {
+      b->h_in.assign(3 * W, nullptr);
+      for (size_t w = 0; w < W; ++w) {
+        const size_t n = (size_t)b->ns[w];
+        FX_CUDA(cudaMalloc(&b->h_in[w], n * n * es));
+        FX_CUDA(cudaMalloc(&b->h_in[W + w], n * es));
+        FX_CUDA(cudaMalloc(&b->h_in[2 * W + w], n * es));
+      }
+    }
+    for (size_t w = 0; w < W; ++w) {
+      const size_t n = (size_t)b->ns[w];
+      FX_CUDA(cudaMemcpyAsync(b->h_in[w], X[w], n * n * es, cudaMemcpyHostToDevice, b->stream));
+      FX_CUDA(cudaMemcpyAsync(b->h_in[W + w], psi0[w], n * es, cudaMemcpyHostToDevice, b->stream));
+    }
+    b->p->run((const void* const*)b->h_in.data(), (const void* const*)(b->h_in.data() + W),
+              (void* const*)(b->h_in.data() + 2 * W), nullptr, b->stream);
+    for (size_t w = 0; w < W; ++w) {
+      const size_t n = (size_t)b->ns[w];
+      FX_CUDA(cudaMemcpyAsync(psi[w], b->h_in[2 * W + w], n * es, cudaMemcpyDeviceToHost, b->stream));
+    }
+    FX_CUDA(cudaStreamSynchronize(b->stream));
+  });
+}
+
+int fx_batch_selection(fx_batch_handle b, int32_t* m, int32_t* s) {
+  if (!b || !m || !s) return FX_ERR_VALUE;
+  for (int w = 0; w < b->p->count(); ++w) b->p->selection(w, &m[w], &s[w]);
+  return FX_OK;
+}
+
+int fx_batch_info(fx_batch_handle b, double* ms, double* flops, int32_t* launches) {
+  if (!b) return FX_ERR_VALUE;
+  if (ms) *ms = b->ms;
+  if (flops) *flops = b->p->flops();
+  if (launches) *launches = b->p->launches();
+  return FX_OK;
+}
+
+const char* fx_batch_last_error(fx_batch_handle b) {
+  if (b) return b->last_error.c_str();
+  std::lock_guard<std::mutex> lk(g_batch_mu);
+  return g_batch_err.c_str();
+}
+
+}  // extern "C"

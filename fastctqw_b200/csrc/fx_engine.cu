@@ -1037,6 +1037,8 @@ struct fx_engine {
   void* h_psi = nullptr;
   bool u_valid = false;   // h_out holds the U of the last fx_walk_host
   size_t elem = 8;
+  fx::BatchPipeline* grouped = nullptr;   // grouped pipeline for walk generators (lazy)
+  void* check_buf = nullptr;              // input statistics of the routing check
   fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0};
   fx_stats stats{};
   std::string last_error;
@@ -1091,9 +1093,47 @@ void ensure_pipeline(fx_handle h) {
   }
 }
 
+// Walk generators X = i*(real symmetric) in complex storage with the default plain-form options
+// run through the grouped pipeline (fx_batch.cu) as a batch of one: blocked Cholesky of
+// Q^H Q, explicit triangular inverse and triangle-aware products for the Pade solve, and
+// device-side norm estimation (no host round trips after the selection).  Everything else
+// (general complex or real inputs, other forms or options) runs the pipeline of this file.
+bool grouped_eligible(fx_handle h) {
+  const fx::RunOpts& o = h->opts;
+  return (h->dtype == FX_C64 || h->dtype == FX_C128) && o.form == FX_FORM_PLAIN && o.shift == 2 &&
+         o.structure == 1 && o.ipe == 1 && o.debug_stage == 0 && o.force_m < 0 && o.force_s < 0;
+}
+bool input_is_walk_generator(fx_handle h, const void* dA, cudaStream_t s) {
+  const int64_t n = h->n;
+  if (!h->check_buf) FX_CUDA(cudaMalloc(&h->check_buf, sizeof(double) * (6 * (size_t)n + 16)));
+  double* b = (double*)h->check_buf;
+  fx::InputStats is{b, b + 2 * n, b + 4 * n, (int*)(b + 6 * n)};
+  FX_CUDA(cudaMemsetAsync(is.flags, 0, sizeof(int) * 8, s));
+  fx::launch_input_stats(dA, h->dtype, n, is, s);
+  int f[8];
+  FX_CUDA(cudaMemcpyAsync(f, is.flags, sizeof(int) * 8, cudaMemcpyDeviceToHost, s));
+  FX_CUDA(cudaStreamSynchronize(s));
+  if (f[4]) throw fx::Error{FX_ERR_NONFINITE, "input contains NaN or Inf"};
+  return !f[0] && !f[2];
+}
+
 void run_device(fx_handle h, const void* dA, void* dU, const void* dpsi0, void* dpsi, cudaStream_t s) {
   if (h->freed) throw fx::Error{FX_ERR_FREED, "handle was freed"};
   if (h->n == 0) return;
+  if (grouped_eligible(h) && fx_device_ok() && input_is_walk_generator(h, dA, s)) {
+    if (!h->grouped) h->grouped = fx::batch_pipeline_create(h->n, h->dtype);
+    FX_CUDA(cudaEventRecord(h->ev0, s));
+    fx::batch_pipeline_run(h->grouped, dA, dpsi0, dpsi, dU, h->opts.profile != 0, h->opts.timeout_ms, s);
+    FX_CUDA(cudaEventRecord(h->ev1, s));
+    FX_CUDA(cudaEventSynchronize(h->ev1));
+    float ms = 0;
+    FX_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->stats = fx_stats{};
+    fx::batch_pipeline_stats(h->grouped, &h->stats);
+    h->stats.form = FX_FORM_PLAIN;
+    h->stats.ms_total = ms;
+    return;
+  }
   ensure_pipeline(h);
   FX_CUDA(cudaEventRecord(h->ev0, s));
   if (h->p32)
@@ -1167,6 +1207,10 @@ int fx_free(fx_handle h) {
   return guarded(h, [&] {
     h->p32.reset();
     h->p64.reset();
+    if (h->grouped) fx::batch_pipeline_destroy(h->grouped);
+    h->grouped = nullptr;
+    if (h->check_buf) cudaFree(h->check_buf);
+    h->check_buf = nullptr;
     if (h->h_in) cudaFree(h->h_in);
     if (h->h_out) cudaFree(h->h_out);
     if (h->h_psi) cudaFree(h->h_psi);

@@ -64,6 +64,9 @@ struct I8Params {
   int64_t ldd;
   int* err;
   unsigned long long timeout_ns;
+  // grouped mode: per-tile jobs and per-problem descriptors (device memory)
+  const GProblem* probs;
+  const GTile* tiles;
 };
 
 __host__ __device__ constexpr uint32_t idesc_i8(int m, int n) {
@@ -118,7 +121,47 @@ __device__ __forceinline__ void tile_of(const I8Params& p, int tile, int& mb, in
   nb = rr / gsize;
 }
 
-template <int S, typename TO>
+// Everything a role needs to know about one output tile.
+struct TileJob {
+  int mb, nb;          // tile coordinates inside its problem
+  int kb0, kb1;        // K steps [kb0, kb1) of kBK bytes
+  int arow, brow;      // first slice row of the A / Bt tile in the (stacked) slice planes
+  int M, N;            // problem extent (stores are clipped to it)
+  int sym;
+  int prob;            // problem index (grouped) or -1
+};
+
+template <bool G>
+__device__ __forceinline__ TileJob job_of(const I8Params& p, int tile) {
+  TileJob j;
+  if constexpr (G) {
+    const GTile t = p.tiles[tile];
+    const GProblem& q = p.probs[t.prob];
+    j.mb = t.mb;
+    j.nb = t.nb;
+    j.kb0 = t.kb0;
+    j.kb1 = t.kb1;
+    j.arow = q.a_row0 + t.mb * kBM;
+    j.brow = q.b_row0 + t.nb * p.bn;
+    j.M = q.M;
+    j.N = q.N;
+    j.sym = q.sym;
+    j.prob = t.prob;
+  } else {
+    tile_of(p, tile, j.mb, j.nb);
+    j.kb0 = 0;
+    j.kb1 = p.K / kBK;
+    j.arow = j.mb * kBM;
+    j.brow = j.nb * p.bn;
+    j.M = p.M;
+    j.N = p.N;
+    j.sym = p.sym;
+    j.prob = -1;
+  }
+  return j;
+}
+
+template <int S, typename TO, bool G>
 __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__ I8Params p) {
   using Cf = I8Cfg<S>;
   constexpr int kBN = Cf::kBN;
@@ -133,7 +176,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
   __shared__ volatile int s_abort;
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int nkb = p.K / kBK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -169,10 +211,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
       int issued[kStages];
       for (int s = 0; s < kStages; ++s) issued[s] = -1;
       for (int tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x) {
-        int mb, nb;
-        tile_of(p, tile, mb, nb);
+        const TileJob jb = job_of<G>(p, tile);
         for (int t = 0; t < p.nterms && ok; ++t) {
-          for (int kb = 0; kb < nkb; ++kb, ++kit) {
+          for (int kb = jb.kb0; kb < jb.kb1; ++kb, ++kit) {
             const int s = kit % kStages;
             const uint32_t ph = (kit / kStages) & 1;
             if (!mbar_wait(&empty_bar[s], ph ^ 1, &s_abort, p.timeout_ns, p.err)) {
@@ -182,9 +223,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
             uint8_t* st = smem + (size_t)s * kStage;
             mbar_expect_tx(&full_bar[s], kStage);
             for (int q = 0; q < S; ++q) {
-              tma_load_2d(st + q * Cf::kATile, &p.map_a[t][q], &full_bar[s], kb * kBK, mb * kBM);
+              tma_load_2d(st + q * Cf::kATile, &p.map_a[t][q], &full_bar[s], kb * kBK, jb.arow);
               tma_load_2d(st + S * Cf::kATile + q * Cf::kBTile, &p.map_b[t][q], &full_bar[s], kb * kBK,
-                          nb * kBN);
+                          jb.brow);
             }
             issued[s] = (int)(kit / kStages);
           }
@@ -208,11 +249,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
       for (int tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x, ++it) {
         if (!mbar_wait(&tempty_bar, (it & 1) ^ 1, &s_abort, p.timeout_ns, p.err)) break;
         tc_fence_after();
+        const TileJob jb = job_of<G>(p, tile);
         bool first[S];
 #pragma unroll
         for (int l = 0; l < S; ++l) first[l] = true;
         for (int t = 0; t < p.nterms && ok; ++t) {
-          for (int kb = 0; kb < nkb; ++kb, ++kit) {
+          for (int kb = jb.kb0; kb < jb.kb1; ++kb, ++kit) {
             const int s = kit % kStages;
             const uint32_t ph = (kit / kStages) & 1;
             if (!mbar_wait(&full_bar[s], ph, &s_abort, p.timeout_ns, p.err)) {
@@ -261,41 +303,62 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++it) {
       if (!mbar_wait(&tfull_bar, it & 1, &s_abort, p.timeout_ns, p.err)) break;
       tc_fence_after();
-      int mb, nb;
-      tile_of(p, tile, mb, nb);
-      const int64_t row = (int64_t)mb * kBM + q * 32 + lane;
-      const bool row_ok = row < p.M;
-      const int ea = row_ok ? p.aexp[row] : 0;
+      const TileJob jb = job_of<G>(p, tile);
+      double alpha = p.alpha, beta = p.beta, gamma = p.gamma;
+      const TO* Cq = Cp;
+      TO* Dq = Dp;
+      int64_t ldc = p.ldc, ldd = p.ldd;
+      const int* aexp = p.aexp;
+      const int* bexp = p.bexp;
+      if constexpr (G) {
+        const GProblem& pr = p.probs[jb.prob];
+        alpha = pr.alpha;
+        beta = pr.beta;
+        gamma = pr.gamma;
+        Cq = (const TO*)pr.C;
+        Dq = (TO*)pr.D;
+        ldc = pr.ldc;
+        ldd = pr.ldd;
+        aexp += pr.a_row0;
+        bexp += pr.b_row0;
+      }
+      const bool acc = jb.kb1 > jb.kb0;   // an empty K range leaves the accumulator unwritten
+      const int64_t row = (int64_t)jb.mb * kBM + q * 32 + lane;
+      const bool row_ok = row < jb.M;
+      const int ea = row_ok ? aexp[row] : 0;
       for (int cc = 0; cc < kBN / 16; ++cc) {
         int lv[S][16];
         const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(cc * 16);
 #pragma unroll
         for (int l = 0; l < S; ++l) tmem_ld16(ta + l * kBN, lv[l]);
         tmem_wait_ld();
-        const int64_t col0 = (int64_t)nb * kBN + cc * 16;
-        if (!row_ok || col0 >= p.N) continue;
+        const int64_t col0 = (int64_t)jb.nb * kBN + cc * 16;
+        if (!row_ok || col0 >= jb.N) continue;
         TO out[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const int64_t col = col0 + i;
-          double v = (double)lv[S - 1][i];
+          double v = 0.0;
+          if (acc) {
+            v = (double)lv[S - 1][i];
 #pragma unroll
-          for (int l = S - 2; l >= 0; --l) v = v * 0x1p-7 + (double)lv[l][i];
-          v = ldexp(v, ea + p.bexp[col] - 14);
-          v *= p.alpha;
-          if (p.beta != 0.0) v += p.beta * (double)Cp[row * p.ldc + col];
-          if (col == row) v += p.gamma;
+            for (int l = S - 2; l >= 0; --l) v = v * 0x1p-7 + (double)lv[l][i];
+            v = ldexp(v, ea + bexp[col] - 14);
+          }
+          v *= alpha;
+          if (beta != 0.0) v += beta * (double)Cq[row * ldc + col];
+          if (col == row) v += gamma;
           out[i] = (TO)v;
         }
-        if (!p.sym) {
+        if (!jb.sym) {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) Dp[row * p.ldd + col0 + i] = out[i];
+          for (int i = 0; i < 16; ++i) Dq[row * ldd + col0 + i] = out[i];
         } else {
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             const int64_t col = col0 + i;
-            if (col >= row) Dp[row * p.ldd + col] = out[i];
-            if (col > row) Dp[col * p.ldd + row] = out[i];
+            if (col >= row) Dq[row * ldd + col] = out[i];
+            if (col > row) Dq[col * ldd + row] = out[i];
           }
         }
       }
@@ -313,16 +376,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
 }
 
 // ---- slicing: warp per row; the row exponent is shared by the real and imaginary planes.
+// rre / rim: the source row (rim may be null); orow: offset of the row in the slice planes.
 template <typename TI>
-__global__ void k_slice_rows(const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K, int S,
-                             I8Slices out, bool want_neg) {
-  const int lane = threadIdx.x & 31;
-  const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-  if (row >= rows) return;
+__device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t K, int S, const I8Slices& out,
+                                          int64_t orow, bool want_neg, int lane) {
   double mx = 0.0;
   for (int64_t k = lane; k < K; k += 32) {
-    mx = fmax(mx, fabs((double)re[row * ld + k]));
-    if (im) mx = fmax(mx, fabs((double)im[row * ld + k]));
+    mx = fmax(mx, fabs((double)rre[k]));
+    if (rim) mx = fmax(mx, fabs((double)rim[k]));
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -333,18 +394,18 @@ __global__ void k_slice_rows(const TI* re, const TI* im, int64_t ld, int64_t row
     frexp(mx, &e);
     if (ldexp(mx, 7 - e) > 127.5) e += 1;
   }
-  if (lane == 0) out.exp[row] = e;
+  if (lane == 0) out.exp[orow] = e;
   for (int64_t k0 = (int64_t)lane * 4; k0 < K; k0 += 128) {
 #pragma unroll
     for (int plane = 0; plane < 2; ++plane) {
-      const TI* src = plane == 0 ? re : im;
+      const TI* src = plane == 0 ? rre : rim;
       if (!src) continue;
       uint32_t packed[kMaxSlices] = {0, 0, 0, 0, 0}, packed_neg[kMaxSlices] = {0, 0, 0, 0, 0};
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         // Exact in FP64 for FP32 and FP64 inputs: scaling by 2^-e, multiplying by 128 and
         // subtracting the rounded integer never round.
-        double x = (k0 + j < K) ? ldexp((double)src[row * ld + k0 + j], -e) : 0.0;
+        double x = (k0 + j < K) ? ldexp((double)src[k0 + j], -e) : 0.0;
 #pragma unroll
         for (int q = 0; q < kMaxSlices; ++q) {
           if (q < S) {
@@ -361,12 +422,42 @@ __global__ void k_slice_rows(const TI* re, const TI* im, int64_t ld, int64_t row
       for (int q = 0; q < kMaxSlices; ++q) {
         if (q >= S) continue;
         int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
-        if (dst) *reinterpret_cast<uint32_t*>(dst + row * out.ld + k0) = packed[q];
+        if (dst) *reinterpret_cast<uint32_t*>(dst + orow * out.ld + k0) = packed[q];
         if (plane == 1 && want_neg && out.neg_im[q])
-          *reinterpret_cast<uint32_t*>(out.neg_im[q] + row * out.ld + k0) = packed_neg[q];
+          *reinterpret_cast<uint32_t*>(out.neg_im[q] + orow * out.ld + k0) = packed_neg[q];
       }
     }
   }
+}
+
+template <typename TI>
+__global__ void k_slice_rows(const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K, int S,
+                             I8Slices out, bool want_neg) {
+  const int lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (row >= rows) return;
+  slice_row<TI>(re + row * ld, im ? im + row * ld : nullptr, K, S, out, row, want_neg, lane);
+}
+
+// Grouped slicing: warp per stacked row; the slab is found by binary search on row0.
+template <typename TI>
+__global__ void k_slice_rows_grouped(const GSlab* slabs, int nslabs, int64_t total_rows, int S, I8Slices out,
+                                     bool want_neg) {
+  const int lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (row >= total_rows) return;
+  int lo = 0, hi = nslabs - 1;
+  while (lo < hi) {   // last slab with row0 <= row
+    const int mid = (lo + hi + 1) >> 1;
+    if (slabs[mid].row0 <= row) lo = mid;
+    else hi = mid - 1;
+  }
+  const GSlab sb = slabs[lo];
+  const int64_t local = row - sb.row0;
+  if (local < 0 || local >= sb.rows) return;
+  const TI* re = (const TI*)sb.re + local * sb.ld;
+  const TI* im = sb.im ? (const TI*)sb.im + local * sb.ld : nullptr;
+  slice_row<TI>(re, im, sb.K, S, out, row, want_neg && sb.im != nullptr, lane);
 }
 
 void make_map_u8(CUtensorMap* m, const int8_t* base, int64_t rows, int64_t cols, int64_t ld, int box_rows);
@@ -431,6 +522,18 @@ template void launch_slice_rows<float>(int, const float*, const float*, int64_t,
 template void launch_slice_rows<double>(int, const double*, const double*, int64_t, int64_t, int64_t, I8Slices,
                                         bool, cudaStream_t);
 
+template <typename TI>
+void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, I8Slices out,
+                               bool want_neg_im, cudaStream_t s) {
+  if (S < 4 || S > kMaxSlices) throw Error{FX_ERR_VALUE, "slice count must be 4 or 5"};
+  if (out.ld % 16 != 0) throw Error{FX_ERR_VALUE, "grouped slice: pitch must be a multiple of 16"};
+  if (nslabs <= 0 || total_rows <= 0) return;
+  k_slice_rows_grouped<TI><<<cdiv(total_rows, 8), 256, 0, s>>>(slabs, nslabs, total_rows, S, out, want_neg_im);
+  FX_LAUNCH_CHECK();
+}
+template void launch_slice_rows_grouped<float>(int, const GSlab*, int, int64_t, I8Slices, bool, cudaStream_t);
+template void launch_slice_rows_grouped<double>(int, const GSlab*, int, int64_t, I8Slices, bool, cudaStream_t);
+
 namespace {
 template <int S, typename TO>
 void launch_i8_cfg(I8Params& p, const I8Term* terms, int nterms, int64_t M, int64_t N, int64_t K, int64_t lda,
@@ -438,7 +541,7 @@ void launch_i8_cfg(I8Params& p, const I8Term* terms, int nterms, int64_t M, int6
   using Cf = I8Cfg<S>;
   static bool attr = false;
   if (!attr) {
-    FX_CUDA(cudaFuncSetAttribute(k_gemm_i8<S, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::kSmem));
+    FX_CUDA(cudaFuncSetAttribute(k_gemm_i8<S, TO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::kSmem));
     attr = true;
   }
   for (int t = 0; t < nterms; ++t)
@@ -456,7 +559,7 @@ void launch_i8_cfg(I8Params& p, const I8Term* terms, int nterms, int64_t M, int6
     p.ntiles = p.tiles_m * p.tiles_n;
   }
   const int grid = p.ntiles < sm_count() ? p.ntiles : sm_count();
-  k_gemm_i8<S, TO><<<grid, kThreads, Cf::kSmem, s>>>(p);
+  k_gemm_i8<S, TO, false><<<grid, kThreads, Cf::kSmem, s>>>(p);
   FX_LAUNCH_CHECK();
 }
 }  // namespace
@@ -503,5 +606,75 @@ template void launch_gemm_i8<float>(int, int64_t, int64_t, int64_t, const I8Term
 template void launch_gemm_i8<double>(int, int64_t, int64_t, int64_t, const I8Term*, int, int64_t, int64_t,
                                      const int*, const int*, double, double, const double*, int64_t, double,
                                      double*, int64_t, bool, int*, unsigned, cudaStream_t);
+
+int i8_tile_bn(int S) { return S == 4 ? I8Cfg<4>::kBN : I8Cfg<5>::kBN; }
+
+namespace {
+template <int S, typename TO>
+void set_i8_grouped_attr() {
+  static bool attr = false;
+  if (!attr) {
+    FX_CUDA(cudaFuncSetAttribute(k_gemm_i8<S, TO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 I8Cfg<S>::kSmem));
+    attr = true;
+  }
+}
+template <int S, typename TO>
+void launch_i8_grouped_cfg(I8Params& p, const I8Term* terms, int nterms, int64_t pitch, int64_t a_rows,
+                           int64_t b_rows, int ntiles, cudaStream_t s) {
+  using Cf = I8Cfg<S>;
+  set_i8_grouped_attr<S, TO>();
+  for (int t = 0; t < nterms; ++t)
+    for (int q = 0; q < S; ++q) {
+      make_map_u8(&p.map_a[t][q], terms[t].a[q], a_rows, pitch, pitch, kBM);
+      make_map_u8(&p.map_b[t][q], terms[t].b[q], b_rows, pitch, pitch, Cf::kBN);
+    }
+  p.bn = Cf::kBN;
+  p.ntiles = ntiles;
+  const int grid = ntiles < sm_count() ? ntiles : sm_count();
+  k_gemm_i8<S, TO, true><<<grid, kThreads, Cf::kSmem, s>>>(p);
+  FX_LAUNCH_CHECK();
+}
+}  // namespace
+
+void prepare_gemm_i8_grouped(int S) {
+  if (S == 4) {
+    set_i8_grouped_attr<4, double>();
+    set_i8_grouped_attr<4, float>();
+  } else {
+    set_i8_grouped_attr<5, double>();
+    set_i8_grouped_attr<5, float>();
+  }
+}
+
+template <typename TO>
+void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitch, int64_t a_rows, int64_t b_rows,
+                            const int* aexp, const int* bexp, const GProblem* probs, const GTile* tiles, int ntiles,
+                            int* err, unsigned timeout_ms, cudaStream_t s) {
+  if (nterms < 1 || nterms > kMaxTerms) throw Error{FX_ERR_VALUE, "int8 product: 1 or 2 terms"};
+  if (ntiles <= 0) return;
+  if (pitch % kBK || pitch <= 0 || pitch > 32768) throw Error{FX_ERR_VALUE, "grouped int8 product: bad pitch"};
+  I8Params p;
+  memset(&p, 0, sizeof(p));
+  p.nterms = nterms;
+  p.aexp = aexp;
+  p.bexp = bexp;
+  p.err = err;
+  p.timeout_ns = (unsigned long long)timeout_ms * 1000000ull;
+  p.probs = probs;
+  p.tiles = tiles;
+  if (S == 4)
+    launch_i8_grouped_cfg<4, TO>(p, terms, nterms, pitch, a_rows, b_rows, ntiles, s);
+  else if (S == 5)
+    launch_i8_grouped_cfg<5, TO>(p, terms, nterms, pitch, a_rows, b_rows, ntiles, s);
+  else
+    throw Error{FX_ERR_VALUE, "slice count must be 4 or 5"};
+}
+template void launch_gemm_i8_grouped<float>(int, const I8Term*, int, int64_t, int64_t, int64_t, const int*,
+                                            const int*, const GProblem*, const GTile*, int, int*, unsigned,
+                                            cudaStream_t);
+template void launch_gemm_i8_grouped<double>(int, const I8Term*, int, int64_t, int64_t, int64_t, const int*,
+                                             const int*, const GProblem*, const GTile*, int, int*, unsigned,
+                                             cudaStream_t);
 
 }  // namespace fx

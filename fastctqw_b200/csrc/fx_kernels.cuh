@@ -157,6 +157,26 @@ struct I8Slices {
 template <typename TI>
 void launch_slice_rows(int S, const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K,
                        I8Slices out, bool want_neg_im, cudaStream_t s);
+// Grouped int8 product: many independent problems D_p = alpha_p A_p Bt_p^T + beta_p C_p +
+// gamma_p I in one launch.  The A (Bt) slices of every problem are rows of the same stacked
+// slice planes (one common pitch); each problem names its first rows there.
+struct GProblem {
+  int a_row0, b_row0;   // first slice row of A_p / Bt_p in the stacked planes
+  int M, N, K;          // M, N multiples of 16; K multiple of 64 and <= the pitch
+  int sym;              // symmetric output: only tiles touching the upper triangle are listed
+  double alpha, beta, gamma;
+  const void* C;        // element type of the launch (T)
+  int64_t ldc;
+  void* D;
+  int64_t ldd;
+};
+// One output tile of a grouped launch: problem, tile coordinates (BM = 128, BN = the launch's
+// tile width: 128 for 4 slices, 96 for 5), and the K steps [kb0, kb1) of 64 bytes to run (a
+// triangular factor has zero blocks that need no K steps).
+struct GTile {
+  int prob, mb, nb, kb0, kb1, pad;
+};
+int i8_tile_bn(int S);
 struct I8Term {
   const int8_t* a[5];
   const int8_t* b[5];
@@ -169,8 +189,49 @@ void launch_gemm_i8(int S, int64_t M, int64_t N, int64_t K, const I8Term* terms,
                     int64_t lda, int64_t ldb, const int* aexp, const int* bexp, double alpha,
                     double beta, const TO* C, int64_t ldc, double gamma, TO* D, int64_t ldd, bool sym,
                     int* err, unsigned timeout_ms, cudaStream_t s);
+// Grouped Cholesky block step: one job per matrix (nb <= 128; every job's block is nb wide).
+struct GChol {
+  void* G;
+  int64_t ld, k0;
+  int nb, pad;
+  void* Linv;
+  void* LinvT;
+};
+template <typename T>
+void launch_potrf_inv_grouped(const GChol* jobs, int njobs, int* err, cudaStream_t s);
+// Set the kernels' shared-memory attributes ahead of a stream capture.
+void prepare_potrf_inv_grouped();
+void prepare_gemm_i8_grouped(int S);
+// Grouped pipeline of fx_batch.cu, as a one-walk pipeline for the per-walk engine: walk
+// generators X = i*(real symmetric), plain form (int8 slices on FP64 masters).  Any of dpsi0 /
+// dpsi / dU may be null.  Throws fx::Error (FX_ERR_VALUE when X is not of that form).
+class BatchPipeline;
+BatchPipeline* batch_pipeline_create(int64_t n, int dtype);
+void batch_pipeline_destroy(BatchPipeline* p);
+void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU, bool profile,
+                        unsigned timeout_ms, cudaStream_t s);
+void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st);
 // Records the message returned by fx_product_error (fx_debug.cu).
 void set_product_error(const std::string& msg);
+// Grouped form of launch_gemm_i8: `probs` and `tiles` are device arrays; the slice planes of
+// `terms` are the stacked planes (pitch bytes per row, a_rows / b_rows rows); aexp / bexp are
+// indexed by stacked row.
+template <typename TO>
+void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitch, int64_t a_rows,
+                            int64_t b_rows, const int* aexp, const int* bexp, const GProblem* probs,
+                            const GTile* tiles, int ntiles, int* err, unsigned timeout_ms, cudaStream_t s);
+// Grouped slicing: slab k copies rows [0, rows_k) of a planar (re, im) source with leading
+// dimension ld_k, K_k columns, into stacked rows [row0_k, row0_k + rows_k).  Slabs are sorted
+// by row0 and do not overlap; rows between slabs are left alone.
+struct GSlab {
+  const void* re;
+  const void* im;
+  int64_t ld;
+  int rows, K, row0, pad;
+};
+template <typename TI>
+void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, I8Slices out,
+                               bool want_neg_im, cudaStream_t s);
 // In place A <- (A + A^T) / 2 of an n x n plane (exact symmetry of a result known to be
 // symmetric in exact arithmetic).
 template <typename T>

@@ -148,6 +148,37 @@ int fx_product_f32_noalloc(int64_t M, int64_t N, int64_t K, const float* A, int6
                            const float* Bt, int64_t ldb, float alpha, float beta, const float* C,
                            int64_t ldc, float gamma, float* D, int64_t ldd, void* stream);
 
+/* ---- Batched walks: many independent walks of uneven sizes in grouped launches.
+ * No counterpart in the reference (it ran one matrix per MatrixExpCalculator object,
+ * include/MatrixExpCalculator.h:17-103, one walk per Ctqw.runWalk, FastCTQW/Ctqw.py:90-94);
+ * this is the batched form of fx_walk_device for walk generators X_w = i*(real symmetric)
+ * (X = -iHt with real symmetric H).  Every phase of the pipeline is one grouped launch over
+ * all walks (tensor-core products over a tile list spanning the walks, one-CTA-per-walk
+ * Cholesky blocks and 1-norm estimates); everything after the (m, s) selection is replayed
+ * as one CUDA graph.  Products: int8 Ozaki slices on FP64 masters (the plain form). */
+typedef struct fx_batch* fx_batch_handle;
+enum fx_batch_option {
+  FX_BATCH_OPT_GRAPH = 0,       /* 1 (default): replay the post-selection phases as a CUDA graph */
+  FX_BATCH_OPT_TIMEOUT_MS = 1,  /* bound of every device-side wait (default 2000)               */
+  FX_BATCH_OPT_FORCE_M = 2      /* diagnostics: force the Pade degree (-1 automatic)            */
+};
+/* count walks of sizes n[0..count); dtype FX_C64 or FX_C128 (of X, psi0 and psi). */
+int fx_batch_create(size_t count, const int64_t* n, int dtype, fx_batch_handle* out);
+int fx_batch_destroy(fx_batch_handle b);
+int fx_batch_set_option(fx_batch_handle b, int key, double value);
+/* psi_w = expm(X_w) psi0_w for all walks; arrays of `count` device pointers (X_w: n_w x n_w
+ * row-major interleaved complex; psi0_w, psi_w: n_w). */
+int fx_batch_walk_device(fx_batch_handle b, const void* const* dX, const void* const* dpsi0,
+                         void* const* dpsi, void* stream);
+/* The same with host buffers (copies in and out inside the call). */
+int fx_batch_walk_host(fx_batch_handle b, const void* const* X, const void* const* psi0,
+                       void* const* psi);
+/* (m, s) chosen for every walk by the last run (arrays of `count`). */
+int fx_batch_selection(fx_batch_handle b, int32_t* m, int32_t* s);
+/* Device time (ms, CUDA events), algorithmic flops and kernel launches of the last run. */
+int fx_batch_info(fx_batch_handle b, double* ms, double* flops, int32_t* launches);
+const char* fx_batch_last_error(fx_batch_handle b);
+
 /* Device memory currently in use on the current device, GB. */
 double fx_gpu_memory_gb(void);
 /* 1 if a device with compute capability 10.x is present. */

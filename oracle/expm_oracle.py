@@ -288,12 +288,24 @@ class Shift:
 
 
 def common_line_sum(A: np.ndarray):
-    """Return c if all row sums and column sums of A equal c exactly (FP64 sums), else None."""
+    """Return c (row 0's sum) if every row sum and column sum of A equals it within the
+    rounding of a sum, 4 n 2^-53 max_i sum_j (|Re A_ij| + |Im A_ij|); else None.
+
+    Exact equality of floating-point sums depends on the order of summation (row sums of a
+    weighted regular graph with non-representable weights differ in the last bit), so the test
+    is made at rounding level; the device makes the same test.
+    """
     if A.shape[0] == 0:
         return None
-    r = A.astype(np.complex128).sum(axis=1)
-    c = A.astype(np.complex128).sum(axis=0)
-    if np.all(r == r[0]) and np.all(c == r[0]):
+    n = A.shape[0]
+    A = A.astype(np.complex128)
+    r = A.sum(axis=1)
+    c = A.sum(axis=0)
+    scale = float(np.max(np.abs(A.real).sum(axis=1) + np.abs(A.imag).sum(axis=1)))
+    tol = 4.0 * n * 2.0 ** -53 * scale
+    dev = max(np.max(np.abs(r.real - r[0].real)), np.max(np.abs(r.imag - r[0].imag)),
+              np.max(np.abs(c.real - r[0].real)), np.max(np.abs(c.imag - r[0].imag)))
+    if dev <= tol:
         return complex(r[0])
     return None
 

@@ -81,9 +81,17 @@ def test_shift_identities():
     a = np.triu(a, 1)
     a = a + a.T
     L = np.diag(a.sum(1)) - a
-    # 0.8 is not a binary fraction: the rounded diagonal breaks exact zero row sums, so the
-    # rank-one shift must not apply (it would change the matrix being exponentiated).
-    assert not eo.preprocess(1j * 0.8 * L, "auto")[1].rank1
+    # 0.8 is not a binary fraction: the rounded entries leave row sums of order 1e-16 instead
+    # of exact zeros.  The shift still applies (the line sums agree to rounding level) and the
+    # result stays exact to rounding.
+    X8 = 1j * 0.8 * L
+    assert eo.preprocess(X8, "auto")[1].rank1
+    assert eo.rel_error(eo.expm(X8, shift="auto", structure=True), sl.expm(X8)) < 1e-12
+    # Row sums that differ by more than rounding: no rank-one shift.
+    b = np.ones((n, n)) - np.eye(n)
+    b[0, 1] = b[1, 0] = 1.0 + 1e-9
+    assert not eo.preprocess(1j * b, "auto")[1].rank1
+    assert eo.preprocess(1j * (np.ones((n, n)) - np.eye(n)), "auto")[1].rank1
     X = 1j * 0.75 * L
     Y, sh = eo.preprocess(X, "auto")
     assert sh.rank1
