@@ -1041,6 +1041,18 @@ class BatchPipeline {
   }
 
   // ---- recorded grouped operations --------------------------------------------------
+  // Tile order of one problem: 8 x 8 blocks of tiles, row-major inside a block and over the
+  // blocks.  The ~148 tiles in flight then cover two or three blocks, so every A row panel
+  // and Bt column panel of a K step is fetched from HBM once and served to up to eight CTAs
+  // from L2 (a row-major order would stream a distinct Bt panel for every CTA).
+  template <typename F>
+  static void for_tiles(int tm, int tn, F&& f) {
+    constexpr int G = 8;
+    for (int bm = 0; bm < tm; bm += G)
+      for (int bn = 0; bn < tn; bn += G)
+        for (int mb = bm; mb < std::min(tm, bm + G); ++mb)
+          for (int nb = bn; nb < std::min(tn, bn + G); ++nb) f(mb, nb);
+  }
   // Real multiply-adds x 2 that the listed tiles compute (tile-level: 128 x BN x 64 per K step
   // and term); the int8 MMA operations issued are S(S+1)/2 times that.
   static double tile_ops(const std::vector<GTile>& tiles, int nterms) {
@@ -1088,15 +1100,14 @@ class BatchPipeline {
     for (int i = 0; i < (int)pr.size(); ++i) {
       const GProblem& p = pr[i];
       const int tm = (p.M + 127) / 128, tn = (p.N + bn - 1) / bn, kbs = p.K / 64;
-      for (int mb = 0; mb < tm; ++mb)
-        for (int nb = 0; nb < tn; ++nb) {
-          if (p.sym && !((long long)nb * bn + bn - 1 >= (long long)mb * 128)) continue;
-          int kb0 = 0, kb1 = kbs;
-          if (tri == 1) kb1 = std::min(kbs, (nb * bn + bn + 63) / 64);
-          if (tri == 2) kb0 = std::min(kbs, (nb * bn) / 64);
-          if (tri == 3) kb1 = std::min(kbs, (mb * 128 + 128 + 63) / 64);
-          tiles.push_back(GTile{i, mb, nb, kb0, kb1, 0});
-        }
+      for_tiles(tm, tn, [&](int mb, int nb) {
+        if (p.sym && !((long long)nb * bn + bn - 1 >= (long long)mb * 128)) return;
+        int kb0 = 0, kb1 = kbs;
+        if (tri == 1) kb1 = std::min(kbs, (nb * bn + bn + 63) / 64);
+        if (tri == 2) kb0 = std::min(kbs, (nb * bn) / 64);
+        if (tri == 3) kb1 = std::min(kbs, (mb * 128 + 128 + 63) / 64);
+        tiles.push_back(GTile{i, mb, nb, kb0, kb1, 0});
+      });
     }
     // Largest K ranges first: the persistent CTAs then finish close together.
     std::stable_sort(tiles.begin(), tiles.end(),
@@ -1108,6 +1119,9 @@ class BatchPipeline {
     const size_t o_sa = st.put(a_sorted), o_sb = st.put(b_sorted), o_pr = st.put(pr), o_t = st.put(tiles);
     const int nsa = (int)a_sorted.size(), nsb = (int)b_sorted.size(), nt = (int)tiles.size();
     const double ops = tile_ops(tiles, 1);
+    int64_t a_span = 0, b_span = 0;
+    for (const GSlab& g : a_sorted) a_span = std::max<int64_t>(a_span, (int64_t)g.row0 + g.rows);
+    for (const GSlab& g : b_sorted) b_span = std::max<int64_t>(b_span, (int64_t)g.row0 + g.rows);
     r.launches += same ? 2 : 3;
     r.gemms += 1;
     r.ops.push_back([=]() {
@@ -1119,11 +1133,11 @@ class BatchPipeline {
       outa.exp = aexp();
       outb.exp = bexp();
       outa.ld = outb.ld = pitch_;
-      launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, a_rows_, outa, false, stream_);
+      launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, a_span, outa, false, stream_);
       I8Term t{};
       for (int q = 0; q < kS; ++q) t.a[q] = outa.re[q];
       if (!same) {
-        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sb), nsb, rows_, outb, false, stream_);
+        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sb), nsb, b_span, outb, false, stream_);
         for (int q = 0; q < kS; ++q) t.b[q] = outb.re[q];
       } else {
         for (int q = 0; q < kS; ++q) t.b[q] = outa.re[q];
@@ -1284,8 +1298,7 @@ class BatchPipeline {
     combo(st, r, all, kY, m_a2, cf);                              // P2 im -> Y
     cholesky(st, r, kA4);
     transpose(st, r, all, kA4, kT1);                              // L^T -> T1
-    inverse(st, r, kA4, kT1, kT2, kA2);                           // X = L^-1 -> T2 (scratch A2)
-    transpose(st, r, all, kT2, kW);                               // X^T -> W
+    inverse(st, r, kT1, kT2, kW, kA2);                            // X = L^-1 -> T2, X^T -> W (scratch A2)
     // Z = P2 X^T (re -> V, im -> T1); R^T = Z X (re -> A4, im -> A2)
     complex_by_real(st, r, all, kA6, kY, kT2, kV, kT1, 1);
     complex_by_real(st, r, all, kV, kT1, kW, kA4, kA2, 2);
@@ -1408,9 +1421,9 @@ class BatchPipeline {
       std::vector<GTile> tiles;
       for (int i = 0; i < (int)prr.size(); ++i) {
         const int tm = (prr[i].M + 127) / 128, tn = (prr[i].N + bn - 1) / bn;
-        for (int mb = 0; mb < tm; ++mb)
-          for (int nb = 0; nb < tn; ++nb)
-            if ((long long)nb * bn + bn - 1 >= (long long)mb * 128) tiles.push_back(GTile{i, mb, nb, 0, prr[i].K / 64, 0});
+        for_tiles(tm, tn, [&](int mb, int nb) {
+          if ((long long)nb * bn + bn - 1 >= (long long)mb * 128) tiles.push_back(GTile{i, mb, nb, 0, prr[i].K / 64, 0});
+        });
       }
       std::stable_sort(tiles.begin(), tiles.end(),
                        [](const GTile& x, const GTile& y) { return (x.kb1 - x.kb0) > (y.kb1 - y.kb0); });
@@ -1539,11 +1552,26 @@ class BatchPipeline {
     }
   }
 
-  // X = L^-1 (arena x) from L (arena l, lower), L^T (arena lt) and the diagonal-block inverses;
-  // blocked, backward over block columns: X[>j, j] = -(X[>j, >j] L[>j, j]) Linv_jj.
-  void inverse(Staging& st, Rec& r, int l, int lt, int x, int scratch) {
+  // X = L^-1 (arena x) and X^T (arena xt) from L^T (arena lt) and the inverted 128 x 128
+  // diagonal blocks, by recursive halving: for a block range split into [first | second],
+  //   X21 = -X22 L21 X11,
+  // computed as T = X22 L21 (X22 lower triangular: K steps bounded per tile row) and
+  // X21 = -T X11 (X11 lower triangular; its transpose X11^T is read by rows), whose epilogue
+  // also stores X21^T.  All nodes of one depth, over all walks, form one grouped launch pair,
+  // deepest first, so a walk of J blocks takes 2 ceil(log2 J) launches.
+  struct Node {
+    int w, r0, h1, r1, h2;   // first block [r0, r0 + h1), second block [r1, r1 + h2), elements
+  };
+  void collect(int w, int a, int b, int depth, std::vector<std::vector<Node>>& lv) {
+    if (b - a <= 1) return;
+    const int mid = a + (b - a) / 2;
+    if ((int)lv.size() <= depth) lv.resize(depth + 1);
+    lv[depth].push_back(Node{w, a * kNb, (mid - a) * kNb, mid * kNb, (b - mid) * kNb});
+    collect(w, a, mid, depth + 1, lv);
+    collect(w, mid, b, depth + 1, lv);
+  }
+  void inverse(Staging& st, Rec& r, int lt, int x, int xt, int scratch) {
     const int W = count();
-    (void)l;
     std::vector<int64_t> loff(W);
     std::vector<int> all(W);
     for (int w = 0; w < W; ++w) {
@@ -1552,51 +1580,60 @@ class BatchPipeline {
     }
     const size_t o_lo = st.put(loff), o_all = st.put(all);
     double* X = A(x);
+    double* XT = A(xt);
     const double* Li = (const double*)linv_.p;
+    const double* LiT = (const double*)linv_.p + (size_t)rows_ * kNb;
     const dim3 g(grid_x_for(maxnp_ * maxnp_, W), W);
-    r.launches += 1;
+    r.launches += 2;
     r.ops.push_back([=]() {
       kb_init_inverse<<<g, 256, 0, stream_>>>(X, Li, dev<int>(o_all), (const BWalk*)d_walks_.p, dev<int64_t>(o_lo));
       FX_LAUNCH_CHECK();
+      kb_init_inverse<<<g, 256, 0, stream_>>>(XT, LiT, dev<int>(o_all), (const BWalk*)d_walks_.p, dev<int64_t>(o_lo));
+      FX_LAUNCH_CHECK();
     });
-    int jmax = 0;
-    for (int w = 0; w < W; ++w) jmax = std::max(jmax, walks_[w].np / kNb);
-    for (int j = jmax - 2; j >= 0; --j) {
+    std::vector<std::vector<Node>> lv;
+    for (int w = 0; w < W; ++w) collect(w, 0, walks_[w].np / kNb, 0, lv);
+    for (int d = (int)lv.size() - 1; d >= 0; --d) {
       std::vector<GSlab> sa, sb, sa2, sb2;
       std::vector<GProblem> pa, pb;
-      for (int w = 0; w < W; ++w) {
-        const BWalk& b = walks_[w];
-        const int rest = b.np - (j + 1) * kNb;
-        if (rest <= 0) continue;
-        const int64_t k1 = (int64_t)(j + 1) * kNb, k0 = (int64_t)j * kNb;
-        double* T = A(scratch) + b.off;   // rest x 128, ld 128
-        // T = X[>j, >j] L[>j, j]: A = X rows k1.., cols k1.. (lower triangular), Bt = L^T rows j-block, cols k1..
-        sa.push_back(GSlab{X + b.off + k1 * b.np + k1, nullptr, b.np, rest, rest, (int)b.row0, 0});
-        sb.push_back(GSlab{A(lt) + b.off + k0 * b.np + k1, nullptr, b.np, kNb, rest, (int)b.row0, 0});
+      for (const Node& nd : lv[d]) {
+        const BWalk& b = walks_[nd.w];
+        const int64_t np = b.np;
+        double* T = A(scratch) + b.off + (int64_t)nd.r1 * np + nd.r0;   // h2 x h1, ld np
+        // T = X22 L21: A = X22 (rows r1.., cols r1..), Bt = L21^T = rows r0.. of L^T, cols r1..
+        sa.push_back(GSlab{X + b.off + (int64_t)nd.r1 * np + nd.r1, nullptr, np, nd.h2, nd.h2,
+                           (int)(b.row0 + nd.r1), 0});
+        sb.push_back(GSlab{A(lt) + b.off + (int64_t)nd.r0 * np + nd.r1, nullptr, np, nd.h1, nd.h2,
+                           (int)(b.row0 + nd.r0), 0});
         GProblem p{};
-        p.a_row0 = p.b_row0 = (int)b.row0;
-        p.M = rest;
-        p.N = kNb;
-        p.K = rest;
+        p.a_row0 = (int)(b.row0 + nd.r1);
+        p.b_row0 = (int)(b.row0 + nd.r0);
+        p.M = nd.h2;
+        p.N = nd.h1;
+        p.K = nd.h2;
         p.alpha = 1.0;
         p.D = T;
-        p.ldd = kNb;
+        p.ldd = np;
         pa.push_back(p);
-        // X[>j, j] = -T Linv_jj: A = T, Bt = Linv_jj^T
-        sa2.push_back(GSlab{T, nullptr, kNb, rest, kNb, (int)b.row0, 0});
-        sb2.push_back(GSlab{linvT(w) + k0 * kNb, nullptr, kNb, kNb, kNb, (int)b.row0, 0});
+        // X21 = -T X11: A = T, Bt = X11^T (rows r0.. of X^T, cols r0..); also store X21^T
+        sa2.push_back(GSlab{T, nullptr, np, nd.h2, nd.h1, (int)(b.row0 + nd.r1), 0});
+        sb2.push_back(GSlab{XT + b.off + (int64_t)nd.r0 * np + nd.r0, nullptr, np, nd.h1, nd.h1,
+                            (int)(b.row0 + nd.r0), 0});
         GProblem q{};
-        q.a_row0 = q.b_row0 = (int)b.row0;
-        q.M = rest;
-        q.N = kNb;
-        q.K = kNb;
+        q.a_row0 = (int)(b.row0 + nd.r1);
+        q.b_row0 = (int)(b.row0 + nd.r0);
+        q.M = nd.h2;
+        q.N = nd.h1;
+        q.K = nd.h1;
         q.alpha = -1.0;
-        q.D = X + b.off + k1 * b.np + k0;
-        q.ldd = b.np;
+        q.D = X + b.off + (int64_t)nd.r1 * np + nd.r0;
+        q.ldd = np;
+        q.Dt = XT + b.off + (int64_t)nd.r0 * np + nd.r1;
+        q.ldt = np;
         pb.push_back(q);
       }
       grouped(st, r, sa, &sb, pa, false, 3);
-      grouped(st, r, sa2, &sb2, pb, false, 0);
+      grouped(st, r, sa2, &sb2, pb, false, 2);
     }
   }
 };

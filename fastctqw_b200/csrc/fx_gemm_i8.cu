@@ -3,9 +3,10 @@
 // matrix multiplication by using fast routines of matrix multiplication").
 //
 // Every row i of the left factor A (and every row j of the transposed right factor Bt) is
-// scaled by a power of two 2^-e so that |x| <= 127.5/128, then cut into S signed slices by
-// round-to-nearest (unbiased -- truncation toward zero biases every product coherently):
-//     x = sum_{p=1..S} s_p 2^(-7p) + r,   s_1 in [-127, 127], s_p in [-64, 64],  |r| <= 2^-(7S+1).
+// scaled by a power of two 2^-e so that |x| < 127/128, rounded to the nearest multiple of
+// 2^-7S (unbiased -- truncation toward zero biases every product coherently) and cut into S
+// signed balanced base-128 digits:
+//     x = sum_{p=1..S} s_p 2^(-7p) + r,   s_1 in [-127, 127], s_p in [-64, 63],  |r| <= 2^-(7S+1).
 // The product sum_k x_ik y_jk is assembled from the slice products with p + q <= S + 1,
 // grouped by "level" l = p + q in S int32 accumulators in tensor memory (TMEM):
 //     L_l = sum_{p+q=l} S_p T_q^T        (exact for K <= 32768)
@@ -307,7 +308,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
       double alpha = p.alpha, beta = p.beta, gamma = p.gamma;
       const TO* Cq = Cp;
       TO* Dq = Dp;
-      int64_t ldc = p.ldc, ldd = p.ldd;
+      TO* Dt = nullptr;
+      int64_t ldc = p.ldc, ldd = p.ldd, ldt = 0;
       const int* aexp = p.aexp;
       const int* bexp = p.bexp;
       if constexpr (G) {
@@ -317,8 +319,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
         gamma = pr.gamma;
         Cq = (const TO*)pr.C;
         Dq = (TO*)pr.D;
+        Dt = (TO*)pr.Dt;
         ldc = pr.ldc;
         ldd = pr.ldd;
+        ldt = pr.ldt;
         aexp += pr.a_row0;
         bexp += pr.b_row0;
       }
@@ -353,6 +357,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
         if (!jb.sym) {
 #pragma unroll
           for (int i = 0; i < 16; ++i) Dq[row * ldd + col0 + i] = out[i];
+          if (Dt) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) Dt[(col0 + i) * ldt + row] = out[i];
+          }
         } else {
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
@@ -376,46 +384,107 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
 }
 
 // ---- slicing: warp per row; the row exponent is shared by the real and imaginary planes.
-// rre / rim: the source row (rim may be null); orow: offset of the row in the slice planes.
+//
+// With the row maximum mx = m 2^e (m in [0.5, 1), e raised by one when 128 m >= 127.5), every
+// x of the row becomes the integer v = rint(x 2^(7S - e)) (exact scaling by a power of two,
+// one rounding: |x 2^-e - v 2^-7S| <= 2^-(7S+1)), and v is cut into digits from the top, each
+// the round-to-nearest-even of what is left: d_1 = rint(v / 2^7(S-1)) in [-127, 127], then
+// d_q = rint(r / 2^7(S-q)) in [-64, 64] of the remainder r.  These are the digits of the
+// greedy expansion x 128 -> rint -> remainder; they are symmetric about zero, so the
+// cross terms that the product leaves out (p + q > S + 1) average out instead of adding up
+// along K (bottom-up digits in [-64, 63] carry a bias of -1/2 that the squarings amplify).
 template <typename TI>
+struct Vec4;
+template <>
+struct Vec4<double> {
+  static __device__ __forceinline__ void load(const double* p, double v[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = b.x;
+    v[3] = b.y;
+  }
+};
+template <>
+struct Vec4<float> {
+  static __device__ __forceinline__ void load(const float* p, double v[4]) {
+    const float4 a = reinterpret_cast<const float4*>(p)[0];
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = a.z;
+    v[3] = a.w;
+  }
+};
+
+template <typename TI>
+__device__ __forceinline__ void load4(const TI* src, int64_t k0, int64_t K, bool vec, double v[4]) {
+  if (vec && k0 + 4 <= K) {
+    Vec4<TI>::load(src + k0, v);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = (k0 + j < K) ? (double)src[k0 + j] : 0.0;
+  }
+}
+
+// rre / rim: the source row (rim may be null); orow: offset of the row in the slice planes;
+// NEG: also write the slices of -im (out.neg_im).
+template <typename TI, bool NEG>
 __device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t K, int S, const I8Slices& out,
-                                          int64_t orow, bool want_neg, int lane) {
+                                          int64_t orow, int lane) {
+  const bool vec = ((reinterpret_cast<uintptr_t>(rre) | reinterpret_cast<uintptr_t>(rim)) & 15) == 0;
   double mx = 0.0;
-  for (int64_t k = lane; k < K; k += 32) {
-    mx = fmax(mx, fabs((double)rre[k]));
-    if (rim) mx = fmax(mx, fabs((double)rim[k]));
+  for (int64_t k0 = (int64_t)lane * 4; k0 < K; k0 += 128) {
+    double v[4];
+    load4<TI>(rre, k0, K, vec, v);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) mx = fmax(mx, fabs(v[j]));
+    if (rim) {
+      load4<TI>(rim, k0, K, vec, v);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mx = fmax(mx, fabs(v[j]));
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  // mx = m 2^e with m in [0.5, 1); bump e when 128 m would round to 128, so that the first
-  // slice rint(128 x) stays in [-127, 127].
   int e = 0;
   if (mx > 0.0) {
-    frexp(mx, &e);
-    if (ldexp(mx, 7 - e) > 127.5) e += 1;
+    const double m = frexp(mx, &e);
+    if (m * 128.0 >= 127.5) e += 1;
   }
   if (lane == 0) out.exp[orow] = e;
+  // 2^(7S - e) as one factor when it is a normal double (always, unless the row is tiny)
+  const int sh = 7 * S - e;
+  const bool one_factor = sh <= 1000;
+  const double scale = one_factor ? ldexp(1.0, sh) : 0.0;
   for (int64_t k0 = (int64_t)lane * 4; k0 < K; k0 += 128) {
 #pragma unroll
     for (int plane = 0; plane < 2; ++plane) {
       const TI* src = plane == 0 ? rre : rim;
       if (!src) continue;
+      double x[4];
+      load4<TI>(src, k0, K, vec, x);
       uint32_t packed[kMaxSlices] = {0, 0, 0, 0, 0}, packed_neg[kMaxSlices] = {0, 0, 0, 0, 0};
+      const bool neg = NEG && plane == 1;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        // Exact in FP64 for FP32 and FP64 inputs: scaling by 2^-e, multiplying by 128 and
-        // subtracting the rounded integer never round.
-        double x = (k0 + j < K) ? ldexp((double)src[k0 + j], -e) : 0.0;
+        const double xs = one_factor ? x[j] * scale : ldexp(ldexp(x[j], -e), 7 * S);
+        long long r = __double2ll_rn(xs);
 #pragma unroll
         for (int q = 0; q < kMaxSlices; ++q) {
-          if (q < S) {
-            x *= 128.0;
-            const double r = rint(x);
-            x -= r;
-            const int v = (int)r;
-            packed[q] |= ((uint32_t)(uint8_t)(int8_t)v) << (8 * j);
-            packed_neg[q] |= ((uint32_t)(uint8_t)(int8_t)(-v)) << (8 * j);
+          if (q >= S) continue;
+          int d;
+          if (q < S - 1) {
+            const int k = 7 * (S - 1 - q);
+            const long long half = 1ll << (k - 1);
+            long long t = (r + half) >> k;                       // round half up
+            if (((r + half) & ((1ll << k) - 1)) == 0 && (t & 1)) t -= 1;   // ties to even
+            d = (int)t;
+            r -= t << k;
+          } else {
+            d = (int)r;
           }
+          packed[q] |= ((uint32_t)(uint8_t)(int8_t)d) << (8 * j);
+          if (neg) packed_neg[q] |= ((uint32_t)(uint8_t)(int8_t)(-d)) << (8 * j);
         }
       }
 #pragma unroll
@@ -423,26 +492,24 @@ __device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t 
         if (q >= S) continue;
         int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
         if (dst) *reinterpret_cast<uint32_t*>(dst + orow * out.ld + k0) = packed[q];
-        if (plane == 1 && want_neg && out.neg_im[q])
-          *reinterpret_cast<uint32_t*>(out.neg_im[q] + orow * out.ld + k0) = packed_neg[q];
+        if (neg && out.neg_im[q]) *reinterpret_cast<uint32_t*>(out.neg_im[q] + orow * out.ld + k0) = packed_neg[q];
       }
     }
   }
 }
 
-template <typename TI>
-__global__ void k_slice_rows(const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K, int S,
-                             I8Slices out, bool want_neg) {
+template <typename TI, bool NEG>
+__global__ void __launch_bounds__(256, 3) k_slice_rows(const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K, int S,
+                             I8Slices out) {
   const int lane = threadIdx.x & 31;
   const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   if (row >= rows) return;
-  slice_row<TI>(re + row * ld, im ? im + row * ld : nullptr, K, S, out, row, want_neg, lane);
+  slice_row<TI, NEG>(re + row * ld, im ? im + row * ld : nullptr, K, S, out, row, lane);
 }
 
 // Grouped slicing: warp per stacked row; the slab is found by binary search on row0.
-template <typename TI>
-__global__ void k_slice_rows_grouped(const GSlab* slabs, int nslabs, int64_t total_rows, int S, I8Slices out,
-                                     bool want_neg) {
+template <typename TI, bool NEG>
+__global__ void __launch_bounds__(256, 3) k_slice_rows_grouped(const GSlab* slabs, int nslabs, int64_t total_rows, int S, I8Slices out) {
   const int lane = threadIdx.x & 31;
   const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   if (row >= total_rows) return;
@@ -457,7 +524,7 @@ __global__ void k_slice_rows_grouped(const GSlab* slabs, int nslabs, int64_t tot
   if (local < 0 || local >= sb.rows) return;
   const TI* re = (const TI*)sb.re + local * sb.ld;
   const TI* im = sb.im ? (const TI*)sb.im + local * sb.ld : nullptr;
-  slice_row<TI>(re, im, sb.K, S, out, row, want_neg && sb.im != nullptr, lane);
+  slice_row<TI, NEG>(re, im, sb.K, S, out, row, lane);
 }
 
 void make_map_u8(CUtensorMap* m, const int8_t* base, int64_t rows, int64_t cols, int64_t ld, int box_rows);
@@ -514,7 +581,10 @@ void launch_slice_rows(int S, const TI* re, const TI* im, int64_t ld, int64_t ro
   if (!im) {
     for (int q = 0; q < kMaxSlices; ++q) out.im[q] = out.neg_im[q] = nullptr;
   }
-  k_slice_rows<TI><<<cdiv(rows, 8), 256, 0, s>>>(re, im, ld, rows, K, S, out, want_neg_im && im != nullptr);
+  if (want_neg_im && im != nullptr)
+    k_slice_rows<TI, true><<<cdiv(rows, 8), 256, 0, s>>>(re, im, ld, rows, K, S, out);
+  else
+    k_slice_rows<TI, false><<<cdiv(rows, 8), 256, 0, s>>>(re, im, ld, rows, K, S, out);
   FX_LAUNCH_CHECK();
 }
 template void launch_slice_rows<float>(int, const float*, const float*, int64_t, int64_t, int64_t, I8Slices, bool,
@@ -528,7 +598,10 @@ void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t to
   if (S < 4 || S > kMaxSlices) throw Error{FX_ERR_VALUE, "slice count must be 4 or 5"};
   if (out.ld % 16 != 0) throw Error{FX_ERR_VALUE, "grouped slice: pitch must be a multiple of 16"};
   if (nslabs <= 0 || total_rows <= 0) return;
-  k_slice_rows_grouped<TI><<<cdiv(total_rows, 8), 256, 0, s>>>(slabs, nslabs, total_rows, S, out, want_neg_im);
+  if (want_neg_im)
+    k_slice_rows_grouped<TI, true><<<cdiv(total_rows, 8), 256, 0, s>>>(slabs, nslabs, total_rows, S, out);
+  else
+    k_slice_rows_grouped<TI, false><<<cdiv(total_rows, 8), 256, 0, s>>>(slabs, nslabs, total_rows, S, out);
   FX_LAUNCH_CHECK();
 }
 template void launch_slice_rows_grouped<float>(int, const GSlab*, int, int64_t, I8Slices, bool, cudaStream_t);

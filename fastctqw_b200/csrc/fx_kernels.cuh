@@ -169,6 +169,8 @@ struct GProblem {
   int64_t ldc;
   void* D;
   int64_t ldd;
+  void* Dt;             // optional: also store D^T here (non-symmetric problems only)
+  int64_t ldt;
 };
 // One output tile of a grouped launch: problem, tile coordinates (BM = 128, BN = the launch's
 // tile width: 128 for 4 slices, 96 for 5), and the K steps [kb0, kb1) of 64 bytes to run (a

@@ -84,3 +84,26 @@ def test_batch_rejects_general_generators():
     b = WalkBatch([40])
     with pytest.raises(ValueError):
         b.run([X], [np.ones(40, np.complex64) / np.sqrt(40)])
+
+
+def test_large_scaling_walks_keep_double_level_accuracy():
+    """Walks with many squarings (G(n, p) adjacency, no rank-one shift, s ~ 10-11) amplify any
+    systematic bias of the int8 products: the slice digits must be symmetric about zero
+    (a bias of -1/2 per digit once cost three orders of magnitude here).  Bar: 5e-12."""
+    from fastctqw_b200 import graphs
+    from fastctqw_b200.batch import WalkBatch
+    Xs, p0, refs = [], [], []
+    for n, p, t, seed in ((1536, 0.45, 6.81, 11), (1280, 0.21, 5.22, 12)):
+        A = graphs.erdos_renyi(n, p, seed=seed, dtype=np.float64)
+        t32 = float(np.float32(t))
+        Xs.append(np.asarray(1j * A * t32, dtype=np.complex64))
+        psi0 = graphs.uniform_state(n)
+        p0.append(psi0)
+        lam, V = np.linalg.eigh(A)
+        refs.append(V @ (np.exp(1j * lam * t32) * (V.T @ psi0.astype(np.complex128))))
+    b = WalkBatch([X.shape[0] for X in Xs])
+    psis = b.run(Xs, p0)
+    m, s = b.selection()
+    for k in range(len(Xs)):
+        assert s[k] >= 9, (m, s)
+        assert eo.infidelity(psis[k], refs[k]) <= 5e-12, (k, eo.infidelity(psis[k], refs[k]), s[k])
