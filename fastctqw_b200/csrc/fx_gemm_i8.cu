@@ -23,7 +23,8 @@
 //          5 x 96 TMEM columns.
 //
 // Kernel layout: persistent CTAs, K step 64 bytes (64B swizzle), one stage = S A-slice tiles +
-// S Bt-slice tiles, 3 stages; warp 0 TMA producer, warp 1 MMA issuer, warps 2-5 epilogue.
+// S Bt-slice tiles, 3 stages; warp 0 TMA producer, warp 1 MMA issuer, warps 2-9 epilogue
+// (two warps per TMEM lane quarter, each draining half of the tile columns).
 // Symmetric-output mode computes only tiles touching the upper triangle and mirrors them.
 // All waits are bounded (see fx_tc_common.cuh).
 #include "fx_kernels.cuh"
@@ -35,7 +36,7 @@ using namespace tc;
 
 constexpr int kBM = 128, kBK = 64;  // kBK in int8 elements (= bytes)
 constexpr int kMaxSlices = 5;
-constexpr int kThreads = 192;
+constexpr int kThreads = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 constexpr int kMaxTerms = 2;
 constexpr int kStages = 3;
 
@@ -122,6 +123,11 @@ __device__ __forceinline__ void tile_of(const I8Params& p, int tile, int& mb, in
   nb = rr / gsize;
 }
 
+// 2^k as a double for |k| < 1000 (exact), else 0 (the caller then falls back to ldexp).
+__device__ __forceinline__ double pow2_or_zero(int k) {
+  return (k > -1000 && k < 1000) ? __longlong_as_double((long long)(k + 1023) << 52) : 0.0;
+}
+
 // Everything a role needs to know about one output tile.
 struct TileJob {
   int mb, nb;          // tile coordinates inside its problem
@@ -184,7 +190,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
       mbar_init(&empty_bar[s], 1);
     }
     mbar_init(&tfull_bar, 1);
-    mbar_init(&tempty_bar, 128);
+    mbar_init(&tempty_bar, 256);
     mbar_init(&drain_bar, 1);
     s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -299,7 +305,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
       }
     }
   } else {
+    // Two epilogue warps per TMEM lane quarter (warp % 4), each draining half of the columns.
     const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    constexpr int kChunks = kBN / 32;   // 16-column chunks per half
     int it = 0;
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++it) {
       if (!mbar_wait(&tfull_bar, it & 1, &s_abort, p.timeout_ns, p.err)) break;
@@ -330,7 +339,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
       const int64_t row = (int64_t)jb.mb * kBM + q * 32 + lane;
       const bool row_ok = row < jb.M;
       const int ea = row_ok ? aexp[row] : 0;
-      for (int cc = 0; cc < kBN / 16; ++cc) {
+      const double rowscale = pow2_or_zero(ea - 14);
+      for (int cc = half * kChunks; cc < (half + 1) * kChunks; ++cc) {
         int lv[S][16];
         const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(cc * 16);
 #pragma unroll
@@ -347,7 +357,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
             v = (double)lv[S - 1][i];
 #pragma unroll
             for (int l = S - 2; l >= 0; --l) v = v * 0x1p-7 + (double)lv[l][i];
-            v = ldexp(v, ea + bexp[col] - 14);
+            const int eb = bexp[col];
+            v = (rowscale != 0.0 && eb > -1000 && eb < 1000) ? v * rowscale * pow2_or_zero(eb)
+                                                             : ldexp(v, ea + eb - 14);
           }
           v *= alpha;
           if (beta != 0.0) v += beta * (double)Cq[row * ldc + col];
