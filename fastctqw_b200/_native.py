@@ -21,7 +21,8 @@ CODE_DTYPE = {v: k for k, v in DTYPE_CODE.items()}
 
 FORM_PLAIN, FORM_MIXED, FORM_SIMT, FORM_FP64 = 0, 1, 2, 3
 FORMS = {"plain": FORM_PLAIN, "mixed": FORM_MIXED, "simt": FORM_SIMT, "fp64": FORM_FP64}
-OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE, OPT_DEBUG_STAGE, OPT_PROFILE = range(10)
+OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE, OPT_DEBUG_STAGE, OPT_PROFILE, OPT_SELECTOR = range(11)
+SELECTORS = {"plain": 0, "certified": 1, "learned": 2}
 
 OK, ERR_TYPE, ERR_VALUE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_NONFINITE, ERR_SINGULAR, ERR_NODEV, ERR_FREED = range(10)
 
@@ -35,7 +36,9 @@ class FxStats(ctypes.Structure):
                 ("d", ctypes.c_double * 5), ("ms_total", ctypes.c_double),
                 ("flops", ctypes.c_double), ("prod_ms", ctypes.c_double),
                 ("prod_ops", ctypes.c_double), ("prod_flops", ctypes.c_double),
-                ("prod_launches", ctypes.c_int32), ("reserved2", ctypes.c_int32)]
+                ("prod_launches", ctypes.c_int32), ("reserved2", ctypes.c_int32),
+                ("selector", ctypes.c_int32), ("sel_outcome", ctypes.c_int32),
+                ("plain_m", ctypes.c_int32), ("plain_s", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         out = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("d", "reserved", "reserved2")}
@@ -84,12 +87,24 @@ SIGNATURES = {
     "fx_batch_info": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)],
     "fx_batch_last_error": [ctypes.c_void_p],
+    "fx_batch_details": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32),
+                         ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                         ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
+    "fx_selector_set_weights": [ctypes.POINTER(ctypes.c_float), ctypes.c_int64],
+    "fx_mlp_param_count": [],
+    "fx_mlp_infer": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
+    "fx_mlp_loss_grad": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                         ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    "fx_mlp_train": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                     ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_uint64,
+                     ctypes.POINTER(ctypes.c_float), ctypes.c_void_p],
+    "fx_mlp_error": [],
     "fx_gpu_memory_gb": [],
     "fx_device_ok": [],
     "fx_version": [],
 }
 RESTYPES = {"fx_last_error": ctypes.c_char_p, "fx_version": ctypes.c_char_p,
-            "fx_batch_last_error": ctypes.c_char_p,
+            "fx_batch_last_error": ctypes.c_char_p, "fx_mlp_error": ctypes.c_char_p,
             "fx_product_error": ctypes.c_char_p,
             "fx_gpu_memory_gb": ctypes.c_double}
 
@@ -172,7 +187,7 @@ class Engine:
                   structure: bool | None = None, force_m: int | None = None,
                   force_s: int | None = None, ipe: bool | None = None,
                   timeout_ms: float | None = None, debug_stage: int | None = None,
-                  profile: bool | None = None) -> None:
+                  profile: bool | None = None, selector: str | None = None) -> None:
         if form is not None:
             if form not in FORMS:
                 raise ValueError(f"form must be one of {sorted(FORMS)}")
@@ -193,6 +208,10 @@ class Engine:
             self.set_option(OPT_DEBUG_STAGE, debug_stage)
         if profile is not None:
             self.set_option(OPT_PROFILE, int(bool(profile)))
+        if selector is not None:
+            if selector not in SELECTORS:
+                raise ValueError(f"selector must be one of {sorted(SELECTORS)}")
+            self.set_option(OPT_SELECTOR, SELECTORS[selector])
 
     def stats(self) -> dict:
         st = FxStats()

@@ -20,7 +20,9 @@ import numpy as np
 from . import _native
 from ._native import check, lib
 
-OPT_GRAPH, OPT_TIMEOUT_MS, OPT_FORCE_M = 0, 1, 2
+OPT_GRAPH, OPT_TIMEOUT_MS, OPT_FORCE_M, OPT_SELECTOR, OPT_ANALYZE_ONLY = 0, 1, 2, 3, 4
+OUTCOMES = {0: "plain", 1: "certified", 2: "learned", -1: "learned rejected by the bound",
+            -2: "failed an a-posteriori check, redone with the plain (m, s)"}
 
 
 def _check(rc: int, h) -> None:
@@ -45,7 +47,8 @@ def walk_generator(A: np.ndarray, t: float, gamma: float = 1.0, laplacian: bool 
 class WalkBatch:
     """Owner of one ``fx_batch`` handle: device workspace for walks of sizes ``ns``."""
 
-    def __init__(self, ns, dtype=np.complex64, graph: bool = True) -> None:
+    def __init__(self, ns, dtype=np.complex64, graph: bool = True, selector: str = "plain",
+                 analyze_only: bool = False) -> None:
         self.ns = [int(n) for n in ns]
         self.dtype = np.dtype(dtype)
         if self.dtype not in (np.dtype(np.complex64), np.dtype(np.complex128)):
@@ -56,6 +59,10 @@ class WalkBatch:
         self._h = h
         if not graph:
             self.set_option(OPT_GRAPH, 0)
+        if selector != "plain":
+            self.set_option(OPT_SELECTOR, _native.SELECTORS[selector])
+        if analyze_only:
+            self.set_option(OPT_ANALYZE_ONLY, 1)
 
     def set_option(self, key: int, value: float) -> None:
         _check(lib().fx_batch_set_option(self._h, int(key), float(value)), self._h)
@@ -63,11 +70,13 @@ class WalkBatch:
     def _ptrs(self, xs):
         return (ctypes.c_void_p * len(xs))(*[ctypes.c_void_p(x) for x in xs])
 
-    def run(self, Xs, psi0s) -> list[np.ndarray]:
+    def run(self, Xs, psi0s=None) -> list[np.ndarray]:
         """psi_w = expm(X_w) psi0_w for host ndarrays; returns a list of new arrays."""
-        if len(Xs) != len(self.ns) or len(psi0s) != len(self.ns):
+        if len(Xs) != len(self.ns) or (psi0s is not None and len(psi0s) != len(self.ns)):
             raise ValueError(f"expected {len(self.ns)} generators and states")
         xs, p0, p1 = [], [], []
+        if psi0s is None:
+            psi0s = [np.full(n, 1.0 / np.sqrt(n), dtype=self.dtype) for n in self.ns]
         for X, p, n in zip(Xs, psi0s, self.ns):
             X = np.ascontiguousarray(X, dtype=self.dtype)
             if X.shape != (n, n):
@@ -97,6 +106,18 @@ class WalkBatch:
         s = (ctypes.c_int32 * len(self.ns))()
         _check(lib().fx_batch_selection(self._h, m, s), self._h)
         return np.array(m[:], dtype=np.int32), np.array(s[:], dtype=np.int32)
+
+    def details(self) -> dict:
+        """Per walk of the last run: selector features (n x 8), the Al-Mohy & Higham (m, s),
+        the certified (m, s) and the selection outcome (see OUTCOMES)."""
+        W = len(self.ns)
+        f = (ctypes.c_double * (8 * W))()
+        arr = [(ctypes.c_int32 * W)() for _ in range(5)]
+        _check(lib().fx_batch_details(self._h, f, *arr), self._h)
+        out = {"features": np.array(f[:], dtype=np.float64).reshape(W, 8)}
+        for name, a in zip(("plain_m", "plain_s", "cert_m", "cert_s", "outcome"), arr):
+            out[name] = np.array(a[:], dtype=np.int32)
+        return out
 
     def info(self) -> dict:
         """Device time (ms), algorithmic flops and kernel launches of the last run."""

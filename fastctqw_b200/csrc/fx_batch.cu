@@ -60,8 +60,8 @@ __global__ void kb_combo(double* D, Planes4 M, const int* list, const BWalk* wk,
        idx += (int64_t)gridDim.x * blockDim.x) {
     double v = 0.0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (M.m[k]) v += c[k] * M.m[k][b.off + idx];
+    for (int k = 0; k < 4; ++k)   // a zero coefficient skips the term: its plane may be unset
+      if (M.m[k] && c[k] != 0.0) v += c[k] * M.m[k][b.off + idx];
     const int64_t i = idx / b.np;
     if (idx - i * b.np == i) v += c[4];
     D[b.off + idx] = v;
@@ -69,9 +69,11 @@ __global__ void kb_combo(double* D, Planes4 M, const int* list, const BWalk* wk,
 }
 
 // Statistics of the interleaved input of each walk, warp per row i < n:
-// rowstat[kRS * (row0 + i)] = (Re row sum, Im row sum, Re X_ii, Im X_ii, sum |Re| + |Im|);
-// flags[w] |= 1 (Re != 0), 2 (not symmetric), 4 (non-finite).
-constexpr int kRS = 6;
+// rowstat[kRS * (row0 + i)] = (Re row sum, Im row sum, Re X_ii, Im X_ii, sum |Re| + |Im|,
+// sum |X_ij|^2, number of nonzero off-diagonal entries); flags[w] |= 1 (Re != 0),
+// 2 (not symmetric), 4 (non-finite).
+constexpr int kRS = 8;
+constexpr int kWO = 16;   // per-walk record of kb_walk_reduce
 template <typename C>
 __global__ void kb_stats(const void* const* X, const int* list, const BWalk* wk, double* rowstat, int* flags) {
   const int w = list[blockIdx.y];
@@ -81,13 +83,15 @@ __global__ void kb_stats(const void* const* X, const int* list, const BWalk* wk,
   const int wpb = blockDim.x / 32;
   int f = 0;
   for (int64_t i = (int64_t)blockIdx.x * wpb + threadIdx.x / 32; i < b.n; i += (int64_t)gridDim.x * wpb) {
-    double sr = 0, si = 0, sa = 0;
+    double sr = 0, si = 0, sa = 0, sq = 0, nz = 0;
     for (int64_t j = lane; j < b.n; j += 32) {
       const C v = x[i * b.n + j];
       const double vr = (double)v.x, vi = (double)v.y;
       sr += vr;
       si += vi;
       sa += fabs(vr) + fabs(vi);
+      sq += vr * vr + vi * vi;
+      if (j != i && (vr != 0.0 || vi != 0.0)) nz += 1.0;
       if (vr != 0.0) f |= 1;
       if (!isfinite(vr) || !isfinite(vi)) f |= 4;
       if (j > i) {
@@ -100,6 +104,8 @@ __global__ void kb_stats(const void* const* X, const int* list, const BWalk* wk,
       sr += __shfl_xor_sync(0xffffffffu, sr, o);
       si += __shfl_xor_sync(0xffffffffu, si, o);
       sa += __shfl_xor_sync(0xffffffffu, sa, o);
+      sq += __shfl_xor_sync(0xffffffffu, sq, o);
+      nz += __shfl_xor_sync(0xffffffffu, nz, o);
     }
     if (lane == 0) {
       const C d = x[i * b.n + i];
@@ -109,6 +115,8 @@ __global__ void kb_stats(const void* const* X, const int* list, const BWalk* wk,
       r[2] = (double)d.x;
       r[3] = (double)d.y;
       r[4] = sa;
+      r[5] = sq;
+      r[6] = nz;
     }
   }
 #pragma unroll
@@ -119,41 +127,47 @@ __global__ void kb_stats(const void* const* X, const int* list, const BWalk* wk,
 // One CTA per walk: the shifts.  mu = trace / n (ordered sum of the diagonal); the rank-one
 // shift applies when every row sum equals row 0's within the rounding of a sum,
 // 4 n 2^-53 max_i sum_j |X_ij| (the input is exactly symmetric, so the column sums are the
-// same numbers); then nu = c0 - mu.  out[8 w ..] = (mu re, mu im, nu re, nu im, rank1, mu_im,
-// nu_im / n, 0); the last two are the load parameters of kb_load_imag.
+// same numbers); then nu = c0 - mu.  out[kWO w ..] = (mu re, mu im, nu re, nu im, rank1, mu_im,
+// nu_im / n, 0, ||X||_F^2, max off-diagonal nonzeros of a row, max absolute row sum); mu_im and
+// nu_im / n are the load parameters of kb_load_imag.
 __global__ void kb_walk_reduce(const int* list, const BWalk* wk, const double* rowstat, double* out) {
   const int w = list[blockIdx.x];
   const BWalk b = wk[w];
   const double* r = rowstat + kRS * b.row0;
   __shared__ double s_max[256];
   __shared__ double s_dev[256];
+  __shared__ double s_nz[256];
   const double c0r = r[0], c0i = r[1];
-  double mx = 0.0, dev = 0.0;
+  double mx = 0.0, dev = 0.0, nz = 0.0;
   for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
     mx = fmax(mx, r[kRS * i + 4]);
     dev = fmax(dev, fmax(fabs(r[kRS * i] - c0r), fabs(r[kRS * i + 1] - c0i)));
+    nz = fmax(nz, r[kRS * i + 6]);
   }
   s_max[threadIdx.x] = mx;
   s_dev[threadIdx.x] = dev;
+  s_nz[threadIdx.x] = nz;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
     if (threadIdx.x < o) {
       s_max[threadIdx.x] = fmax(s_max[threadIdx.x], s_max[threadIdx.x + o]);
       s_dev[threadIdx.x] = fmax(s_dev[threadIdx.x], s_dev[threadIdx.x + o]);
+      s_nz[threadIdx.x] = fmax(s_nz[threadIdx.x], s_nz[threadIdx.x + o]);
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    double tr = 0, ti = 0;
+    double tr = 0, ti = 0, fro2 = 0;
     for (int i = 0; i < b.n; ++i) {
       tr += r[kRS * i + 2];
       ti += r[kRS * i + 3];
+      fro2 += r[kRS * i + 5];
     }
     const double n = b.n;
     const double mur = tr / n, mui = ti / n;
     const bool rank1 = b.n > 1 && s_dev[0] <= 4.0 * n * 0x1p-53 * s_max[0];
     const double nur = rank1 ? c0r - mur : 0.0, nui = rank1 ? c0i - mui : 0.0;
-    double* o = out + 8 * w;
+    double* o = out + kWO * w;
     o[0] = mur;
     o[1] = mui;
     o[2] = nur;
@@ -162,18 +176,21 @@ __global__ void kb_walk_reduce(const int* list, const BWalk* wk, const double* r
     o[5] = mui;
     o[6] = nui / n;
     o[7] = 0.0;
+    o[8] = fro2;
+    o[9] = s_nz[0];
+    o[10] = s_max[0];
   }
 }
 
 // Y = Im(X) - mu_im I - nu_im/n J on the n x n block, 0 in the padding (imaginary plane of the
-// shifted generator; its real plane is zero for X = i*(real symmetric)).  sh[8 w + 5, 6] =
+// shifted generator; its real plane is zero for X = i*(real symmetric)).  sh[kWO w + 5, 6] =
 // (mu_im, nu_im/n) as written by kb_walk_reduce.
 template <typename C>
 __global__ void kb_load_imag(const void* const* X, const int* list, const BWalk* wk, const double* sh, double* Y) {
   const int w = list[blockIdx.y];
   const BWalk b = wk[w];
   const C* x = (const C*)X[w];
-  const double mu = sh[8 * w + 5], nun = sh[8 * w + 6];
+  const double mu = sh[kWO * w + 5], nun = sh[kWO * w + 6];
   const int64_t n2 = (int64_t)b.np * b.np;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -339,6 +356,37 @@ __global__ void kb_apply(const double* const* Ere, const double* const* Eim, con
     }
   }
 }
+// nrm[2 w .. 2 w + 1] = (||psi0_w||^2, ||psi_w||^2): the unitarity residual of the result on the
+// walk's own state (one CTA per walk).
+template <typename C>
+__global__ void kb_psi_norms(const void* const* psi0, void* const* psi, const int* list, const BWalk* wk,
+                             double* nrm) {
+  const int w = list[blockIdx.x];
+  const C* a = (const C*)psi0[w];
+  const C* b = (const C*)psi[w];
+  __shared__ double sa[256], sb[256];
+  double xa = 0, xb = 0;
+  if (a && b)
+    for (int j = threadIdx.x; j < wk[w].n; j += blockDim.x) {
+      xa += (double)a[j].x * a[j].x + (double)a[j].y * a[j].y;
+      xb += (double)b[j].x * b[j].x + (double)b[j].y * b[j].y;
+    }
+  sa[threadIdx.x] = xa;
+  sb[threadIdx.x] = xb;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sa[threadIdx.x] += sa[threadIdx.x + o];
+      sb[threadIdx.x] += sb[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    nrm[2 * w] = sa[0];
+    nrm[2 * w + 1] = sb[0];
+  }
+}
+
 // psum[w] = sum_j psi0_w[j] (ordered, one thread).
 template <typename C>
 __global__ void kb_psi_sum(const void* const* psi0, const int* list, const BWalk* wk, double* psum) {
@@ -599,6 +647,53 @@ std::vector<double> pade_coeffs(int m) {
 }
 int pade_products(int m) { return m == 3 ? 2 : m == 5 ? 3 : m == 7 ? 4 : m == 9 ? 5 : 6; }
 
+// ---- certified truncation bound for normal generators Y = i B (B real symmetric).
+// The [m/m] Pade approximant maps the imaginary axis onto the unit circle, r_m(ix) =
+// p_m(ix) / conj(p_m(ix)), so its only error at an eigenvalue i lambda is the phase
+// phi_m(x) = 2 arg p_m(ix) - x, x = lambda / 2^s, and after s squarings 2^s phi_m(x).  |phi_m| is
+// increasing in |x| until the phase wraps (|phi| = pi near x = 10, 14.4, 18.7, 23, 31.4 for
+// m = 3..13); below half that point the error over every |lambda| <= rho is at most
+// 2^s |phi_m(rho / 2^s)|.  rho_up = min(||Y||_1, d4, d6) bounds the spectral radius (exact
+// norms of powers), so the bound holds for every eigenvalue.
+const int kDegrees[5] = {3, 5, 7, 9, 13};
+double pade_phase_error(int m, double x) {
+  const std::vector<double> b = pade_coeffs(m);
+  const std::complex<double> z(0.0, x);
+  std::complex<double> acc(0.0, 0.0);
+  for (int j = m; j >= 0; --j) acc = acc * z + b[j];
+  return std::remainder(2.0 * std::atan2(acc.imag(), acc.real()) - x, 2.0 * M_PI);
+}
+double pade_x_limit(int m) { return m == 3 ? 5.0 : m == 5 ? 7.2 : m == 7 ? 9.3 : m == 9 ? 11.4 : 15.6; }
+bool certified(int m, int s, double rho_up, double tol) {
+  const double x = std::ldexp(rho_up, -s);
+  if (x > pade_x_limit(m)) return false;
+  return std::ldexp(std::fabs(pade_phase_error(m, x)), s) <= tol;
+}
+// Cheapest (m, s) (products pi_m + s; ties to the larger m) that the bound certifies.
+void certified_choice(double rho_up, double tol, int* m_out, int* s_out) {
+  int bm = 13, bs = 0, best = 1 << 30;
+  for (int m : kDegrees) {
+    int s = 0;
+    while (s < 200 && !certified(m, s, rho_up, tol)) ++s;
+    const int cost = pade_products(m) + s;
+    if (cost <= best) {
+      best = cost;
+      bm = m;
+      bs = s;
+    }
+  }
+  *m_out = bm;
+  *s_out = bs;
+}
+// Phase tolerance of the certified and learned selections: 1e-6 per eigenvalue keeps the
+// infidelity of any state below 1e-12 and the relative error of U below 1e-6.
+constexpr double kPhaseTol = 1e-6;
+
+// Process-wide weights of the learned selector (device copy; fx_selector_set_weights).
+std::mutex g_sel_mu;
+float* g_sel_weights = nullptr;
+int g_sel_device = -1;
+
 struct DevArena {
   void* p = nullptr;
   size_t bytes = 0;
@@ -668,7 +763,7 @@ class BatchPipeline {
     linv_.alloc(sizeof(double) * (size_t)rows_ * kNb * 2);
     // small: rowstat (kRS per row), estimator vectors (kEstScratch per row), row sums (1 per
     // row), per-walk records (8 + 8 + 4 + 8 + W ints)
-    small_.alloc(sizeof(double) * (size_t)(rows_ * (kRS + kEstScratch + 1) + 32 * W + 64));
+    small_.alloc(sizeof(double) * (size_t)(rows_ * (kRS + kEstScratch + 1) + (kWO + 8 + 4 + 8 + 8) * W + 64));
     err_.alloc(sizeof(int) * 8);
     d_walks_.alloc(sizeof(BWalk) * W);
     FX_CUDA(cudaMemcpy(d_walks_.p, walks_.data(), sizeof(BWalk) * W, cudaMemcpyHostToDevice));
@@ -697,6 +792,19 @@ class BatchPipeline {
   void set_graph(bool g) { use_graph_ = g; }
   void set_timeout(unsigned ms) { timeout_ms_ = ms; }
   void set_profile(bool p) { profile_ = p; }
+  // 0 plain (Al-Mohy & Higham), 1 certified bound, 2 learned (gated by the bound).
+  void set_selector(int k) { selector_ = k; }
+  // Stop after the selection (statistics, norms, estimates, features; no exponential).
+  void set_analyze_only(bool a) { analyze_only_ = a; }
+  int selector() const { return selector_; }
+  void details(int w, double* feat, int* pm, int* ps, int* cm, int* cs, int* outcome) const {
+    for (int k = 0; k < 8; ++k) feat[k] = features_.empty() ? 0.0 : features_[8 * w + k];
+    *pm = plain_m_.empty() ? 0 : plain_m_[w];
+    *ps = plain_s_.empty() ? 0 : plain_s_[w];
+    *cm = cert_m_.empty() ? 0 : cert_m_[w];
+    *cs = cert_s_.empty() ? 0 : cert_s_[w];
+    *outcome = outcome_.empty() ? 0 : outcome_[w];
+  }
   // Per walk: ||Y||_1, d4, d6, d8, d10 and the shift flags of the last run.
   void walk_stats(int w, fx_stats* st) const {
     st->m = sel_m_[w];
@@ -739,9 +847,10 @@ class BatchPipeline {
 
     // ---- phase 1: statistics and shifts, powers, exact norms, estimates (one host round trip)
     run_recorded(desc1_, st1_, r1_, graph1_, use_graph_ && !profile_);
-    std::vector<double> h_wo(8 * W);
+    std::vector<double>& h_wo = walkrec_;
+    h_wo.assign(kWO * W, 0.0);
     std::vector<int> h_flags(W);
-    FX_CUDA(cudaMemcpyAsync(h_wo.data(), walkout(), sizeof(double) * 8 * W, cudaMemcpyDeviceToHost, s));
+    FX_CUDA(cudaMemcpyAsync(h_wo.data(), walkout(), sizeof(double) * kWO * W, cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaMemcpyAsync(h_flags.data(), flags(), sizeof(int) * W, cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaMemcpyAsync(norms_.data(), norms(), sizeof(double) * 8 * W, cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaStreamSynchronize(s));
@@ -751,13 +860,21 @@ class BatchPipeline {
       if (h_flags[w] & 3)
         throw Error{FX_ERR_VALUE, "batched walks need generators X = i*(real symmetric); input " +
                                       std::to_string(w) + " is not"};
-      mu_[w] = std::complex<double>(h_wo[8 * w], h_wo[8 * w + 1]);
-      nu_[w] = std::complex<double>(h_wo[8 * w + 2], h_wo[8 * w + 3]);
-      rank1_[w] = h_wo[8 * w + 4] != 0.0;
+      mu_[w] = std::complex<double>(h_wo[kWO * w], h_wo[kWO * w + 1]);
+      nu_[w] = std::complex<double>(h_wo[kWO * w + 2], h_wo[kWO * w + 3]);
+      rank1_[w] = h_wo[kWO * w + 4] != 0.0;
     }
 
-    // ---- selection (m, s) per walk: Al-Mohy & Higham (2009) Alg. 6.1, normal input (l = 0)
+    // ---- selection (m, s) per walk: Al-Mohy & Higham (2009) Alg. 6.1, normal input (l = 0),
+    // then optionally the certified or the learned selection (both gated by the certified
+    // truncation bound; the plain choice is the fallback).
     flops_ = 0;
+    plain_m_.assign(W, 13);
+    plain_s_.assign(W, 0);
+    cert_m_.assign(W, 13);
+    cert_s_.assign(W, 0);
+    outcome_.assign(W, 0);
+    features_.assign(8 * W, 0.0);
     for (int w = 0; w < W; ++w) {
       const double* nw = norms_.data() + 8 * w;
       const double anorm = nw[0], d4 = std::pow(nw[1], 0.25), d6 = std::pow(nw[2], 1.0 / 6);
@@ -781,18 +898,116 @@ class BatchPipeline {
           sq = eta5 == 0.0 ? 0 : std::max((int)std::ceil(std::log2(eta5 / kTheta13)), 0);
         }
       }
+      if (m != 13) sq = 0;
+      plain_m_[w] = m;
+      plain_s_[w] = sq;
+      const double rho_up = std::min(anorm, std::min(d4, d6));
+      certified_choice(rho_up, kPhaseTol, &cert_m_[w], &cert_s_[w]);
+      // features of the learned selection
+      const double n = walks_[w].n;
+      const double* rec = walkrec_.data() + kWO * w;
+      double* f = features_.data() + 8 * w;
+      f[0] = std::log2(n);
+      f[1] = std::log2(anorm + 1e-300);
+      f[2] = std::log2(std::sqrt(rec[8] / n) + 1e-300);
+      f[3] = std::log2(1.0 + rec[9]);
+      f[4] = std::log2(1.0 + std::abs(mu_[w]));
+      f[5] = rank1_[w] ? 1.0 : 0.0;
+      f[6] = std::log2(d4 + 1e-300);
+      f[7] = std::log2(d6 + 1e-300);
+    }
+    std::vector<float> prop;
+    if (selector_ == 2) prop = infer_proposals();
+    for (int w = 0; w < W; ++w) {
+      int m = plain_m_[w], sq = plain_s_[w];
+      const double* nw = norms_.data() + 8 * w;
+      const double rho_up = std::min(nw[0], std::min(std::pow(nw[1], 0.25), std::pow(nw[2], 1.0 / 6)));
+      if (selector_ == 1 && pade_products(cert_m_[w]) + cert_s_[w] < pade_products(m) + sq) {
+        m = cert_m_[w];
+        sq = cert_s_[w];
+        outcome_[w] = 1;
+      } else if (selector_ == 2) {
+        const float* o = prop.data() + 6 * w;
+        int c = 0;
+        for (int k = 1; k < 5; ++k)
+          if (o[k] > o[c]) c = k;
+        const int pm = kDegrees[c];
+        const int ps = std::max(0, (int)std::lround(o[5]));
+        if (pade_products(pm) + ps < pade_products(m) + sq) {
+          if (certified(pm, ps, rho_up, kPhaseTol)) {
+            m = pm;
+            sq = ps;
+            outcome_[w] = 2;
+          } else {
+            outcome_[w] = -1;   // rejected by the bound: plain (m, s)
+          }
+        }
+      }
       if (force_m_ > 0) m = force_m_;
       if (force_s_ >= 0 && m == 13) sq = force_s_;
-      if (m != 13) sq = 0;
+      if (m != 13 && force_s_ < 0 && outcome_[w] <= 0) sq = 0;
       sel_m_[w] = m;
       sel_s_[w] = sq;
       const double N3 = (double)walks_[w].n * walks_[w].n * walks_[w].n;
       flops_ += 8.0 * N3 * (pade_products(m) + sq) + (8.0 / 3.0) * N3 + 8.0 * N3;
     }
+    if (analyze_only_) return;
 
-    // ---- phase 2: Pade, solve, squarings, outputs.  The recorded launch sequence (and its
-    // CUDA graph) depends only on the sizes, (m, s), the shifts and which outputs are wanted;
-    // it is rebuilt only when one of those changed since the last run.
+    // ---- phase 2, then the a-posteriori checks of the non-plain selections: a walk whose
+    // Pade denominator fails to factor, or whose state loses its norm, is redone alone with the
+    // plain (m, s) in a pipeline of its own (its outputs are overwritten; the other walks keep
+    // theirs).  A failure under the plain choice is an error.
+    FX_CUDA(cudaMemsetAsync(walk_err(), 0, sizeof(int) * W, s));
+    run_phase2(tab);
+    std::vector<int> werr(W), own(W, 0);
+    int herr = 0;
+    FX_CUDA(cudaMemcpyAsync(werr.data(), walk_err(), sizeof(int) * W, cudaMemcpyDeviceToHost, s));
+    FX_CUDA(cudaMemcpyAsync(&herr, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FX_CUDA(cudaStreamSynchronize(s));
+    bool any = false;
+    for (int w = 0; w < W; ++w) {
+      if (!werr[w]) continue;
+      if (outcome_[w] <= 0) throw Error{FX_ERR_SINGULAR, "Pade denominator is not positive definite (walk " + std::to_string(w) + ")"};
+      own[w] = 1;
+      any = true;
+    }
+    any = verify_states(tab, own) || any;
+    if (any) {
+      if (herr & kDevTimeout) throw Error{FX_ERR_TIMEOUT, "a device-side wait timed out"};
+      FX_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int) * 8, s));
+      std::vector<int> redo;
+      for (int w = 0; w < W; ++w)
+        if (own[w]) redo.push_back(w);
+      std::vector<int64_t> ns;
+      std::vector<const void*> x, p0;
+      std::vector<void*> p1, u;
+      for (int w : redo) {
+        ns.push_back(walks_[w].n);
+        x.push_back(tab[w]);
+        p0.push_back(tab[W + w]);
+        p1.push_back((void*)tab[2 * W + w]);
+        u.push_back((void*)tab[3 * W + w]);
+      }
+      BatchPipeline sub(ns, dtype_);
+      sub.set_timeout(timeout_ms_);
+      sub.run(x.data(), p0.data(), p1.data(), u.data(), s);
+      launches_ += sub.launches();
+      for (size_t i = 0; i < redo.size(); ++i) {
+        const int w = redo[i];
+        outcome_[w] = -2;
+        sub.selection((int)i, &sel_m_[w], &sel_s_[w]);
+      }
+    }
+    FX_CUDA(cudaStreamSynchronize(s));
+    check_err();
+    prof_collect();
+  }
+
+  // Phase 2: Pade, solve, squarings, outputs.  The recorded launch sequence (and its CUDA graph)
+  // depends only on the sizes, (m, s), the shifts and which outputs are wanted; it is rebuilt
+  // only when one of those changed since the last run.
+  void run_phase2(const std::vector<const void*>& tab) {
+    const int W = count();
     std::vector<double> key;
     for (int w = 0; w < W; ++w) {
       key.insert(key.end(), {(double)sel_m_[w], (double)sel_s_[w], (double)rank1_[w], mu_[w].real(),
@@ -808,13 +1023,41 @@ class BatchPipeline {
       }
       record_rest(st2_, r2_);
       desc2_.alloc(std::max<size_t>(st2_.buf.size(), 256));
-      FX_CUDA(cudaMemcpyAsync(desc2_.p, st2_.buf.data(), st2_.buf.size(), cudaMemcpyHostToDevice, s));
+      FX_CUDA(cudaMemcpyAsync(desc2_.p, st2_.buf.data(), st2_.buf.size(), cudaMemcpyHostToDevice, stream_));
       key2_ = profile_ ? std::vector<double>() : key;
     }
     run_recorded(desc2_, st2_, r2_, graph2_, use_graph_ && !profile_, false);
-    FX_CUDA(cudaStreamSynchronize(s));
-    check_err();
-    prof_collect();
+  }
+
+  // A-posteriori unitarity check of the walks that did not take the plain (m, s): ||psi|| must
+  // equal ||psi0|| to 1e-6 (U is unitary in exact arithmetic whatever (m, s)).  Returns true
+  // when a walk failed.
+  bool verify_states(const std::vector<const void*>& tab, std::vector<int>& own) {
+    const int W = count();
+    std::vector<int> list;
+    for (int w = 0; w < W; ++w)
+      if (outcome_[w] > 0 && tab[W + w] && tab[2 * W + w]) list.push_back(w);
+    if (list.empty()) return false;
+    const size_t need = sizeof(double) * 2 * W + sizeof(int) * list.size() + 64;
+    if (ver_io_.bytes < need) ver_io_.alloc(need);
+    double* nrm = (double*)ver_io_.p;
+    int* dl = (int*)(nrm + 2 * W);
+    FX_CUDA(cudaMemcpyAsync(dl, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, stream_));
+    if (dtype_ == FX_C64)
+      kb_psi_norms<float2><<<(unsigned)list.size(), 256, 0, stream_>>>(dP0(), dP1(), dl, (const BWalk*)d_walks_.p, nrm);
+    else
+      kb_psi_norms<double2><<<(unsigned)list.size(), 256, 0, stream_>>>(dP0(), dP1(), dl, (const BWalk*)d_walks_.p, nrm);
+    FX_LAUNCH_CHECK();
+    ++launches_;
+    std::vector<double> h(2 * W);
+    FX_CUDA(cudaMemcpyAsync(h.data(), nrm, sizeof(double) * 2 * W, cudaMemcpyDeviceToHost, stream_));
+    FX_CUDA(cudaStreamSynchronize(stream_));
+    bool bad = false;
+    for (int w : list) {
+      const double a = std::sqrt(h[2 * w]), b = std::sqrt(h[2 * w + 1]);
+      if (!(std::fabs(b - a) <= 1e-6 * a)) own[w] = 1, bad = true;
+    }
+    return bad;
   }
 
  private:
@@ -835,6 +1078,12 @@ class BatchPipeline {
   std::vector<int> sel_m_, sel_s_, rank1_;
   std::vector<std::complex<double>> mu_, nu_;
   std::vector<double> norms_;
+  std::vector<double> walkrec_;
+  std::vector<int> plain_m_, plain_s_, cert_m_, cert_s_, outcome_;
+  std::vector<double> features_;
+  int selector_ = 0;
+  bool analyze_only_ = false;
+  DevArena sel_io_, ver_io_;
   cudaStream_t stream_ = nullptr;
   unsigned timeout_ms_ = 2000;
   bool use_graph_ = true, profile_ = false;
@@ -862,10 +1111,11 @@ class BatchPipeline {
   double* est_scr() const { return rowstat() + kRS * rows_; }
   double* rsum() const { return est_scr() + kEstScratch * rows_; }
   double* walkout() const { return rsum() + rows_; }
-  double* norms() const { return walkout() + 8 * count(); }
+  double* norms() const { return walkout() + kWO * count(); }
   double* estst() const { return norms() + 8 * count(); }
   double* misc() const { return estst() + 4 * count(); }   // 8 per walk: psum, projection totals
   int* flags() const { return (int*)(misc() + 8 * count()); }
+  int* walk_err() const { return flags() + count(); }   // per walk: Cholesky of G failed
   const void* const* dX() const { return (const void* const*)ptrs_.p; }
   const void* const* dP0() const { return dX() + count(); }
   void* const* dP1() const { return (void* const*)(dX() + 2 * count()); }
@@ -892,6 +1142,31 @@ class BatchPipeline {
     FX_CUDA(cudaMemcpy(&h, err_.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (h & kDevTimeout) throw Error{FX_ERR_TIMEOUT, "a device-side wait timed out"};
     if (h & kDevSingular) throw Error{FX_ERR_SINGULAR, "Pade denominator is not positive definite"};
+  }
+
+  // MLP proposals for every walk (6 floats each: 5 logits, s), from the process-wide weights.
+  std::vector<float> infer_proposals() {
+    const int W = count();
+    float* wts = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(g_sel_mu);
+      int dev = -1;
+      FX_CUDA(cudaGetDevice(&dev));
+      if (!g_sel_weights || g_sel_device != dev)
+        throw Error{FX_ERR_VALUE, "learned selection needs weights on this device (fx_selector_set_weights)"};
+      wts = g_sel_weights;
+    }
+    if (sel_io_.bytes < sizeof(float) * 14 * (size_t)W) sel_io_.alloc(sizeof(float) * 14 * (size_t)W);
+    std::vector<float> fx(8 * W), out(6 * W);
+    for (int i = 0; i < 8 * W; ++i) fx[i] = (float)features_[i];
+    float* dfx = (float*)sel_io_.p;
+    float* dout = dfx + 8 * W;
+    FX_CUDA(cudaMemcpyAsync(dfx, fx.data(), sizeof(float) * 8 * W, cudaMemcpyHostToDevice, stream_));
+    launch_mlp_infer(wts, dfx, W, dout, stream_);
+    ++launches_;
+    FX_CUDA(cudaMemcpyAsync(out.data(), dout, sizeof(float) * 6 * W, cudaMemcpyDeviceToHost, stream_));
+    FX_CUDA(cudaStreamSynchronize(stream_));
+    return out;
   }
 
   void prof_reset() {
@@ -1252,11 +1527,13 @@ class BatchPipeline {
     for (int w = 0; w < W; ++w) {
       const int m = sel_m_[w];
       const auto b = pade_coeffs(m);
+      // powers of the scaled generator Y / 2^s: A_k -> 2^(-k s) A_k (s = 0 for the plain
+      // choice of m < 13; the certified and learned choices may scale any degree)
       if (m == 13) cf[w] = {1.0, b[7] * cs(w, 6), b[5] * cs(w, 4), b[3] * cs(w, 2), b[1]};
-      else if (m == 9) cf[w] = {b[9], b[7], b[5], b[3], b[1]};
-      else if (m == 7) cf[w] = {0.0, b[7], b[5], b[3], b[1]};
-      else if (m == 5) cf[w] = {0.0, 0.0, b[5], b[3], b[1]};
-      else cf[w] = {0.0, 0.0, 0.0, b[3], b[1]};
+      else if (m == 9) cf[w] = {b[9] * cs(w, 8), b[7] * cs(w, 6), b[5] * cs(w, 4), b[3] * cs(w, 2), b[1]};
+      else if (m == 7) cf[w] = {0.0, b[7] * cs(w, 6), b[5] * cs(w, 4), b[3] * cs(w, 2), b[1]};
+      else if (m == 5) cf[w] = {0.0, 0.0, b[5] * cs(w, 4), b[3] * cs(w, 2), b[1]};
+      else cf[w] = {0.0, 0.0, 0.0, b[3] * cs(w, 2), b[1]};
       al[w] = cs(w, 1);
     }
     combo(st, r, all, kT1, m_t2642, cf);
@@ -1276,10 +1553,10 @@ class BatchPipeline {
     for (int w : mlt13) {
       const int m = sel_m_[w];
       const auto b = pade_coeffs(m);
-      if (m == 9) cf[w] = {b[8], b[6], b[4], b[2], b[0]};
-      else if (m == 7) cf[w] = {0.0, b[6], b[4], b[2], b[0]};
-      else if (m == 5) cf[w] = {0.0, 0.0, b[4], b[2], b[0]};
-      else cf[w] = {0.0, 0.0, 0.0, b[2], b[0]};
+      if (m == 9) cf[w] = {b[8] * cs(w, 8), b[6] * cs(w, 6), b[4] * cs(w, 4), b[2] * cs(w, 2), b[0]};
+      else if (m == 7) cf[w] = {0.0, b[6] * cs(w, 6), b[4] * cs(w, 4), b[2] * cs(w, 2), b[0]};
+      else if (m == 5) cf[w] = {0.0, 0.0, b[4] * cs(w, 4), b[2] * cs(w, 2), b[0]};
+      else cf[w] = {0.0, 0.0, 0.0, b[2] * cs(w, 2), b[0]};
     }
     combo(st, r, mlt13, kV, m_t2642, cf);
     product(st, r, m13, kA6, kT1, 1.0, kT2, 1.0, 0.0, kV, true, &al, &ga);
@@ -1509,7 +1786,7 @@ class BatchPipeline {
         if (b.np <= j * kNb) continue;
         double* G = A(g) + b.off;
         const int64_t k0 = (int64_t)j * kNb;
-        jobs.push_back(GChol{G, b.np, k0, kNb, 0, linv(w) + k0 * kNb, linvT(w) + k0 * kNb});
+        jobs.push_back(GChol{G, b.np, k0, kNb, w, linv(w) + k0 * kNb, linvT(w) + k0 * kNb});
         const int rest = b.np - (j + 1) * kNb;
         if (rest <= 0) continue;
         double* G21 = G + (k0 + kNb) * b.np + k0;
@@ -1542,7 +1819,7 @@ class BatchPipeline {
       const size_t o_j = st.put(jobs);
       const int nj = (int)jobs.size();
       r.launches += 1;
-      r.ops.push_back([=]() { launch_potrf_inv_grouped<double>(dev<GChol>(o_j), nj, (int*)err_.p, stream_); });
+      r.ops.push_back([=]() { launch_potrf_inv_grouped<double>(dev<GChol>(o_j), nj, (int*)err_.p, walk_err(), stream_); });
       if (p21.empty()) continue;
       grouped(st, r, sa21, &sb_l, p21, false, 0);
       // the updated G21 (= L21) is both factors of the trailing update
@@ -1642,7 +1919,8 @@ class BatchPipeline {
 BatchPipeline* batch_pipeline_create(int64_t n, int dtype) { return new BatchPipeline({n}, dtype); }
 void batch_pipeline_destroy(BatchPipeline* p) { delete p; }
 void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU, bool profile,
-                        unsigned timeout_ms, cudaStream_t s) {
+                        unsigned timeout_ms, int selector, cudaStream_t s) {
+  p->set_selector(selector);
   const void* x[1] = {dX};
   const void* p0[1] = {dpsi0};
   void* p1[1] = {dpsi};
@@ -1653,6 +1931,13 @@ void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, voi
 }
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st) {
   p->walk_stats(0, st);
+  double f[8];
+  int pm, ps, cm, cs, oc;
+  p->details(0, f, &pm, &ps, &cm, &cs, &oc);
+  st->selector = p->selector();
+  st->sel_outcome = oc;
+  st->plain_m = pm;
+  st->plain_s = ps;
   st->gemm_launches = p->gemm_launches();
   st->launches = p->launches();
   st->flops = p->flops();
@@ -1745,6 +2030,12 @@ int fx_batch_set_option(fx_batch_handle b, int key, double value) {
       b->p->set_timeout((unsigned)value);
       return FX_OK;
     case FX_BATCH_OPT_FORCE_M: b->p->force((int)value, -1); return FX_OK;
+    case FX_BATCH_OPT_SELECTOR:
+      if (value != 0 && value != 1 && value != 2)
+        return bfail(b, fx::Error{FX_ERR_VALUE, "selector must be 0 (plain), 1 (certified) or 2 (learned)"});
+      b->p->set_selector((int)value);
+      return FX_OK;
+    case FX_BATCH_OPT_ANALYZE_ONLY: b->p->set_analyze_only(value != 0.0); return FX_OK;
   }
   return bfail(b, fx::Error{FX_ERR_VALUE, "unknown batch option"});
 }
@@ -1804,6 +2095,42 @@ int fx_batch_info(fx_batch_handle b, double* ms, double* flops, int32_t* launche
   if (ms) *ms = b->ms;
   if (flops) *flops = b->p->flops();
   if (launches) *launches = b->p->launches();
+  return FX_OK;
+}
+
+int fx_batch_details(fx_batch_handle b, double* features, int32_t* plain_m, int32_t* plain_s, int32_t* cert_m,
+                     int32_t* cert_s, int32_t* outcome) {
+  if (!b || !features || !plain_m || !plain_s || !cert_m || !cert_s || !outcome)
+    return bfail(b, fx::Error{FX_ERR_VALUE, "null argument"});
+  for (int w = 0; w < b->p->count(); ++w) {
+    int pm, ps, cm, cs, oc;
+    b->p->details(w, features + 8 * w, &pm, &ps, &cm, &cs, &oc);
+    plain_m[w] = pm;
+    plain_s[w] = ps;
+    cert_m[w] = cm;
+    cert_s[w] = cs;
+    outcome[w] = oc;
+  }
+  return FX_OK;
+}
+
+int fx_selector_set_weights(const float* w, int64_t n) {
+  try {
+    if (!w || n != fx_mlp_param_count())
+      throw fx::Error{FX_ERR_VALUE, "selector weights: expected " + std::to_string(fx_mlp_param_count()) + " floats"};
+    std::lock_guard<std::mutex> lk(fx::g_sel_mu);
+    int dev = -1;
+    FX_CUDA(cudaGetDevice(&dev));
+    if (fx::g_sel_weights && fx::g_sel_device != dev) {
+      cudaFree(fx::g_sel_weights);
+      fx::g_sel_weights = nullptr;
+    }
+    if (!fx::g_sel_weights) FX_CUDA(cudaMalloc((void**)&fx::g_sel_weights, sizeof(float) * n));
+    fx::g_sel_device = dev;
+    FX_CUDA(cudaMemcpy(fx::g_sel_weights, w, sizeof(float) * n, cudaMemcpyHostToDevice));
+  } catch (const fx::Error& e) {
+    return bfail(nullptr, e);
+  }
   return FX_OK;
 }
 

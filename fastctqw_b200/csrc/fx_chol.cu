@@ -26,7 +26,7 @@ namespace {
 //   strict upper triangle, X_ic -> a[c][i].
 template <typename T>
 __device__ __forceinline__ void potrf_inv_block(T* G, int64_t ld, int64_t k0, int nb, T* Linv, T* LinvT,
-                                                int* err) {
+                                                int* err, int* own_err = nullptr) {
   extern __shared__ unsigned char smem_raw[];
   const int sld = nb + 1;
   T* a = reinterpret_cast<T*>(smem_raw);   // nb x sld
@@ -42,7 +42,10 @@ __device__ __forceinline__ void potrf_inv_block(T* G, int64_t ld, int64_t k0, in
   for (int j = 0; j < nb; ++j) {
     const T d = a[j * sld + j];
     if (!(d > (T)0)) {
-      if (tid == 0) atomicOr(err, kDevSingular);
+      if (tid == 0) {
+        atomicOr(err, kDevSingular);
+        if (own_err) *own_err = 1;
+      }
       s_bad = 1;
       break;
     }
@@ -111,9 +114,9 @@ __global__ void __launch_bounds__(1024) k_potrf_inv(T* G, int64_t ld, int64_t k0
 
 // One CTA per job: the same block factorisation for many independent matrices.
 template <typename T>
-__global__ void __launch_bounds__(1024) k_potrf_inv_grouped(const GChol* jobs, int* err) {
+__global__ void __launch_bounds__(1024) k_potrf_inv_grouped(const GChol* jobs, int* err, int* job_err) {
   const GChol j = jobs[blockIdx.x];
-  potrf_inv_block<T>((T*)j.G, j.ld, j.k0, j.nb, (T*)j.Linv, (T*)j.LinvT, err);
+  potrf_inv_block<T>((T*)j.G, j.ld, j.k0, j.nb, (T*)j.Linv, (T*)j.LinvT, err, job_err ? job_err + j.tag : nullptr);
 }
 
 }  // namespace
@@ -128,14 +131,14 @@ void prepare_potrf_inv_grouped() {
 }
 
 template <typename T>
-void launch_potrf_inv_grouped(const GChol* jobs, int njobs, int* err, cudaStream_t s) {
+void launch_potrf_inv_grouped(const GChol* jobs, int njobs, int* err, int* job_err, cudaStream_t s) {
   if (njobs <= 0) return;
   const size_t sm = sizeof(T) * ((size_t)128 * 129 + 128);
   prepare_potrf_inv_grouped();
-  k_potrf_inv_grouped<T><<<njobs, 1024, sm, s>>>(jobs, err);
+  k_potrf_inv_grouped<T><<<njobs, 1024, sm, s>>>(jobs, err, job_err);
   FX_LAUNCH_CHECK();
 }
-template void launch_potrf_inv_grouped<double>(const GChol*, int, int*, cudaStream_t);
+template void launch_potrf_inv_grouped<double>(const GChol*, int, int*, int*, cudaStream_t);
 
 template <typename T>
 void launch_potrf_inv(T* G, int64_t ld, int64_t k0, int nb, T* Linv, T* LinvT, int* err, cudaStream_t s) {

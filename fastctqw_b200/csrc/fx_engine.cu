@@ -87,6 +87,7 @@ struct RunOpts {
   int ipe;
   int debug_stage;   // 0: normal output; k > 0: output an intermediate (diagnostics)
   int profile;       // 1: time every int8 product launch with CUDA events
+  int selector;      // (m, s) selection of the grouped path: 0 plain, 1 certified, 2 learned
 };
 
 // Planar complex matrix view over owned storage; a missing plane is identically zero.
@@ -1039,7 +1040,7 @@ struct fx_engine {
   size_t elem = 8;
   fx::BatchPipeline* grouped = nullptr;   // grouped pipeline for walk generators (lazy)
   void* check_buf = nullptr;              // input statistics of the routing check
-  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0};
+  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0, 0};
   fx_stats stats{};
   std::string last_error;
 };
@@ -1123,7 +1124,8 @@ void run_device(fx_handle h, const void* dA, void* dU, const void* dpsi0, void* 
   if (grouped_eligible(h) && fx_device_ok() && input_is_walk_generator(h, dA, s)) {
     if (!h->grouped) h->grouped = fx::batch_pipeline_create(h->n, h->dtype);
     FX_CUDA(cudaEventRecord(h->ev0, s));
-    fx::batch_pipeline_run(h->grouped, dA, dpsi0, dpsi, dU, h->opts.profile != 0, h->opts.timeout_ms, s);
+    fx::batch_pipeline_run(h->grouped, dA, dpsi0, dpsi, dU, h->opts.profile != 0, h->opts.timeout_ms,
+                           h->opts.selector, s);
     FX_CUDA(cudaEventRecord(h->ev1, s));
     FX_CUDA(cudaEventSynchronize(h->ev1));
     float ms = 0;
@@ -1269,6 +1271,10 @@ int fx_set_option(fx_handle h, int key, double value) {
     case FX_OPT_REFINE: return v == 0 ? FX_OK : fail(h, fx::Error{FX_ERR_VALUE, "refinement not available"});
     case FX_OPT_DEBUG_STAGE: h->opts.debug_stage = v; return FX_OK;
     case FX_OPT_PROFILE: h->opts.profile = v != 0; return FX_OK;
+    case FX_OPT_SELECTOR:
+      if (v < 0 || v > 2) return fail(h, fx::Error{FX_ERR_VALUE, "selector must be 0, 1 or 2"});
+      h->opts.selector = v;
+      return FX_OK;
   }
   return fail(h, fx::Error{FX_ERR_VALUE, "unknown option"});
 }

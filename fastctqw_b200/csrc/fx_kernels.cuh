@@ -192,15 +192,17 @@ void launch_gemm_i8(int S, int64_t M, int64_t N, int64_t K, const I8Term* terms,
                     double beta, const TO* C, int64_t ldc, double gamma, TO* D, int64_t ldd, bool sym,
                     int* err, unsigned timeout_ms, cudaStream_t s);
 // Grouped Cholesky block step: one job per matrix (nb <= 128; every job's block is nb wide).
+// A block that is not positive definite sets kDevSingular in err and, when job_err is given,
+// job_err[tag] = 1.
 struct GChol {
   void* G;
   int64_t ld, k0;
-  int nb, pad;
+  int nb, tag;
   void* Linv;
   void* LinvT;
 };
 template <typename T>
-void launch_potrf_inv_grouped(const GChol* jobs, int njobs, int* err, cudaStream_t s);
+void launch_potrf_inv_grouped(const GChol* jobs, int njobs, int* err, int* job_err, cudaStream_t s);
 // Set the kernels' shared-memory attributes ahead of a stream capture.
 void prepare_potrf_inv_grouped();
 void prepare_gemm_i8_grouped(int S);
@@ -211,8 +213,10 @@ class BatchPipeline;
 BatchPipeline* batch_pipeline_create(int64_t n, int dtype);
 void batch_pipeline_destroy(BatchPipeline* p);
 void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU, bool profile,
-                        unsigned timeout_ms, cudaStream_t s);
+                        unsigned timeout_ms, int selector, cudaStream_t s);
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st);
+// Learned selector inference (fx_selector.cu): out[n x 6] = MLP(x[n x 8]), device pointers.
+void launch_mlp_infer(const float* w, const float* x, int n, float* out, cudaStream_t s);
 // Records the message returned by fx_product_error (fx_debug.cu).
 void set_product_error(const std::string& msg);
 // Grouped form of launch_gemm_i8: `probs` and `tiles` are device arrays; the slice planes of

@@ -1,0 +1,246 @@
+"""Learned (m, s) selection for the walk exponential: features, training data, training, weights.
+
+The Al-Mohy & Higham selection (the reference's ``scipy.linalg.expm``, FastCTQW/Operator.py:76)
+picks the scaling s so that the Pade truncation error stays below the double-precision unit
+roundoff 2^-53, from 1-norm bounds of the powers of the generator.  A walk needs much less: an
+infidelity of 1e-10, or a relative error of 1e-6 in U.  For walk generators X = -iHt with a real
+symmetric H (after the exact trace and rank-one shifts, Y = iB with B real symmetric) the
+truncation error has a closed form: the [m/m] Pade approximant maps the imaginary axis onto the
+unit circle, so at an eigenvalue i lambda it only rotates the phase, by
+
+    phi_m(x) = 2 arg p_m(ix) - x,   x = lambda / 2^s,   and after s squarings 2^s phi_m(x).
+
+With rho_up = min(||Y||_1, ||Y^4||_1^(1/4), ||Y^6||_1^(1/6)) >= spectral radius (exact norms
+of the powers the pipeline forms anyway), the engine *certifies* a choice (m, s) when
+2^s |phi_m(rho_up / 2^s)| <= 1e-6 (``certified``; the same test runs in C++ in fx_batch.cu).
+
+The learned selector is an MLP 8 -> 64 -> 64 -> (5 logits over m in {3, 5, 7, 9, 13} + s) with
+hand-written CUDA kernels (fx_selector.cu: BF16 inference, fused FP32 forward/backward, Adam).
+It is trained on the GPU on (features, labels) that the engine itself produces for seeded walk
+generators (``make_dataset``: the engine's analyze-only mode returns the features, the
+Al-Mohy & Higham (m, s) and the cheapest certified (m, s), which is the label).  At run time a
+proposal is used only when it is cheaper than the plain choice, the bound certifies it and the
+result passes the unitarity check; otherwise the plain (m, s) is used.
+
+Features (per walk): log2 n, log2 ||Y||_1, log2 (||X||_F / sqrt n), log2 (1 + max off-diagonal
+nonzeros of a row), log2 (1 + |trace shift|), rank-one shift flag, log2 d4, log2 d6.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+import numpy as np
+
+from . import _native
+from ._native import lib
+
+DEGREES = (3, 5, 7, 9, 13)
+PRODUCTS = {3: 2, 5: 3, 7: 4, 9: 5, 13: 6}
+PHASE_TOL = 1e-6
+X_LIMIT = {3: 5.0, 5: 7.2, 7: 9.3, 9: 11.4, 13: 15.6}   # half of where |phi_m| reaches pi
+N_PARAMS = 5126
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "selector_weights.npz")
+FEATURE_NAMES = ("log2 n", "log2 ||Y||_1", "log2 ||X||_F/sqrt(n)", "log2(1+max degree)",
+                 "log2(1+|mu|)", "rank-one shift", "log2 d4", "log2 d6")
+
+
+def pade_coeffs(m: int) -> list[float]:
+    f = math.factorial
+    return [f(2 * m - j) / (f(j) * f(m - j)) for j in range(m + 1)]
+
+
+def phase_error(m: int, x) -> np.ndarray:
+    """phi_m(x) = 2 arg p_m(ix) - x wrapped to (-pi, pi]: the rotation of e^{ix} by r_m."""
+    b = pade_coeffs(m)
+    x = np.asarray(x, dtype=np.float64)
+    z = 1j * x
+    acc = np.zeros_like(z)
+    for j in range(m, -1, -1):
+        acc = acc * z + b[j]
+    return np.remainder(2.0 * np.arctan2(acc.imag, acc.real) - x + np.pi, 2 * np.pi) - np.pi
+
+
+def certified(m: int, s: int, rho_up: float, tol: float = PHASE_TOL) -> bool:
+    x = math.ldexp(rho_up, -s)
+    return x <= X_LIMIT[m] and math.ldexp(abs(float(phase_error(m, x))), s) <= tol
+
+
+def certified_choice(rho_up: float, tol: float = PHASE_TOL) -> tuple[int, int]:
+    """Cheapest (m, s) (products pi_m + s, ties to the larger m) that the bound certifies."""
+    best = None
+    for m in DEGREES:
+        s = 0
+        while s < 200 and not certified(m, s, rho_up, tol):
+            s += 1
+        cost = PRODUCTS[m] + s
+        if best is None or cost <= best[0]:
+            best = (cost, m, s)
+    return best[1], best[2]
+
+
+# ------------------------------------------------------------------------------- data
+def make_walks(count: int, seed: int, nmin: int = 64, nmax: int = 1024, tmin: float = 0.1,
+               tmax: float = 1000.0):
+    """Seeded walk generators X = -1j H t: random d-regular (d 3..16), G(n, p) (p 0.05..0.5) or
+    uniform-[0, 1]-weighted complete graphs, H = -A or -(D - A), t log-uniform; yields (X, meta)."""
+    from . import graphs
+    rng = np.random.default_rng(seed)
+    for _ in range(count):
+        n = int(rng.integers(nmin, nmax + 1))
+        kind = ("regular", "er", "weighted")[int(rng.integers(0, 3))]
+        lap = bool(rng.integers(0, 2))
+        t = float(math.exp(rng.uniform(math.log(tmin), math.log(tmax))))
+        gseed = int(rng.integers(0, 2 ** 31 - 1))
+        if kind == "regular":
+            d = int(rng.integers(3, 17))
+            if (n * d) % 2:
+                d += 1
+            A = graphs.random_regular(n, d, gseed, np.float64)
+        elif kind == "er":
+            A = graphs.erdos_renyi(n, float(rng.uniform(0.05, 0.5)), gseed, np.float64)
+        else:
+            A = graphs.weighted_complete(n, gseed, np.float64)
+        H = -((np.diag(A.sum(axis=1)) - A) if lap else A)
+        yield np.asarray(-1j * H * t, dtype=np.complex64), (kind, n, lap, t)
+
+
+def make_dataset(count: int, seed: int, nmin: int = 64, nmax: int = 1024, tmin: float = 0.1,
+                 tmax: float = 1000.0, chunk: int = 192) -> dict:
+    """The walks of ``make_walks`` run through the engine's analyze-only mode (GPU): features,
+    the Al-Mohy & Higham (m, s) and the certified (m, s), the training label."""
+    from .batch import WalkBatch
+    feats, pm, ps, cm, cs, meta = [], [], [], [], [], []
+    it = make_walks(count, seed, nmin, nmax, tmin, tmax)
+    todo = count
+    while todo > 0:
+        k = min(chunk, todo)
+        Xs = []
+        for _ in range(k):
+            X, mt = next(it)
+            Xs.append(X)
+            meta.append(mt)
+        b = WalkBatch([X.shape[0] for X in Xs], analyze_only=True)
+        b.run(Xs)
+        d = b.details()
+        b.close()
+        feats.append(d["features"])
+        pm.append(d["plain_m"])
+        ps.append(d["plain_s"])
+        cm.append(d["cert_m"])
+        cs.append(d["cert_s"])
+        todo -= k
+    cat = np.concatenate
+    return {"features": cat(feats).astype(np.float32), "plain_m": cat(pm), "plain_s": cat(ps),
+            "cert_m": cat(cm), "cert_s": cat(cs), "meta": np.array(meta, dtype=object)}
+
+
+def rho_up(features: np.ndarray) -> np.ndarray:
+    """min(||Y||_1, d4, d6) from the features (columns 1, 6, 7 are their log2)."""
+    f = np.asarray(features, dtype=np.float64)
+    return np.exp2(np.minimum(f[:, 1], np.minimum(f[:, 6], f[:, 7])))
+
+
+def gate(features, plain_m, plain_s, prop_m, prop_s) -> np.ndarray:
+    """Selection outcome per walk, as the engine decides it: 2 accepted, -1 rejected by the
+    bound, 0 not cheaper than the plain choice."""
+    r = rho_up(features)
+    out = np.zeros(len(r), dtype=np.int32)
+    for i in range(len(r)):
+        pm, ps = int(prop_m[i]), int(prop_s[i])
+        if PRODUCTS[pm] + ps < PRODUCTS[int(plain_m[i])] + int(plain_s[i]):
+            out[i] = 2 if certified(pm, ps, float(r[i])) else -1
+    return out
+
+
+def labels(ds: dict) -> tuple[np.ndarray, np.ndarray]:
+    """Class index of the certified m in DEGREES and the certified s (float)."""
+    idx = {m: i for i, m in enumerate(DEGREES)}
+    return (np.array([idx[int(m)] for m in ds["cert_m"]], dtype=np.int32),
+            np.asarray(ds["cert_s"], dtype=np.float32))
+
+
+# ----------------------------------------------------------------------------- network
+def init_weights(seed: int) -> np.ndarray:
+    """He-initialised FP32 weights in the kernel's layout (W1, b1, W2, b2, W3, b3)."""
+    rng = np.random.default_rng(seed)
+    w1 = rng.standard_normal((64, 8)) * math.sqrt(2 / 8)
+    w2 = rng.standard_normal((64, 64)) * math.sqrt(2 / 64)
+    w3 = rng.standard_normal((6, 64)) * math.sqrt(1 / 64)
+    return np.concatenate([w1.ravel(), np.zeros(64), w2.ravel(), np.zeros(64), w3.ravel(),
+                           np.zeros(6)]).astype(np.float32)
+
+
+def fold_standardisation(w: np.ndarray, mean: np.ndarray, std: np.ndarray) -> np.ndarray:
+    """Weights that take raw features: W1 x' + b1 with x' = (x - mean) / std."""
+    w = w.copy()
+    W1 = w[:512].reshape(64, 8) / std[None, :]
+    w[512:576] = w[512:576] - W1 @ mean
+    w[:512] = W1.ravel()
+    return w
+
+
+def _dev(a, dtype):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+def train(ds: dict, epochs: int = 60, batch: int = 256, lr: float = 2e-3, lam: float = 0.25,
+          seed: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Train on the GPU (fx_mlp_train).  Returns (weights for raw features, loss per epoch)."""
+    import torch
+    X = np.asarray(ds["features"], dtype=np.float32)
+    mean, std = X.mean(axis=0), X.std(axis=0) + 1e-6
+    ym, ys = labels(ds)
+    w = _dev(init_weights(seed), torch.float32)
+    dx = _dev((X - mean) / std, torch.float32)
+    dym, dys = _dev(ym, torch.int32), _dev(ys, torch.float32)
+    losses = (ctypes.c_float * epochs)()
+    rc = lib().fx_mlp_train(w.data_ptr(), dx.data_ptr(), dym.data_ptr(), dys.data_ptr(), len(X), epochs,
+                            batch, lr, lam, seed, losses, torch.cuda.current_stream().cuda_stream)
+    if rc != _native.OK:
+        raise RuntimeError(lib().fx_mlp_error().decode())
+    return fold_standardisation(w.cpu().numpy(), mean, std), np.array(losses[:], dtype=np.float32)
+
+
+def infer(w: np.ndarray, features: np.ndarray) -> np.ndarray:
+    """n x 6 outputs of the network (BF16 inference kernel)."""
+    import torch
+    dw = _dev(w, torch.float32)
+    dx = _dev(np.asarray(features, dtype=np.float32), torch.float32)
+    out = torch.empty((len(features), 6), dtype=torch.float32, device="cuda")
+    rc = lib().fx_mlp_infer(dw.data_ptr(), dx.data_ptr(), len(features), out.data_ptr(),
+                            torch.cuda.current_stream().cuda_stream)
+    if rc != _native.OK:
+        raise RuntimeError(lib().fx_mlp_error().decode())
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def proposals(out: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """(m, s) proposed by network outputs (argmax of the logits, s rounded, >= 0)."""
+    m = np.array([DEGREES[int(i)] for i in np.argmax(out[:, :5], axis=1)], dtype=np.int32)
+    s = np.maximum(0, np.rint(out[:, 5])).astype(np.int32)
+    return m, s
+
+
+# ----------------------------------------------------------------------------- weights
+def save(path: str, w: np.ndarray, **meta) -> None:
+    np.savez(path, weights=np.asarray(w, dtype=np.float32), **meta)
+
+
+def load(path: str = WEIGHTS) -> np.ndarray:
+    with np.load(path) as z:
+        w = np.asarray(z["weights"], dtype=np.float32)
+    if w.size != N_PARAMS:
+        raise ValueError(f"selector weights: expected {N_PARAMS} values, found {w.size}")
+    return w
+
+
+def set_weights(w: np.ndarray | None = None) -> None:
+    """Install weights for the learned selection of every handle (default: the shipped file)."""
+    w = np.ascontiguousarray(load() if w is None else w, dtype=np.float32)
+    rc = lib().fx_selector_set_weights(w.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), w.size)
+    if rc != _native.OK:
+        raise RuntimeError(lib().fx_batch_last_error(None).decode())

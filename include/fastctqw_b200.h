@@ -76,8 +76,13 @@ enum fx_option {
   FX_OPT_DEBUG_STAGE = 8, /* diagnostics: k > 0 makes run write intermediate k instead of
                              U (1 Y, 2-4 A2/A4/A6, 5 U_pade, 6 V_pade, 7 R, 8+j after j
                              squarings) and stop                                       */
-  FX_OPT_PROFILE = 9      /* 1: CUDA-event timing of every tensor-core product launch
+  FX_OPT_PROFILE = 9,     /* 1: CUDA-event timing of every tensor-core product launch
                              (fx_stats.prod_*)                                         */
+  FX_OPT_SELECTOR = 10    /* (m, s) selection for walk generators X = i*(real symmetric):
+                             0 Al-Mohy & Higham (default), 1 the cheapest (m, s) the
+                             truncation bound certifies at phase error 1e-6, 2 the learned
+                             MLP proposal, accepted only when the bound certifies it and
+                             the result passes the unitarity check (else option 0)     */
 };
 
 /* What the last run did. */
@@ -101,6 +106,12 @@ typedef struct fx_stats {
   double prod_flops;    /* real-arithmetic flops they computed           */
   int32_t prod_launches;
   int32_t reserved2;
+  int32_t selector;     /* FX_OPT_SELECTOR of the run                                  */
+  int32_t sel_outcome;  /* 0 plain, 1 certified, 2 learned accepted, -1 learned rejected
+                           by the bound, -2 failed an a-posteriori check (Cholesky of
+                           Q^H Q or unitarity) and was redone with the plain (m, s)  */
+  int32_t plain_m;      /* (m, s) of the Al-Mohy & Higham selection                    */
+  int32_t plain_s;
 } fx_stats;
 
 int fx_create(size_t n, int dtype, fx_handle* out);
@@ -160,7 +171,9 @@ typedef struct fx_batch* fx_batch_handle;
 enum fx_batch_option {
   FX_BATCH_OPT_GRAPH = 0,       /* 1 (default): replay the post-selection phases as a CUDA graph */
   FX_BATCH_OPT_TIMEOUT_MS = 1,  /* bound of every device-side wait (default 2000)               */
-  FX_BATCH_OPT_FORCE_M = 2      /* diagnostics: force the Pade degree (-1 automatic)            */
+  FX_BATCH_OPT_FORCE_M = 2,     /* diagnostics: force the Pade degree (-1 automatic)            */
+  FX_BATCH_OPT_SELECTOR = 3,    /* as FX_OPT_SELECTOR                                           */
+  FX_BATCH_OPT_ANALYZE_ONLY = 4 /* 1: stop after the selection (features and (m, s) only)       */
 };
 /* count walks of sizes n[0..count); dtype FX_C64 or FX_C128 (of X, psi0 and psi). */
 int fx_batch_create(size_t count, const int64_t* n, int dtype, fx_batch_handle* out);
@@ -177,7 +190,34 @@ int fx_batch_walk_host(fx_batch_handle b, const void* const* X, const void* cons
 int fx_batch_selection(fx_batch_handle b, int32_t* m, int32_t* s);
 /* Device time (ms, CUDA events), algorithmic flops and kernel launches of the last run. */
 int fx_batch_info(fx_batch_handle b, double* ms, double* flops, int32_t* launches);
+/* Per walk of the last run: the 8 selector features (features[8 w ..]: log2 n, log2 ||Y||_1,
+ * log2 (||X||_F / sqrt n), log2 (1 + max off-diagonal nonzeros of a row), log2 (1 + |mu|),
+ * rank-one shift flag, log2 d4, log2 d6), the Al-Mohy & Higham (m, s), the certified (m, s) and
+ * the selection outcome (as fx_stats.sel_outcome). */
+int fx_batch_details(fx_batch_handle b, double* features, int32_t* plain_m, int32_t* plain_s,
+                     int32_t* cert_m, int32_t* cert_s, int32_t* outcome);
+/* Weights of the learned selector for every handle of the process (5126 floats, host
+ * pointer; copied to the current device). */
+int fx_selector_set_weights(const float* w, int64_t n);
 const char* fx_batch_last_error(fx_batch_handle b);
+
+/* ---- Learned (m, s) selector: MLP 8 -> 64 -> 64 -> (5 Pade-degree logits + s), ReLU.
+ * No counterpart in the reference (its scaling was chosen inside the absent prebuilt core).
+ * 5126 FP32 weights in the order W1 [64 x 8], b1, W2 [64 x 64], b2, W3 [6 x 64], b3.
+ * All pointers are device pointers.  Inference runs with BF16 weights, FP32 accumulation;
+ * training with fused forward/backward kernels and Adam, all on the device. */
+int fx_mlp_param_count(void);
+/* out[n x 6] = MLP(x[n x 8]). */
+int fx_mlp_infer(const float* w, const float* x, int64_t n, float* out, void* stream);
+/* Mean loss over the n samples (cross-entropy of the class ym in 0..4 + lambda (s_hat - ys)^2)
+ * and its gradient w.r.t. the weights (grad: 5126 floats, loss: 1 float). */
+int fx_mlp_loss_grad(const float* w, const float* x, const int32_t* ym, const float* ys, int64_t n,
+                     float lambda, float* grad, float* loss, void* stream);
+/* Adam training in place of w: `epochs` passes over seeded permutations in minibatches of
+ * `batch`; epoch_loss (host, epochs floats, may be NULL) receives the mean loss per epoch. */
+int fx_mlp_train(float* w, const float* x, const int32_t* ym, const float* ys, int64_t n, int epochs,
+                 int batch, float lr, float lambda, uint64_t seed, float* epoch_loss, void* stream);
+const char* fx_mlp_error(void);
 
 /* Device memory currently in use on the current device, GB. */
 double fx_gpu_memory_gb(void);
