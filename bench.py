@@ -194,20 +194,34 @@ def bench_batch(args, dev):
     dP0 = [torch.from_numpy(p).to(dev) for p in P0]
     dP = [torch.empty_like(p) for p in dP0]
     stream = torch.cuda.current_stream(dev)
-    b = WalkBatch(ns)
-    for _ in range(max(1, args.warmup)):
-        b.run_device(dX, dP0, dP, stream)
-    torch.cuda.synchronize()
+    if args.selector == "learned":
+        from fastctqw_b200 import selector as sel
+        sel.set_weights()
     reps = max(1, min(args.steps, 3))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(reps):
-        b.run_device(dX, dP0, dP, stream)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    batch_ms = ev0.elapsed_time(ev1) / reps
+
+    def timed(bb):
+        for _ in range(max(1, args.warmup)):
+            bb.run_device(dX, dP0, dP, stream)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(reps):
+            bb.run_device(dX, dP0, dP, stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / reps
+
+    plain_batch_ms = None
+    if args.selector != "plain":
+        bpl = WalkBatch(ns)
+        plain_batch_ms = timed(bpl)
+        _, s_plain = bpl.selection()
+        bpl.close()
+    b = WalkBatch(ns, selector=args.selector)
+    batch_ms = timed(b)
     info = b.info()
     m, s = b.selection()
+    outcome = b.details()["outcome"]
     # accuracy on the largest walks: FP64 eigendecomposition of A on the device
     worst = 0.0
     for k in sorted(range(len(ns)), key=lambda k: -ns[k])[:4]:
@@ -244,6 +258,11 @@ def bench_batch(args, dev):
         "loop_ms": round(loop_ms, 1) if loop_ms else None,
         "speedup_vs_loop": round(loop_ms / batch_ms, 2) if loop_ms else None,
         "launches_per_batch": info["launches"], "algorithmic_tflops": round(info["flops"] / (batch_ms * 1e-3) / 1e12, 1),
+        "selector": args.selector,
+        "plain_selection_ms": round(plain_batch_ms, 2) if plain_batch_ms else None,
+        "plain_selection_walks_per_s": round(walks / (plain_batch_ms * 1e-3), 1) if plain_batch_ms else None,
+        "squarings_chosen": int(s.sum()), "squarings_plain": int(s_plain.sum()) if plain_batch_ms else None,
+        "outcomes": {int(k): int(v) for k, v in zip(*np.unique(outcome, return_counts=True))},
         "m_hist": {int(k): int(v) for k, v in zip(*np.unique(m, return_counts=True))},
         "s_max": int(s.max()), "s_mean": round(float(s.mean()), 2),
         "worst_infidelity_4_largest": worst,
@@ -260,6 +279,8 @@ def main():
     ap.add_argument("--t", type=float, default=4.5)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--form", default="plain", choices=["plain", "mixed", "simt"])
+    ap.add_argument("--selector", default="learned", choices=["plain", "certified", "learned"],
+                    help="(m, s) selection of the timed walk; the plain selection is timed beside it")
     ap.add_argument("--ref-sample-n", type=int, default=1024)
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 infidelity check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -303,8 +324,11 @@ def main():
     dpsi0 = torch.from_numpy(psi0).to(dev)
     dpsi = torch.empty_like(dpsi0)
     dU = torch.empty_like(dX)
+    if args.selector == "learned":
+        from fastctqw_b200 import selector as sel
+        sel.set_weights()
     eng = Engine(n, np.complex64)
-    eng.configure(form=args.form)
+    eng.configure(form=args.form, selector=args.selector)
     stream = torch.cuda.current_stream(dev)
 
     def step():
@@ -331,6 +355,7 @@ def main():
     total_ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     st = eng.stats()
+    psi_chosen = dpsi.clone()
     if world > 1:
         tt = torch.tensor([total_ms], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -359,17 +384,37 @@ def main():
         "useful_real_tflops": round(pst["prod_flops"] / (pst["prod_ms"] * 1e-3) / 1e12, 2) if pst["prod_ms"] else None,
     }
 
-    # ---- accuracy of this run against the FP64 eigendecomposition propagator
+    # ---- the plain (Al-Mohy & Higham) selection on the same walk, timed the same way
+    plain = None
+    psi_plain = None
+    if args.selector != "plain":
+        eng.configure(selector="plain")
+        step()
+        torch.cuda.synchronize()
+        reps = max(1, min(args.steps, 3))
+        ev0.record(stream)
+        for _ in range(reps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        pst2 = eng.stats()
+        plain = {"ms": round(ev0.elapsed_time(ev1) / reps, 3), "m": pst2["m"], "s": pst2["s"],
+                 "steps": reps}
+        psi_plain = dpsi.clone()
+        eng.configure(selector=args.selector)
+
+    # ---- accuracy of both against the FP64 eigendecomposition propagator
     accuracy = None
     if not args.no_check and rank == 0:
         from oracle import expm_oracle as eo
         Hd = torch.from_numpy(H).to(dev)
         lam, V = torch.linalg.eigh(Hd)
         Vc = V.to(torch.complex128)
-        ref = Vc @ (torch.exp(-1j * lam * args.t) * Vc[0])
-        psi = dpsi.cpu().numpy()
-        accuracy = {"infidelity_e0": eo.infidelity(psi, ref.cpu().numpy())}
-        del Hd, V, lam
+        ref = (Vc @ (torch.exp(-1j * lam * args.t) * Vc[0])).cpu().numpy()
+        accuracy = {"infidelity_e0": eo.infidelity(psi_chosen.cpu().numpy(), ref)}
+        if psi_plain is not None:
+            accuracy["infidelity_e0_plain"] = eo.infidelity(psi_plain.cpu().numpy(), ref)
+        del Hd, V, lam, Vc
         torch.cuda.empty_cache()
 
     # ---- end to end through the drop-in API (host ndarray in, host ndarray out)
@@ -377,7 +422,7 @@ def main():
     if rank == 0 and not args.no_e2e:
         X_pinned = torch.from_numpy(X).pin_memory().numpy()
         em = fastexpm.ExpMatComplex64(n)
-        em.configure(form=args.form)
+        em.configure(form=args.form, selector=args.selector)
         em.run(X_pinned)
         e_steps = max(1, min(args.steps, 3))
         t0 = time.perf_counter()
@@ -411,12 +456,16 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 (int8 Ozaki-slice products, FP64 masters)",
             "data": "synthetic (seeded G(n,0.5) Laplacian)",
             "config": {"workload": f"dense ER G(n={n}, p=0.5) Laplacian, t={args.t}, complex64 expm + U psi0, psi0=|0>",
-                       "n": n, "t": args.t, "form": args.form, "m": st["m"], "s": st["s"],
+                       "n": n, "t": args.t, "form": args.form, "selector": args.selector,
+                       "selection_outcome": st["sel_outcome"], "m": st["m"], "s": st["s"],
+                       "plain_m": st["plain_m"], "plain_s": st["plain_s"],
                        "solver": "cholesky(Q^H Q)" if st["solver"] == 1 else "pivoted LU",
                        "l2": "working set ~25 GB >> 126 MB L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
             "clocks": clk, "e2e": e2e, "gpu_launches": int(st["launches"]) * args.steps,
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "batch": batch,
+            "plain_selection": plain,
+            "chosen_vs_plain_speedup": round(plain["ms"] / ms_per_step, 3) if plain else None,
             "algorithmic_tflops": round(st["flops"] / (ms_per_step * 1e-3) / 1e12, 2),
         }
         print(json.dumps(out), flush=True)

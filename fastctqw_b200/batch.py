@@ -20,7 +20,7 @@ import numpy as np
 from . import _native
 from ._native import check, lib
 
-OPT_GRAPH, OPT_TIMEOUT_MS, OPT_FORCE_M, OPT_SELECTOR, OPT_ANALYZE_ONLY = 0, 1, 2, 3, 4
+OPT_GRAPH, OPT_TIMEOUT_MS, OPT_FORCE_M, OPT_SELECTOR, OPT_ANALYZE_ONLY, OPT_DIAG_SPLIT = 0, 1, 2, 3, 4, 5
 OUTCOMES = {0: "plain", 1: "certified", 2: "learned", -1: "learned rejected by the bound",
             -2: "failed an a-posteriori check, redone with the plain (m, s)"}
 
@@ -48,7 +48,7 @@ class WalkBatch:
     """Owner of one ``fx_batch`` handle: device workspace for walks of sizes ``ns``."""
 
     def __init__(self, ns, dtype=np.complex64, graph: bool = True, selector: str = "plain",
-                 analyze_only: bool = False) -> None:
+                 analyze_only: bool = False, diag_split: int = 3) -> None:
         self.ns = [int(n) for n in ns]
         self.dtype = np.dtype(dtype)
         if self.dtype not in (np.dtype(np.complex64), np.dtype(np.complex128)):
@@ -63,6 +63,8 @@ class WalkBatch:
             self.set_option(OPT_SELECTOR, _native.SELECTORS[selector])
         if analyze_only:
             self.set_option(OPT_ANALYZE_ONLY, 1)
+        if int(diag_split) != 3:
+            self.set_option(OPT_DIAG_SPLIT, int(diag_split))
 
     def set_option(self, key: int, value: float) -> None:
         _check(lib().fx_batch_set_option(self._h, int(key), float(value)), self._h)

@@ -69,6 +69,8 @@ struct I8Params {
   // grouped mode: per-tile jobs and per-problem descriptors (device memory)
   const GProblem* probs;
   const GTile* tiles;
+  const double* adg;   // diagonal split: removed diagonals by stacked row
+  const double* bdg;
 };
 
 __host__ __device__ constexpr uint32_t idesc_i8(int m, int n) {
@@ -137,6 +139,40 @@ struct TileJob {
   int sym;
   int prob;            // problem index (grouped) or -1
 };
+
+// L2 prefetch of the blocks a grouped tile's epilogue reads (the C block, and the FP64 masters
+// of a split problem), issued by the epilogue threads one tile ahead, while the MMAs run: the
+// epilogue's loads then find them in L2.  A hint only: ranges that are not 16-byte aligned
+// multiples of 16 bytes are skipped.
+__device__ __forceinline__ void prefetch_l2(const void* a, int64_t bytes) {
+  if ((reinterpret_cast<uintptr_t>(a) & 15) == 0 && bytes > 0 && (bytes & 15) == 0)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)bytes) : "memory");
+}
+template <typename TO>
+__device__ __forceinline__ void prefetch_tile(const I8Params& p, int tile, int bn, int et, int nthreads) {
+  const GTile t = p.tiles[tile];
+  const GProblem& q = p.probs[t.prob];
+  const int64_t r0 = (int64_t)t.mb * kBM, c0 = (int64_t)t.nb * bn;
+  const int rows = (int)min((int64_t)kBM, (int64_t)q.M - r0), cols = (int)min((int64_t)bn, (int64_t)q.N - c0);
+  if (rows <= 0 || cols <= 0) return;
+  const int nc = (q.beta != 0.0 && q.C) ? rows : 0;                 // C rows (row-major)
+  const int na = q.split == 2 ? cols : (q.split == 1 ? rows : 0);   // A: columns (symmetric) or rows
+  const int nb = (q.split && !(q.split == 2 && q.Am == q.Btm && q.ldam == q.ldbm)) ? cols : 0;
+  for (int k = et; k < nc + na + nb; k += nthreads) {
+    if (k < nc) {
+      prefetch_l2((const TO*)q.C + (r0 + k) * q.ldc + c0, (int64_t)cols * sizeof(TO));
+    } else if (k < nc + na) {
+      const int i = k - nc;
+      if (q.split == 2)
+        prefetch_l2((const TO*)q.Am + (c0 + i) * q.ldam + r0, (int64_t)rows * sizeof(TO));
+      else
+        prefetch_l2((const TO*)q.Am + (r0 + i) * q.ldam + c0, (int64_t)cols * sizeof(TO));
+    } else {
+      const int j = k - nc - na;
+      prefetch_l2((const TO*)q.Btm + (c0 + j) * q.ldbm + r0, (int64_t)rows * sizeof(TO));
+    }
+  }
+}
 
 template <bool G>
 __device__ __forceinline__ TileJob job_of(const I8Params& p, int tile) {
@@ -311,79 +347,166 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
     constexpr int kChunks = kBN / 32;   // 16-column chunks per half
     int it = 0;
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++it) {
+      if constexpr (G) {
+        const int et = (int)threadIdx.x - 64;
+        if (it == 0) prefetch_tile<TO>(p, tile, kBN, et, kThreads - 64);
+        if (tile + (int)gridDim.x < p.ntiles) prefetch_tile<TO>(p, tile + gridDim.x, kBN, et, kThreads - 64);
+      }
       if (!mbar_wait(&tfull_bar, it & 1, &s_abort, p.timeout_ns, p.err)) break;
       tc_fence_after();
       const TileJob jb = job_of<G>(p, tile);
-      double alpha = p.alpha, beta = p.beta, gamma = p.gamma;
-      const TO* Cq = Cp;
-      TO* Dq = Dp;
-      TO* Dt = nullptr;
-      int64_t ldc = p.ldc, ldd = p.ldd, ldt = 0;
-      const int* aexp = p.aexp;
-      const int* bexp = p.bexp;
-      if constexpr (G) {
-        const GProblem& pr = p.probs[jb.prob];
-        alpha = pr.alpha;
-        beta = pr.beta;
-        gamma = pr.gamma;
-        Cq = (const TO*)pr.C;
-        Dq = (TO*)pr.D;
-        Dt = (TO*)pr.Dt;
-        ldc = pr.ldc;
-        ldd = pr.ldd;
-        ldt = pr.ldt;
-        aexp += pr.a_row0;
-        bexp += pr.b_row0;
-      }
       const bool acc = jb.kb1 > jb.kb0;   // an empty K range leaves the accumulator unwritten
       const int64_t row = (int64_t)jb.mb * kBM + q * 32 + lane;
       const bool row_ok = row < jb.M;
-      const int ea = row_ok ? aexp[row] : 0;
-      const double rowscale = pow2_or_zero(ea - 14);
-      for (int cc = half * kChunks; cc < (half + 1) * kChunks; ++cc) {
-        int lv[S][16];
-        const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(cc * 16);
-#pragma unroll
-        for (int l = 0; l < S; ++l) tmem_ld16(ta + l * kBN, lv[l]);
-        tmem_wait_ld();
-        const int64_t col0 = (int64_t)jb.nb * kBN + cc * 16;
-        if (!row_ok || col0 >= jb.N) continue;
-        TO out[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int64_t col = col0 + i;
-          double v = 0.0;
-          if (acc) {
-            v = (double)lv[S - 1][i];
-#pragma unroll
-            for (int l = S - 2; l >= 0; --l) v = v * 0x1p-7 + (double)lv[l][i];
-            const int eb = bexp[col];
-            v = (rowscale != 0.0 && eb > -1000 && eb < 1000) ? v * rowscale * pow2_or_zero(eb)
-                                                             : ldexp(v, ea + eb - 14);
+      // Columns col0 .. col0 + 15 of this thread's row from the folded levels x: scaling,
+      // diagonal split terms, alpha / beta C / gamma I, stores.  The launch's or the problem's
+      // parameters are read here, after the TMEM reads, to keep them out of the fold's registers.
+      auto finish = [&](const double (&x)[16], int64_t col0) {
+        double alpha = p.alpha, beta = p.beta, gamma = p.gamma;
+        const TO* Cq = Cp;
+        TO* Dq = Dp;
+        TO* Dt = nullptr;
+        int64_t ldc = p.ldc, ldd = p.ldd, ldt = 0;
+        const int* aexp = p.aexp;
+        const int* bexp = p.bexp;
+        int split = 0;
+        const TO* Am = nullptr;
+        const TO* Btm = nullptr;
+        int64_t ldam = 0, ldbm = 0;
+        const double* bdg = nullptr;
+        double adiag = 0.0;
+        if constexpr (G) {
+          const GProblem& pr = p.probs[jb.prob];
+          alpha = pr.alpha;
+          beta = pr.beta;
+          gamma = pr.gamma;
+          Cq = (const TO*)pr.C;
+          Dq = (TO*)pr.D;
+          Dt = (TO*)pr.Dt;
+          ldc = pr.ldc;
+          ldd = pr.ldd;
+          ldt = pr.ldt;
+          aexp += pr.a_row0;
+          bexp += pr.b_row0;
+          split = pr.split;
+          if (split) {
+            Am = (const TO*)pr.Am;
+            Btm = (const TO*)pr.Btm;
+            ldam = pr.ldam;
+            ldbm = pr.ldbm;
+            bdg = p.bdg + pr.b_row0;
+            adiag = p.adg[pr.a_row0 + row];
           }
-          v *= alpha;
-          if (beta != 0.0) v += beta * (double)Cq[row * ldc + col];
-          if (col == row) v += gamma;
-          out[i] = (TO)v;
         }
-        if (!jb.sym) {
+        const int ea = aexp[row];
+        const double rowscale = pow2_or_zero(ea - 14);
+        const bool same_ab = split == 2 && Am == Btm && ldam == ldbm;   // B = A: one read
+        // Eight columns at a time: all loads first, then the stores (loads placed after a
+        // store of the same type could not be hoisted above it).  The masters, diagonals and
+        // exponents take the read-only path (D never overlaps them); C is read plainly, as D
+        // may be C.  split 1: the thread's A row segment in 16-byte loads (the lanes hold
+        // different rows); split 2: A symmetric, read down the columns across the lanes.
 #pragma unroll
-          for (int i = 0; i < 16; ++i) Dq[row * ldd + col0 + i] = out[i];
-          if (Dt) {
+        for (int h = 0; h < 16; h += 8) {
+          const int64_t c0 = col0 + h;
+          double arow[8];
+          if (split == 1) {
+            const TO* ar = Am + row * ldam + c0;
+            if constexpr (sizeof(TO) == 8) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) Dt[(col0 + i) * ldt + row] = out[i];
+              for (int i = 0; i < 8; i += 2) {
+                const double2 t2 = __ldg(reinterpret_cast<const double2*>(ar + i));
+                arow[i] = t2.x;
+                arow[i + 1] = t2.y;
+              }
+            } else {
+#pragma unroll
+              for (int i = 0; i < 8; ++i) arow[i] = (double)__ldg(ar + i);
+            }
           }
-        } else {
+          double v[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const int64_t col = c0 + i;
+            double t = 0.0;
+            if (acc) {
+              const int eb = __ldg(bexp + col);
+              t = (rowscale != 0.0 && eb > -1000 && eb < 1000) ? x[h + i] * rowscale * pow2_or_zero(eb)
+                                                               : ldexp(x[h + i], ea + eb - 14);
+            }
+            if (split) {
+              double aij = split == 2 ? (double)__ldg(Am + col * ldam + row) : arow[i];
+              const double bji = same_ab ? aij : (double)__ldg(Btm + col * ldbm + row);
+              if (col == row) aij = 0.0;
+              t += adiag * bji + aij * __ldg(bdg + col);
+            }
+            t *= alpha;
+            if (beta != 0.0) t += beta * (double)Cq[row * ldc + col];
+            if (col == row) t += gamma;
+            v[i] = t;
+          }
+          if (!jb.sym) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) Dq[row * ldd + c0 + i] = (TO)v[i];
+            if (Dt) {
+#pragma unroll
+              for (int i = 0; i < 8; ++i) Dt[(c0 + i) * ldt + row] = (TO)v[i];
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              const int64_t col = c0 + i;
+              if (col >= row) Dq[row * ldd + col] = (TO)v[i];
+              if (col > row) Dq[col * ldd + row] = (TO)v[i];
+            }
+          }
+        }
+      };
+      // x = sum_l 2^(-7 l) L_l of 16 columns, from the top level down, the levels read two at a
+      // time (for |L_l| < 2^31 every step but the last of five levels is exact in FP64).
+      auto fold = [&](uint32_t ta, double (&x)[16]) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) x[i] = 0.0;
+#pragma unroll
+        for (int l = S - 1; l >= 0; l -= 2) {
+          int hi[16], lo[16];
+          tmem_ld16(ta + l * kBN, hi);
+          if (l >= 1) tmem_ld16(ta + (l - 1) * kBN, lo);
+          tmem_wait_ld();
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
-            const int64_t col = col0 + i;
-            if (col >= row) Dq[row * ldd + col] = out[i];
-            if (col > row) Dq[col * ldd + row] = out[i];
+            double t = x[i] * 0x1p-7 + (double)hi[i];
+            if (l >= 1) t = t * 0x1p-7 + (double)lo[i];
+            x[i] = t;
           }
         }
+      };
+      const uint32_t tq = tmem_base + ((uint32_t)(q * 32) << 16);
+      if constexpr (kChunks <= 3) {
+        // All of this half's columns fit in registers once folded: drain TMEM first and hand it
+        // back to the MMA warp, so that the next tile's products overlap the rest of the epilogue.
+        double xv[kChunks][16];
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) fold(tq + (uint32_t)((half * kChunks + c) * 16), xv[c]);
+        tc_fence_before();
+        mbar_arrive(&tempty_bar);
+        if (row_ok) {
+#pragma unroll
+          for (int c = 0; c < kChunks; ++c) {
+            const int64_t col0 = (int64_t)jb.nb * kBN + (half * kChunks + c) * 16;
+            if (col0 < jb.N) finish(xv[c], col0);
+          }
+        }
+      } else {
+        for (int cc = half * kChunks; cc < (half + 1) * kChunks; ++cc) {
+          double x[16];
+          fold(tq + (uint32_t)(cc * 16), x);
+          const int64_t col0 = (int64_t)jb.nb * kBN + cc * 16;
+          if (row_ok && col0 < jb.N) finish(x, col0);
+        }
+        tc_fence_before();
+        mbar_arrive(&tempty_bar);
       }
-      tc_fence_before();
-      mbar_arrive(&tempty_bar);
     }
   }
 
@@ -442,14 +565,16 @@ __device__ __forceinline__ void load4(const TI* src, int64_t k0, int64_t K, bool
 // NEG: also write the slices of -im (out.neg_im).
 template <typename TI, bool NEG>
 __device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t K, int S, const I8Slices& out,
-                                          int64_t orow, int lane) {
+                                          int64_t orow, int lane, int64_t dcol = -1) {
+  // dcol >= 0: the element at that column (the diagonal of a real plane) is left out of the
+  // slices and stored to out.dg[orow]
   const bool vec = ((reinterpret_cast<uintptr_t>(rre) | reinterpret_cast<uintptr_t>(rim)) & 15) == 0;
   double mx = 0.0;
   for (int64_t k0 = (int64_t)lane * 4; k0 < K; k0 += 128) {
     double v[4];
     load4<TI>(rre, k0, K, vec, v);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) mx = fmax(mx, fabs(v[j]));
+    for (int j = 0; j < 4; ++j) mx = fmax(mx, k0 + j == dcol ? 0.0 : fabs(v[j]));
     if (rim) {
       load4<TI>(rim, k0, K, vec, v);
 #pragma unroll
@@ -464,6 +589,7 @@ __device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t 
     if (m * 128.0 >= 127.5) e += 1;
   }
   if (lane == 0) out.exp[orow] = e;
+  if (dcol >= 0 && lane == 0) out.dg[orow] = (double)rre[dcol];
   // 2^(7S - e) as one factor when it is a normal double (always, unless the row is tiny)
   const int sh = 7 * S - e;
   const bool one_factor = sh <= 1000;
@@ -479,6 +605,7 @@ __device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t 
       const bool neg = NEG && plane == 1;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
+        if (plane == 0 && k0 + j == dcol) x[j] = 0.0;
         const double xs = one_factor ? x[j] * scale : ldexp(ldexp(x[j], -e), 7 * S);
         long long r = __double2ll_rn(xs);
 #pragma unroll
@@ -536,7 +663,8 @@ __global__ void __launch_bounds__(256, 3) k_slice_rows_grouped(const GSlab* slab
   if (local < 0 || local >= sb.rows) return;
   const TI* re = (const TI*)sb.re + local * sb.ld;
   const TI* im = sb.im ? (const TI*)sb.im + local * sb.ld : nullptr;
-  slice_row<TI, NEG>(re, im, sb.K, S, out, row, lane);
+  const int64_t dcol = (sb.diag0 != kNoDiag && out.dg && !sb.im) ? local + sb.diag0 : -1;
+  slice_row<TI, NEG>(re, im, sb.K, S, out, row, lane, (dcol >= 0 && dcol < sb.K) ? dcol : -1);
 }
 
 void make_map_u8(CUtensorMap* m, const int8_t* base, int64_t rows, int64_t cols, int64_t ld, int box_rows);
@@ -735,7 +863,7 @@ void prepare_gemm_i8_grouped(int S) {
 template <typename TO>
 void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitch, int64_t a_rows, int64_t b_rows,
                             const int* aexp, const int* bexp, const GProblem* probs, const GTile* tiles, int ntiles,
-                            int* err, unsigned timeout_ms, cudaStream_t s) {
+                            int* err, unsigned timeout_ms, cudaStream_t s, const double* adg, const double* bdg) {
   if (nterms < 1 || nterms > kMaxTerms) throw Error{FX_ERR_VALUE, "int8 product: 1 or 2 terms"};
   if (ntiles <= 0) return;
   if (pitch % kBK || pitch <= 0 || pitch > 32768) throw Error{FX_ERR_VALUE, "grouped int8 product: bad pitch"};
@@ -748,6 +876,8 @@ void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitc
   p.timeout_ns = (unsigned long long)timeout_ms * 1000000ull;
   p.probs = probs;
   p.tiles = tiles;
+  p.adg = adg;
+  p.bdg = bdg;
   if (S == 4)
     launch_i8_grouped_cfg<4, TO>(p, terms, nterms, pitch, a_rows, b_rows, ntiles, s);
   else if (S == 5)
@@ -757,9 +887,9 @@ void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitc
 }
 template void launch_gemm_i8_grouped<float>(int, const I8Term*, int, int64_t, int64_t, int64_t, const int*,
                                             const int*, const GProblem*, const GTile*, int, int*, unsigned,
-                                            cudaStream_t);
+                                            cudaStream_t, const double*, const double*);
 template void launch_gemm_i8_grouped<double>(int, const I8Term*, int, int64_t, int64_t, int64_t, const int*,
                                              const int*, const GProblem*, const GTile*, int, int*, unsigned,
-                                             cudaStream_t);
+                                             cudaStream_t, const double*, const double*);
 
 }  // namespace fx

@@ -153,6 +153,7 @@ struct I8Slices {
   int8_t* neg_im[5];
   int* exp;
   int64_t ld;   // bytes between rows of a slice
+  double* dg;   // grouped slicing: per row, the diagonal element left out of the slices
 };
 template <typename TI>
 void launch_slice_rows(int S, const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K,
@@ -171,6 +172,15 @@ struct GProblem {
   int64_t ldd;
   void* Dt;             // optional: also store D^T here (non-symmetric problems only)
   int64_t ldt;
+  // Diagonal split (square problems whose slabs left the diagonal out, GSlab::diag0 = 0):
+  // A Bt^T = A' B'^T + a_ii B_ij + A'_ij b_jj with the diagonals a, b from I8Slices::dg and the
+  // FP64 masters A (ldam) and Bt (ldbm) read in the epilogue.  split: 0 off; 1 on; 2 on, and A
+  // is symmetric (read by columns; Am 16-byte aligned with ldam even for split 1).
+  int split;
+  const void* Am;
+  int64_t ldam;
+  const void* Btm;
+  int64_t ldbm;
 };
 // One output tile of a grouped launch: problem, tile coordinates (BM = 128, BN = the launch's
 // tile width: 128 for 4 slices, 96 for 5), and the K steps [kb0, kb1) of 64 bytes to run (a
@@ -225,7 +235,8 @@ void set_product_error(const std::string& msg);
 template <typename TO>
 void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitch, int64_t a_rows,
                             int64_t b_rows, const int* aexp, const int* bexp, const GProblem* probs,
-                            const GTile* tiles, int ntiles, int* err, unsigned timeout_ms, cudaStream_t s);
+                            const GTile* tiles, int ntiles, int* err, unsigned timeout_ms, cudaStream_t s,
+                            const double* adg = nullptr, const double* bdg = nullptr);
 // Grouped slicing: slab k copies rows [0, rows_k) of a planar (re, im) source with leading
 // dimension ld_k, K_k columns, into stacked rows [row0_k, row0_k + rows_k).  Slabs are sorted
 // by row0 and do not overlap; rows between slabs are left alone.
@@ -233,8 +244,11 @@ struct GSlab {
   const void* re;
   const void* im;
   int64_t ld;
-  int rows, K, row0, pad;
+  int rows, K, row0;
+  int diag0;            // kNoDiag, or: local row r holds its diagonal element at column r + diag0,
+                        // which is left out of the slices and written to I8Slices::dg
 };
+constexpr int kNoDiag = -(1 << 30);
 template <typename TI>
 void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, I8Slices out,
                                bool want_neg_im, cudaStream_t s);

@@ -136,6 +136,10 @@ def make_dataset(count: int, seed: int, nmin: int = 64, nmax: int = 1024, tmin: 
             "cert_m": cat(cm), "cert_s": cat(cs), "meta": np.array(meta, dtype=object)}
 
 
+def merge(*sets: dict) -> dict:
+    return {k: np.concatenate([d[k] for d in sets]) for k in sets[0]}
+
+
 def rho_up(features: np.ndarray) -> np.ndarray:
     """min(||Y||_1, d4, d6) from the features (columns 1, 6, 7 are their log2)."""
     f = np.asarray(features, dtype=np.float64)

@@ -88,18 +88,26 @@ def main(argv=None):
     ap.add_argument("--test", type=int, default=2000)
     ap.add_argument("--epochs", type=int, default=80)
     ap.add_argument("--nmax", type=int, default=1024)
+    ap.add_argument("--train-large", type=int, default=1200, help="extra training walks with n in [nmax, nmax-large]")
+    ap.add_argument("--test-large", type=int, default=300)
+    ap.add_argument("--nmax-large", type=int, default=4096)
     ap.add_argument("--e2e", type=int, default=64)
     ap.add_argument("--out", default=os.path.join(DATA, "selector_weights.npz"))
     ap.add_argument("--report", default=os.path.join(DATA, "selector_eval.json"))
     a = ap.parse_args(argv)
     t0 = time.time()
-    ds_train = selector.make_dataset(a.train, seed=1, nmax=a.nmax)
-    ds_test = selector.make_dataset(a.test, seed=2, nmax=a.nmax)
+    ds_train = selector.merge(selector.make_dataset(a.train, seed=1, nmax=a.nmax),
+                              selector.make_dataset(a.train_large, seed=4, nmin=a.nmax, nmax=a.nmax_large,
+                                                    chunk=32))
+    ds_test = selector.merge(selector.make_dataset(a.test, seed=2, nmax=a.nmax),
+                             selector.make_dataset(a.test_large, seed=5, nmin=a.nmax, nmax=a.nmax_large,
+                                                   chunk=32))
     t1 = time.time()
     w, losses = selector.train(ds_train, epochs=a.epochs)
     t2 = time.time()
     selector.save(a.out, w, losses=losses)
-    rep = {"train": a.train, "test": a.test, "n_range": [64, a.nmax], "t_range": [0.1, 1000.0],
+    rep = {"train": a.train + a.train_large, "test": a.test + a.test_large, "n_range": [64, a.nmax_large],
+           "t_range": [0.1, 1000.0],
            "epochs": a.epochs, "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
            "seconds_data": round(t1 - t0, 1), "seconds_train": round(t2 - t1, 1),
            "train_eval": evaluate(w, ds_train), "heldout": evaluate(w, ds_test)}

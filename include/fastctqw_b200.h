@@ -173,7 +173,10 @@ enum fx_batch_option {
   FX_BATCH_OPT_TIMEOUT_MS = 1,  /* bound of every device-side wait (default 2000)               */
   FX_BATCH_OPT_FORCE_M = 2,     /* diagnostics: force the Pade degree (-1 automatic)            */
   FX_BATCH_OPT_SELECTOR = 3,    /* as FX_OPT_SELECTOR                                           */
-  FX_BATCH_OPT_ANALYZE_ONLY = 4 /* 1: stop after the selection (features and (m, s) only)       */
+  FX_BATCH_OPT_ANALYZE_ONLY = 4, /* 1: stop after the selection (features and (m, s) only)      */
+  FX_BATCH_OPT_DIAG_SPLIT = 5    /* mask, default 3: products of the solve that take their       */
+                                 /* operands' diagonals out of the int8 slices and add those    */
+                                 /* terms in FP64; 1 V^2, W^2, VW; 2 P2 L^-T and Z L^-1          */
 };
 /* count walks of sizes n[0..count); dtype FX_C64 or FX_C128 (of X, psi0 and psi). */
 int fx_batch_create(size_t count, const int64_t* n, int dtype, fx_batch_handle* out);
