@@ -269,6 +269,69 @@ def bench_batch(args, dev):
     }
 
 
+def bench_device_setup(args, dev, A: np.ndarray):
+    """Walk set-up and read-out on the device against the reference's host steps, at the
+    bench's N: X = -1j*H*t from the graph (Operator._buildHamiltonian/_buildUnitory,
+    FastCTQW/Operator.py:49-56) and the Hermitian check (:92-103) in numpy on the host, vs
+    fx_build_generator from the edge list and fx_check_hermitian on the device; and a 20-point
+    time curve at N = 2048 (stepped propagator vs one walk per time)."""
+    import time
+    import torch
+    from fastctqw_b200 import device as fd
+    from fastctqw_b200 import graphs
+    n, t = A.shape[0], args.t
+    t0 = time.perf_counter()
+    H = -1.0 * np.asarray(np.diag(A.sum(axis=1)) - A, dtype=np.complex64)
+    X_host = np.asarray(-1j * H * t, dtype=np.complex64)
+    t1 = time.perf_counter()
+    herm_host = bool(np.allclose(H, H.conj().T))
+    t2 = time.perf_counter()
+    del H
+    u, v = np.nonzero(np.triu(A, 1))
+    edges = torch.from_numpy(np.stack([u, v], 1).astype(np.int64)).to(dev)
+    out = torch.empty((n, n), dtype=torch.complex64, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for _ in range(2):
+        fd.build_generator(n, edges, t, 1.0, True, np.complex64, out=out)
+    torch.cuda.synchronize()
+    ev[0].record()
+    fd.build_generator(n, edges, t, 1.0, True, np.complex64, out=out)
+    ev[1].record()
+    herm_dev = fd.is_hermitian(out, skew=True)   # X = -iHt skew-Hermitian <=> H Hermitian
+    ev[2].record()
+    torch.cuda.synchronize()
+    same = bool(np.array_equal(out.cpu().numpy(), X_host))
+    del out, edges, X_host
+    torch.cuda.empty_cache()
+    # time curve: 20 uniform times on G(2048, 0.05), marked nodes 0..7
+    from fastctqw_b200.Ctqw import Ctqw
+    from fastctqw_b200.State import State
+    m = 2048
+    Ag = graphs.erdos_renyi(m, 0.05, seed=args.seed, dtype=np.float32)
+    adj = [np.nonzero(Ag[i])[0] for i in range(m)]
+    w = Ctqw.from_adjacency_list(adj, State.getSingleNodeState(m, 0))
+    grid = 0.25 * np.arange(1, 21)
+    res = {}
+    for method in ("steps", "batch"):
+        w.runWalks(grid, list(range(8)), method=method)
+        torch.cuda.synchronize()
+        s0 = time.perf_counter()
+        curve = w.runWalks(grid, list(range(8)), method=method)
+        torch.cuda.synchronize()
+        res[method] = (round((time.perf_counter() - s0) * 1e3, 2), curve)
+    w.free()
+    return {
+        "n": n, "workload": f"G(n={n}, p=0.5) Laplacian, t={t}, complex64",
+        "host_build_X_ms": round((t1 - t0) * 1e3, 1), "host_hermitian_check_ms": round((t2 - t1) * 1e3, 1),
+        "device_build_X_ms": round(ev[0].elapsed_time(ev[1]), 3),
+        "device_hermitian_check_ms": round(ev[1].elapsed_time(ev[2]), 3),
+        "device_X_equals_host_X": same, "hermitian_host_H": herm_host, "skew_hermitian_device_X": herm_dev,
+        "time_curve": {"workload": "G(2048, 0.05) adjacency, 20 times 0.25..5.0, 8 marked nodes, complex64",
+                       "steps_ms": res["steps"][0], "batch_ms": res["batch"][0],
+                       "max_abs_diff": float(np.abs(res["steps"][1] - res["batch"][1]).max())},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -288,6 +351,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch leg")
     ap.add_argument("--no-batch-loop", action="store_true", help="skip the per-walk loop of the batch leg")
     ap.add_argument("--batch-only", action="store_true", help="run only the uneven-batch leg")
+    ap.add_argument("--no-setup", action="store_true", help="skip the device set-up / time-curve leg")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-nmin", type=int, default=64)
     ap.add_argument("--batch-nmax", type=int, default=2048)
@@ -448,6 +512,12 @@ def main():
         del dX, dU, dpsi0, dpsi
         torch.cuda.empty_cache()
         batch = bench_batch(args, dev)
+    setup = None
+    if rank == 0 and world == 1 and not args.no_setup:
+        if not eng._freed:
+            eng.close()
+        torch.cuda.empty_cache()
+        setup = bench_device_setup(args, dev, A)
 
     if rank == 0:
         out = {
@@ -464,6 +534,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "clocks": clk, "e2e": e2e, "gpu_launches": int(st["launches"]) * args.steps,
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "batch": batch,
+            "device_setup": setup,
             "plain_selection": plain,
             "chosen_vs_plain_speedup": round(plain["ms"] / ms_per_step, 3) if plain else None,
             "algorithmic_tflops": round(st["flops"] / (ms_per_step * 1e-3) / 1e12, 2),

@@ -22,7 +22,10 @@ class Ctqw:
         self._device = device
         self.ctqwId = ctqwId
         self._initStator = initState
-        if isinstance(data, np.ndarray):
+        if isinstance(data, Operator):
+            self._n = data._n
+            self._Operator = data
+        elif isinstance(data, np.ndarray):
             self._n = data.shape[0]
             self._Operator = Operator.from_numpy_array(data, gamma, laplacian, device)
         elif isinstance(data, (int, np.integer)):
@@ -49,6 +52,16 @@ class Ctqw:
                    device=device, ctqwId=ctqwId)
 
     @classmethod
+    def from_adjacency_list(cls, adj_list, initState: State, time: float = 1, gamma: float = 1,
+                            laplacian: bool = False, ctqwId: str = "Undef", dtype=np.float32,
+                            device: str = "cuda") -> "Ctqw":
+        """Walk on the undirected graph ``adj_list[u]`` = neighbours of u, with H built on the
+        device from the edges (FastCTQW/Ctqw.py:60-71 declares this constructor, with the same
+        parameters, but leaves it empty; ``time`` is accepted for that signature and unused)."""
+        return cls(Operator.from_adjacency_list(adj_list, gamma, laplacian, device, dtype), initState,
+                   device=device, ctqwId=ctqwId)
+
+    @classmethod
     def from_num_nodes(cls, n: int, initState: State | None = None, dtype=np.complex64,
                        device: str = "cuda") -> "Ctqw":
         return cls(n, initState, dtype=dtype, device=device)
@@ -68,6 +81,17 @@ class Ctqw:
     def runWalk(self, time: float = 0):
         psi = self._Operator.propagate(time, self._initStator.getState())
         self._finalStator.setState(psi.astype(np.complex64, copy=False))
+
+    def runWalks(self, times, markNodes=None, method: str = "auto") -> np.ndarray:
+        """Probabilities at the marked nodes (all nodes when None) for every time: shape
+        (len(times), len(markNodes)), the ``target_state`` that ``Plot.timeCurve`` plots
+        (FastCTQW/Plot.py:35-49).  The final state becomes the state at the last time.  See
+        ``Operator.time_curve`` for ``method``."""
+        probs = self._Operator.time_curve(times, self._initStator.getState(), markNodes, method)
+        last = getattr(self._Operator, "_last_state", None)
+        if last is not None:
+            self._finalStator.setState(last.cpu().numpy().astype(np.complex64, copy=False))
+        return probs
 
     def getFinalState(self) -> State:
         return self._finalStator

@@ -14,7 +14,12 @@ Differences from the reference, all deliberate:
 * ``propagate(t, psi0)`` returns U psi0 without copying U to the host; ``getOperator()``
   fetches U lazily afterwards,
 * ``from_num_nodes`` / ``reset_networkx_graph`` pass their arguments to the right
-  parameters (the reference mixed them up, :118-120, :144-146).
+  parameters (the reference mixed them up, :118-120, :144-146),
+* ``from_adjacency_list`` (a stub in the reference, :115-117) keeps the graph as an edge list
+  on the device and builds X = -i H t there for every time (``fastctqw_b200.device``); no
+  N x N host matrix is made,
+* ``time_curve(times, psi0, nodes)`` gives the probabilities of a walk at many times: one
+  propagator stepped along a uniform grid, or one grouped batch of walks otherwise.
 """
 from __future__ import annotations
 
@@ -36,6 +41,7 @@ class Operator:
         self._device = device
         self._expmMat = None
         self._walked = False
+        self._edges = None
         if isinstance(data, np.ndarray):
             if not self._is_adjacency_matrix(data):
                 raise ValueError("A is not a adj matrix")
@@ -80,17 +86,94 @@ class Operator:
             return ExpMatComplex128(n)
         raise TypeError(f"dtype {dtype} is not supported")
 
+    @property
+    def _engine(self):
+        return self._expMator._backend._engine
+
     def buildExpmOperator(self, time: float) -> None:
         """U = expm(-i H t), kept as a host array (FastCTQW/Operator.py:70-78)."""
-        self._expmMat = self._expMator.run(self._buildUnitory(time))
+        if self._edges is not None:
+            import torch
+            dX = self._generator_device(time)
+            dU = torch.empty_like(dX)
+            self._engine.run_device(dX, dU)
+            self._expmMat = dU.cpu().numpy()
+        else:
+            self._expmMat = self._expMator.run(self._buildUnitory(time))
         self._walked = False
 
     def propagate(self, time: float, psi0: np.ndarray) -> np.ndarray:
         """psi = expm(-i H t) psi0 on the device; U stays there until getOperator()."""
-        psi = self._expMator._backend._engine.walk_host(self._buildUnitory(time), psi0)
+        if self._edges is not None:
+            import torch
+            dX = self._generator_device(time)
+            p0 = torch.from_numpy(np.ascontiguousarray(psi0, dtype=self._dtype)).cuda()
+            dpsi = torch.empty_like(p0)
+            self._engine.walk_device(dX, p0, dpsi)
+            psi = dpsi.cpu().numpy()
+            self._expmMat = None
+            self._walked = False   # U of a device-built walk is not kept for getOperator
+            return psi
+        psi = self._engine.walk_host(self._buildUnitory(time), psi0)
         self._expmMat = None
         self._walked = True
         return psi
+
+    def _generator_device(self, time: float, out=None):
+        """X = -1j * H * t as a device tensor (built there for an edge-list operator)."""
+        if self._edges is not None:
+            from .device import build_generator
+            return build_generator(self._n, self._edges, time, self._gamma, self._laplacian, self._dtype, out=out)
+        import torch
+        X = torch.from_numpy(self._buildUnitory(time))
+        return X.cuda() if out is None else out.copy_(X)
+
+    def time_curve(self, times, psi0: np.ndarray, nodes=None, method: str = "auto") -> np.ndarray:
+        """Probabilities |psi(t)_v|^2 for every t of ``times`` and every node v of ``nodes``
+        (all nodes when None): an array of shape (len(times), len(nodes)), the ``target_state``
+        of ``Plot.timeCurve`` (FastCTQW/Plot.py:35-49).
+
+        method "steps": the times must be the uniform grid t_k = (k + 1) dt; one exponential
+        gives U(dt) and psi(t_k) = U(dt) psi(t_{k-1}) (one GEMV per time; the error grows with
+        the number of steps by the rounding of U to the walk's dtype).  "batch": one walk per
+        time through the grouped batch pipeline (each at the single-walk accuracy).  "auto":
+        "steps" on a uniform grid, else "batch"."""
+        import torch
+        from .device import apply_propagator, probabilities
+        times = np.asarray(times, dtype=np.float64).reshape(-1)
+        K = times.shape[0]
+        if K == 0:
+            return np.zeros((0, self._n if nodes is None else len(nodes)))
+        uniform = bool(times[0] > 0 and np.allclose(times, times[0] * np.arange(1, K + 1), rtol=1e-12, atol=0.0))
+        if method not in ("auto", "steps", "batch"):
+            raise ValueError(f"unknown method {method!r}")
+        if method == "steps" and not uniform:
+            raise ValueError('method="steps" needs times t_k = (k + 1) * t_0')
+        p0 = torch.from_numpy(np.ascontiguousarray(psi0, dtype=self._dtype)).cuda()
+        nd = None if nodes is None else torch.as_tensor(np.asarray(nodes, dtype=np.int64)).cuda()
+        rows = []
+        if method == "steps" or (method == "auto" and uniform):
+            dX = self._generator_device(float(times[0]))
+            dU = torch.empty_like(dX)
+            a, b = torch.empty_like(p0), torch.empty_like(p0)
+            self._engine.walk_device(dX, p0, a, dU)
+            del dX
+            rows.append(probabilities(a, nd))
+            for _ in range(1, K):
+                apply_propagator(dU, a, b)
+                rows.append(probabilities(b, nd))
+                a, b = b, a
+            self._last_state = a
+        else:
+            from .batch import WalkBatch
+            with WalkBatch([self._n] * K, self._dtype) as wb:
+                dXs = [self._generator_device(float(t)) for t in times]
+                outs = [torch.empty_like(p0) for _ in range(K)]
+                wb.run_device(dXs, [p0] * K, outs)
+                del dXs
+            rows = [probabilities(o, nd) for o in outs]
+            self._last_state = outs[-1]
+        return torch.stack(rows).cpu().numpy()
 
     def configure(self, **kw) -> None:
         self._expMator.configure(**kw)
@@ -127,6 +210,31 @@ class Operator:
     @classmethod
     def from_num_nodes(cls, n: int, dtype=np.complex64, device: str = "cuda") -> "Operator":
         return cls(n, device=device, dtype=dtype)
+
+    @classmethod
+    def from_adjacency_list(cls, adj_list, gamma: float = 1, laplacian: bool = False, device: str = "cuda",
+                            dtype=np.float32) -> "Operator":
+        """Operator of the undirected graph with ``adj_list[u]`` = neighbours of u (edges are
+        symmetrised; a repeated edge counts once).  ``dtype`` float32/complex64 -> complex64
+        walk, float64/complex128 -> complex128, as for an adjacency matrix.  The edges live on
+        the device and X = -i H t is built there (the reference declares this constructor but
+        leaves it empty, FastCTQW/Operator.py:115-117)."""
+        from .device import edges_from_adjacency_list
+        return cls._from_edges(len(adj_list), edges_from_adjacency_list(adj_list), gamma, laplacian, device, dtype)
+
+    @classmethod
+    def _from_edges(cls, n: int, edges: np.ndarray, gamma: float, laplacian: bool, device: str,
+                    dtype) -> "Operator":
+        import torch
+        op = cls(int(n), device=device, dtype=cls._dtype_for(np.zeros(0, dtype=dtype)))
+        op._gamma = gamma
+        op._laplacian = laplacian
+        e = np.ascontiguousarray(edges, dtype=np.int64).reshape(-1, 2)
+        if e.size and (e.min() < 0 or e.max() >= n):
+            raise ValueError("an edge endpoint is outside 0..n-1")
+        op._edges = torch.from_numpy(e).cuda()
+        op._hamiltonian = None
+        return op
 
     def reset_numpy_array(self, A: np.ndarray, gamma: float = 1, laplacian: bool = False):
         self._dtype = self._dtype_for(A)

@@ -69,6 +69,15 @@ SIGNATURES = {
                        ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int64,
                        ctypes.c_float, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
     "fx_product_error": [],
+    "fx_build_generator": [ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int,
+                           ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    "fx_check_hermitian": [ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                           ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p],
+    "fx_apply_propagator": [ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.c_void_p],
+    "fx_probabilities": [ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                         ctypes.c_void_p, ctypes.c_void_p],
+    "fx_graph_error": [],
     "fx_product_f32_noalloc": [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
                                ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int64,
@@ -106,6 +115,7 @@ SIGNATURES = {
 RESTYPES = {"fx_last_error": ctypes.c_char_p, "fx_version": ctypes.c_char_p,
             "fx_batch_last_error": ctypes.c_char_p, "fx_mlp_error": ctypes.c_char_p,
             "fx_product_error": ctypes.c_char_p,
+            "fx_graph_error": ctypes.c_char_p,
             "fx_gpu_memory_gb": ctypes.c_double}
 
 

@@ -222,6 +222,35 @@ int fx_mlp_train(float* w, const float* x, const int32_t* ym, const float* ys, i
                  int batch, float lr, float lambda, uint64_t seed, float* epoch_loss, void* stream);
 const char* fx_mlp_error(void);
 
+/* ---- Device-side set-up and read-out around the propagator (device pointers; stream may be
+ * NULL).  These replace O(N^2) host steps of the reference's walk.  No device allocation.
+ *
+ * X = -1j * H * t for H = -gamma A (laplacian = 0) or -gamma (D - A) (laplacian = 1) of the
+ * undirected graph whose m edges are the int64 pairs edges[2k], edges[2k + 1] (repeated edges
+ * count once; a self-loop sets A_uu = 1).  Replaces Operator._buildHamiltonian and
+ * _buildUnitory (FastCTQW/Operator.py:49-56) on nx.to_numpy_array of the graph
+ * (FastCTQW/Ctqw.py:57; Ctqw.from_adjacency_list, FastCTQW/Ctqw.py:60-71, is a stub in the
+ * reference).  X: n x n row-major, FX_C64 or FX_C128; entries rounded as numpy rounds those
+ * expressions in that dtype.  Synchronises the stream; FX_ERR_VALUE if an endpoint is outside
+ * 0..n-1. */
+int fx_build_generator(int64_t n, const int64_t* edges, int64_t m, double gamma, int laplacian,
+                       double t, int dtype, void* X, void* stream);
+/* *hermitian = np.allclose(H, H^H, rtol, atol) for an n x n row-major H of any fx_dtype, in one
+ * pass over H (Operator._is_hermitian, FastCTQW/Operator.py:92-103); with skew = 1 the same
+ * test of H against -H^H (a walk's X = -iHt is skew-Hermitian exactly when H is Hermitian).
+ * Synchronises the stream. */
+int fx_check_hermitian(int64_t n, int dtype, const void* H, double rtol, double atol, int skew,
+                       int32_t* hermitian, void* stream);
+/* psi_out = U psi_in (the GEMV of Ctqw.runWalk, FastCTQW/Ctqw.py:90-94), complex64 or
+ * complex128, FP64 accumulation; for stepping a state along a time grid with one U. */
+int fx_apply_propagator(int64_t n, int dtype, const void* U, const void* psi_in, void* psi_out,
+                        void* stream);
+/* prob[k] = |psi[nodes[k]]|^2 in FP64 for k < count, or |psi[k]|^2 for every k < n when nodes is
+ * NULL (State.getProbabilities, FastCTQW/State.py:50-51).  A node outside 0..n-1 gives NaN. */
+int fx_probabilities(int64_t n, int dtype, const void* psi, const int64_t* nodes, int64_t count,
+                     double* prob, void* stream);
+const char* fx_graph_error(void);
+
 /* Device memory currently in use on the current device, GB. */
 double fx_gpu_memory_gb(void);
 /* 1 if a device with compute capability 10.x is present. */
