@@ -570,6 +570,7 @@ __device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t 
   // slices and stored to out.dg[orow]
   const bool vec = ((reinterpret_cast<uintptr_t>(rre) | reinterpret_cast<uintptr_t>(rim)) & 15) == 0;
   double mx = 0.0;
+#pragma unroll 4
   for (int64_t k0 = (int64_t)lane * 4; k0 < K; k0 += 128) {
     double v[4];
     load4<TI>(rre, k0, K, vec, v);
@@ -607,18 +608,18 @@ __device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t 
       for (int j = 0; j < 4; ++j) {
         if (plane == 0 && k0 + j == dcol) x[j] = 0.0;
         const double xs = one_factor ? x[j] * scale : ldexp(ldexp(x[j], -e), 7 * S);
-        long long r = __double2ll_rn(xs);
+        // v and every remainder are integers below 2^35 in magnitude, so this runs exactly in
+        // FP64: t = rint(r 2^-k) (round half to even), r -= t 2^k
+        double r = rint(xs);
 #pragma unroll
         for (int q = 0; q < kMaxSlices; ++q) {
           if (q >= S) continue;
           int d;
           if (q < S - 1) {
             const int k = 7 * (S - 1 - q);
-            const long long half = 1ll << (k - 1);
-            long long t = (r + half) >> k;                       // round half up
-            if (((r + half) & ((1ll << k) - 1)) == 0 && (t & 1)) t -= 1;   // ties to even
+            const double t = rint(r * pow2_or_zero(-k));
+            r = fma(-t, pow2_or_zero(k), r);
             d = (int)t;
-            r -= t << k;
           } else {
             d = (int)r;
           }
