@@ -269,6 +269,47 @@ def bench_batch(args, dev):
     }
 
 
+def bench_batch_sharded(args, dev, rank, world):
+    """The uneven batch sharded over the ranks (longest-processing-time by the cost model, one
+    WalkBatch per rank, states gathered on rank 0; fastctqw_b200.shard).  Host buffers in and
+    out; wall time between barriers, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from fastctqw_b200 import shard
+    from fastctqw_b200.batch import WalkBatch
+    specs, As, Xs, P0 = batch_workload(args.batch_count, args.seed, args.batch_nmin, args.batch_nmax)
+    cache = {}
+
+    def runner(xs, ps):
+        key = tuple(X.shape[0] for X in xs)
+        if key not in cache:
+            cache[key] = WalkBatch(list(key), np.complex64, selector=args.selector)
+        return cache[key].run(xs, ps)
+
+    if args.selector == "learned":
+        from fastctqw_b200 import selector as sel
+        sel.set_weights()
+    for _ in range(max(1, args.warmup)):
+        shard.run_sharded(Xs, P0, runner=runner)
+    times = []
+    for _ in range(max(1, min(args.steps, 3))):
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        shard.run_sharded(Xs, P0, runner=runner)
+        torch.cuda.synchronize()
+        dist.barrier()
+        times.append(time.perf_counter() - t0)
+    t = torch.tensor([min(times)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    for b in cache.values():
+        b.close()
+    ms = float(t.item()) * 1e3
+    return {"workload": f"{args.batch_count} uneven walks sharded over {world} ranks (LPT by F(N, m, s))",
+            "ms": round(ms, 2), "walks_per_s": round(args.batch_count / (ms * 1e-3), 1),
+            "scaling": "strong", "timing": "wall, host buffers in and out, max over ranks"}
+
+
 def bench_device_setup(args, dev, A: np.ndarray):
     """Walk set-up and read-out on the device against the reference's host steps, at the
     bench's N: X = -1j*H*t from the graph (Operator._buildHamiltonian/_buildUnitory,
@@ -352,6 +393,8 @@ def main():
     ap.add_argument("--no-batch-loop", action="store_true", help="skip the per-walk loop of the batch leg")
     ap.add_argument("--batch-only", action="store_true", help="run only the uneven-batch leg")
     ap.add_argument("--no-setup", action="store_true", help="skip the device set-up / time-curve leg")
+    ap.add_argument("--batch-shard", action="store_true",
+                    help="with N > 1 ranks: also run the uneven batch sharded over the ranks")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-nmin", type=int, default=64)
     ap.add_argument("--batch-nmax", type=int, default=2048)
@@ -512,6 +555,11 @@ def main():
         del dX, dU, dpsi0, dpsi
         torch.cuda.empty_cache()
         batch = bench_batch(args, dev)
+    if world > 1 and args.batch_shard:
+        if not eng._freed:
+            eng.close()
+        torch.cuda.empty_cache()
+        batch = bench_batch_sharded(args, dev, rank, world)
     setup = None
     if rank == 0 and world == 1 and not args.no_setup:
         if not eng._freed:
