@@ -50,21 +50,45 @@ struct Planes4 {
   const double* m[4];
 };
 
-// D = sum_k c_k M_k + g I on the np x np block of every listed walk; coef[w] = (c0..c3, g).
-__global__ void kb_combo(double* D, Planes4 M, const int* list, const BWalk* wk, const double* coef) {
-  const int w = list[blockIdx.y];
-  const BWalk b = wk[w];
-  const int64_t n2 = (int64_t)b.np * b.np;
-  const double* c = coef + 5 * w;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    double v = 0.0;
+// Elementwise work over walks of uneven sizes is cut into row chunks of about kChunkElems
+// elements (one CTA each, any walk), so that large and small walks load the GPU evenly.
+constexpr int kChunkElems = 16384;
+struct RChunk {
+  int w, r0, r1, pad;   // walk, rows [r0, r1)
+};
+
+// D = sum_k c_k M_k + g I on the np x np block of every chunk's walk; coef[w] = (c0..c3, g).
+// Two elements per thread (np is even); 32-bit indices within the chunk.
+__global__ void kb_combo(double* D, Planes4 M, const RChunk* ch, const BWalk* wk, const double* coef) {
+  const RChunk q = ch[blockIdx.x];
+  const BWalk b = wk[q.w];
+  const double* c = coef + 5 * q.w;
+  const uint32_t half = (uint32_t)b.np / 2, total = (uint32_t)(q.r1 - q.r0) * half;
+  const double2* src[4];
+  double cc[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k)   // a zero coefficient skips the term: its plane may be unset
-      if (M.m[k] && c[k] != 0.0) v += c[k] * M.m[k][b.off + idx];
-    const int64_t i = idx / b.np;
-    if (idx - i * b.np == i) v += c[4];
-    D[b.off + idx] = v;
+  for (int k = 0; k < 4; ++k) {   // a zero coefficient skips the term: its plane may be unset
+    const bool on = M.m[k] && c[k] != 0.0;
+    cc[k] = on ? c[k] : 0.0;
+    src[k] = on ? reinterpret_cast<const double2*>(M.m[k] + b.off) : nullptr;
+  }
+  const double g = c[4];
+  double2* dst = reinterpret_cast<double2*>(D + b.off);
+  for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
+    const uint32_t rr = t / half, c2 = t - rr * half;
+    const int64_t r = q.r0 + (int64_t)rr;
+    const int64_t e2 = r * half + c2;   // double2 index of (r, 2 c2)
+    double vx = 0.0, vy = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (src[k]) {
+        const double2 m = src[k][e2];
+        vx += cc[k] * m.x;
+        vy += cc[k] * m.y;
+      }
+    if (2 * (int64_t)c2 == r) vx += g;
+    else if (2 * (int64_t)c2 + 1 == r) vy += g;
+    dst[e2] = make_double2(vx, vy);
   }
 }
 
@@ -249,16 +273,17 @@ __global__ void kb_walk_vec_reduce(const double* v, const int* list, const BWalk
   }
   if (threadIdx.x == 0) out[(int64_t)w * stride + slot] = sh[0];
 }
-// E <- E - (r_i + r_j)/n + T/n^2 on the n x n block (E symmetric, r its row sums, T = sum r).
-__global__ void kb_apply_proj(double* E, const int* list, const BWalk* wk, const double* rs, const double* tot) {
-  const int w = list[blockIdx.y];
-  const BWalk b = wk[w];
-  const int64_t n2 = (int64_t)b.n * b.n;
-  const double inv = 1.0 / b.n, sig = tot[w] * inv * inv;
+// E <- E - (r_i + r_j)/n + T/n^2 on the n x n block (E symmetric, r its row sums, T = sum r),
+// rows [r0, r1) of the chunk's walk.
+__global__ void kb_apply_proj(double* E, const RChunk* ch, const BWalk* wk, const double* rs, const double* tot) {
+  const RChunk q = ch[blockIdx.x];
+  const BWalk b = wk[q.w];
+  const double inv = 1.0 / b.n, sig = tot[q.w] * inv * inv;
   const double* r = rs + b.row0;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = idx / b.n, j = idx - i * b.n;
+  const uint32_t n = (uint32_t)b.n, total = (uint32_t)(q.r1 - q.r0) * n;
+  for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
+    const uint32_t ii = t / n, j = t - ii * n;
+    const int64_t i = q.r0 + (int64_t)ii;
     double& e = E[b.off + i * b.np + j];
     e = e - r[i] * inv - r[j] * inv + sig;
   }
@@ -301,18 +326,19 @@ __global__ void kb_symmetrize(double* A, const int* list, const BWalk* wk) {
     __syncthreads();
   }
 }
-// Zero every listed walk's block, then copy the diagonal 128 x 128 blocks of L^-1 (stored
-// per walk as np x 128, block j at rows [128 j, 128 j + 128)) into X.
-__global__ void kb_init_inverse(double* X, const double* Linv, const int* list, const BWalk* wk, const int64_t* loff) {
-  const int w = list[blockIdx.y];
-  const BWalk b = wk[w];
-  const int64_t n2 = (int64_t)b.np * b.np;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = idx / b.np, j = idx - i * b.np;
+// Zero the chunk's rows of its walk's block, then copy the diagonal 128 x 128 blocks of L^-1
+// (stored per walk as np x 128, block j at rows [128 j, 128 j + 128)) into X.
+__global__ void kb_init_inverse(double* X, const double* Linv, const RChunk* ch, const BWalk* wk, const int64_t* loff) {
+  const RChunk q = ch[blockIdx.x];
+  const BWalk b = wk[q.w];
+  const uint32_t np = (uint32_t)b.np, total = (uint32_t)(q.r1 - q.r0) * np;
+  for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
+    const uint32_t ii = t / np, j = t - ii * np;
+    const int64_t i = q.r0 + (int64_t)ii;
+    const int64_t bi = i / kNb;
     double v = 0.0;
-    if (i / kNb == j / kNb) v = Linv[loff[w] + i * kNb + (j - (i / kNb) * kNb)];
-    X[b.off + idx] = v;
+    if (bi == (int64_t)(j / kNb)) v = Linv[loff[q.w] + i * kNb + (j - bi * kNb)];
+    X[b.off + i * b.np + j] = v;
   }
 }
 
@@ -438,10 +464,12 @@ __global__ void kb_est_init(const int* list, const BWalk* wk, double* scr, doubl
     est[4 * w + 2] = 0.0;
   }
 }
-// (out0, out1) = M (in0, in1) for every listed walk that is not done; warp per row.
-__global__ void kb_est_matvec(const double* M, const int* list, const BWalk* wk, double* scr, const double* est,
+// (out0, out1) = M (in0, in1) on the chunk's rows of its walk, unless that walk is done; warp
+// per row.
+__global__ void kb_est_matvec(const double* M, const RChunk* ch, const BWalk* wk, double* scr, const double* est,
                               int in0, int out0) {
-  const int w = list[blockIdx.y];
+  const RChunk q = ch[blockIdx.x];
+  const int w = q.w;
   if (est[4 * w + 2] != 0.0) return;
   const BWalk b = wk[w];
   const double* x0 = est_vec(scr, b, in0);
@@ -450,7 +478,7 @@ __global__ void kb_est_matvec(const double* M, const int* list, const BWalk* wk,
   double* y1 = est_vec(scr, b, out0 + 1);
   const double* A = M + b.off;
   const int lane = threadIdx.x & 31, wpb = blockDim.x / 32;
-  for (int64_t i = (int64_t)blockIdx.x * wpb + threadIdx.x / 32; i < b.np; i += (int64_t)gridDim.x * wpb) {
+  for (int64_t i = q.r0 + threadIdx.x / 32; i < q.r1; i += wpb) {
     const double* row = A + i * b.np;
     double a = 0, c = 0;
     for (int64_t j = lane; j < b.np; j += 32) {
@@ -1312,20 +1340,26 @@ class BatchPipeline {
   void estimate(Staging& st, Rec& r, const std::vector<int>& list, int m0, int m1, int slot) {
     const size_t o_l = st.put(list);
     const int nl = (int)list.size();
-    const dim3 g_rows(grid_x_for(maxnp_ * 32, nl), nl);
+    std::vector<RChunk> ch;   // rows per chunk: a multiple of the 8 warps of a CTA
+    for (int w : list) {
+      const int np = walks_[w].np, R = std::max(8, (kChunkElems / np) & ~7);
+      for (int r0 = 0; r0 < np; r0 += R) ch.push_back(RChunk{w, r0, std::min(np, r0 + R), 0});
+    }
+    const size_t o_ch = st.put(ch);
+    const unsigned g_rows = (unsigned)ch.size();
     r.ops.push_back([=]() {
       const BWalk* wk = (const BWalk*)d_walks_.p;
       const int* l = dev<int>(o_l);
       kb_est_init<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), estst());
       FX_LAUNCH_CHECK();
       for (int k = 1; k <= 5; ++k) {
-        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m1), l, wk, est_scr(), estst(), kEX0, kET0);
-        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m0), l, wk, est_scr(), estst(), kET0, kEY0);
+        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m1), dev<RChunk>(o_ch), wk, est_scr(), estst(), kEX0, kET0);
+        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m0), dev<RChunk>(o_ch), wk, est_scr(), estst(), kET0, kEY0);
         kb_est_step1<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), estst(), k);
         FX_LAUNCH_CHECK();
         if (k == 5) break;
-        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m0), l, wk, est_scr(), estst(), kEX0, kET0);
-        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m1), l, wk, est_scr(), estst(), kET0, kEY0);
+        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m0), dev<RChunk>(o_ch), wk, est_scr(), estst(), kEX0, kET0);
+        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(m1), dev<RChunk>(o_ch), wk, est_scr(), estst(), kET0, kEY0);
         kb_est_step2<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), estst(), k);
         FX_LAUNCH_CHECK();
       }
@@ -1461,23 +1495,32 @@ class BatchPipeline {
     });
   }
 
+  // Row chunks of the listed walks' n x n (use_n) or np x np blocks, about kChunkElems each.
+  std::vector<RChunk> row_chunks(const std::vector<int>& list, bool use_n) const {
+    std::vector<RChunk> ch;
+    for (int w : list) {
+      const int rows = use_n ? walks_[w].n : walks_[w].np, cols = rows;
+      const int R = std::max(1, kChunkElems / std::max(1, cols));
+      for (int r0 = 0; r0 < rows; r0 += R) ch.push_back(RChunk{w, r0, std::min(rows, r0 + R), 0});
+    }
+    return ch;
+  }
+
   void combo(Staging& st, Rec& r, const std::vector<int>& list, int d_arena, const int m_arena[4],
              const std::vector<std::array<double, 5>>& coef) {
     if (list.empty()) return;
     std::vector<double> c(5 * count(), 0.0);
     for (int w : list)
       for (int k = 0; k < 5; ++k) c[5 * w + k] = coef[w][k];
-    const size_t o_l = st.put(list), o_c = st.put(c);
+    const std::vector<RChunk> ch = row_chunks(list, false);
+    const size_t o_ch = st.put(ch), o_c = st.put(c);
     Planes4 M{};
     for (int k = 0; k < 4; ++k) M.m[k] = m_arena[k] >= 0 ? A(m_arena[k]) : nullptr;
     double* D = A(d_arena);
-    const int nl = (int)list.size();
-    int64_t mx = 0;
-    for (int w : list) mx = std::max<int64_t>(mx, (int64_t)walks_[w].np * walks_[w].np);
-    const dim3 g(grid_x_for(mx, nl), nl);
+    const unsigned nch = (unsigned)ch.size();
     r.launches += 1;
     r.ops.push_back([=]() {
-      kb_combo<<<g, 256, 0, stream_>>>(D, M, dev<int>(o_l), (const BWalk*)d_walks_.p, dev<double>(o_c));
+      kb_combo<<<nch, 256, 0, stream_>>>(D, M, dev<RChunk>(o_ch), (const BWalk*)d_walks_.p, dev<double>(o_c));
       FX_LAUNCH_CHECK();
     });
   }
@@ -1517,16 +1560,17 @@ class BatchPipeline {
     double* p = A(a);
     double* rs = rsum();
     double* tot = misc();   // W doubles
-    int64_t mx = 0;
-    for (int w : list) mx = std::max<int64_t>(mx, (int64_t)walks_[w].np * walks_[w].np);
-    const dim3 g_el(grid_x_for(mx, nl), nl), g_rows(grid_x_for(maxnp_ * 32, nl), nl);
+    const std::vector<RChunk> ch = row_chunks(list, true);
+    const size_t o_ch = st.put(ch);
+    const unsigned nch = (unsigned)ch.size();
+    const dim3 g_rows(grid_x_for(maxnp_ * 32, nl), nl);
     r.ops.push_back([=]() {
       const BWalk* wk = (const BWalk*)d_walks_.p;
       kb_rowsums<<<g_rows, 256, 0, stream_>>>(p, dev<int>(o_l), wk, rs);
       FX_LAUNCH_CHECK();
       kb_walk_vec_reduce<<<nl, 256, 0, stream_>>>(rs, dev<int>(o_l), wk, 0, 1, tot, 1, 0);
       FX_LAUNCH_CHECK();
-      kb_apply_proj<<<g_el, 256, 0, stream_>>>(p, dev<int>(o_l), wk, rs, tot);
+      kb_apply_proj<<<nch, 256, 0, stream_>>>(p, dev<RChunk>(o_ch), wk, rs, tot);
       FX_LAUNCH_CHECK();
     });
     r.launches += 3;
@@ -1901,17 +1945,19 @@ class BatchPipeline {
       loff[w] = (int64_t)walks_[w].row0 * kNb;
       all[w] = w;
     }
-    const size_t o_lo = st.put(loff), o_all = st.put(all);
+    const std::vector<RChunk> ch = row_chunks(all, false);
+    const size_t o_lo = st.put(loff), o_all = st.put(all), o_ch = st.put(ch);
+    (void)o_all;
     double* X = A(x);
     double* XT = A(xt);
     const double* Li = (const double*)linv_.p;
     const double* LiT = (const double*)linv_.p + (size_t)rows_ * kNb;
-    const dim3 g(grid_x_for(maxnp_ * maxnp_, W), W);
+    const unsigned nch = (unsigned)ch.size();
     r.launches += 2;
     r.ops.push_back([=]() {
-      kb_init_inverse<<<g, 256, 0, stream_>>>(X, Li, dev<int>(o_all), (const BWalk*)d_walks_.p, dev<int64_t>(o_lo));
+      kb_init_inverse<<<nch, 256, 0, stream_>>>(X, Li, dev<RChunk>(o_ch), (const BWalk*)d_walks_.p, dev<int64_t>(o_lo));
       FX_LAUNCH_CHECK();
-      kb_init_inverse<<<g, 256, 0, stream_>>>(XT, LiT, dev<int>(o_all), (const BWalk*)d_walks_.p, dev<int64_t>(o_lo));
+      kb_init_inverse<<<nch, 256, 0, stream_>>>(XT, LiT, dev<RChunk>(o_ch), (const BWalk*)d_walks_.p, dev<int64_t>(o_lo));
       FX_LAUNCH_CHECK();
     });
     std::vector<std::vector<Node>> lv;
