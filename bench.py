@@ -233,6 +233,9 @@ def bench_batch(args, dev):
         psi = dP[k].to(torch.complex128)
         ov = torch.vdot(ref, psi).abs() ** 2 / (torch.vdot(ref, ref).real * torch.vdot(psi, psi).real)
         worst = max(worst, float(1.0 - ov))
+    # | ||psi|| - ||psi0|| | over all walks (U is unitary in exact arithmetic)
+    norm_dev = max(abs(float(torch.linalg.vector_norm(p.to(torch.complex128)) - torch.linalg.vector_norm(q.to(torch.complex128))))
+                   for p, q in zip(dP, dP0))
     b.close()
     del dP
     # per-walk loop of the plain form (compute only: engines are created outside the timing)
@@ -266,6 +269,7 @@ def bench_batch(args, dev):
         "m_hist": {int(k): int(v) for k, v in zip(*np.unique(m, return_counts=True))},
         "s_max": int(s.max()), "s_mean": round(float(s.mean()), 2),
         "worst_infidelity_4_largest": worst,
+        "norm_deviation_max": norm_dev,
     }
 
 
@@ -463,6 +467,15 @@ def main():
     clk = clocks.stop()
     st = eng.stats()
     psi_chosen = dpsi.clone()
+    unitarity = None
+    if not args.no_check and rank == 0:
+        # ||U^H U - I||_F / sqrt(N) of the timed walk's U (complex64 as stored), in complex128
+        U128 = dU.to(torch.complex128)
+        G = U128.conj().T @ U128
+        G.diagonal().sub_(1.0)
+        unitarity = float(torch.linalg.matrix_norm(G).item() / np.sqrt(n))
+        del U128, G
+        torch.cuda.empty_cache()
     if world > 1:
         tt = torch.tensor([total_ms], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -518,7 +531,8 @@ def main():
         lam, V = torch.linalg.eigh(Hd)
         Vc = V.to(torch.complex128)
         ref = (Vc @ (torch.exp(-1j * lam * args.t) * Vc[0])).cpu().numpy()
-        accuracy = {"infidelity_e0": eo.infidelity(psi_chosen.cpu().numpy(), ref)}
+        accuracy = {"infidelity_e0": eo.infidelity(psi_chosen.cpu().numpy(), ref),
+                    "unitarity_residual": unitarity}
         if psi_plain is not None:
             accuracy["infidelity_e0_plain"] = eo.infidelity(psi_plain.cpu().numpy(), ref)
         del Hd, V, lam, Vc
