@@ -478,13 +478,20 @@ __global__ void kb_est_matvec(const double* M, const RChunk* ch, const BWalk* wk
   double* y1 = est_vec(scr, b, out0 + 1);
   const double* A = M + b.off;
   const int lane = threadIdx.x & 31, wpb = blockDim.x / 32;
+  // 16-byte loads (np and every row start are even), two steps per iteration in flight
+  const int64_t h = b.np / 2;
+  const double2* u0 = reinterpret_cast<const double2*>(x0);
+  const double2* u1 = reinterpret_cast<const double2*>(x1);
   for (int64_t i = q.r0 + threadIdx.x / 32; i < q.r1; i += wpb) {
-    const double* row = A + i * b.np;
+    const double2* row = reinterpret_cast<const double2*>(A + i * b.np);
     double a = 0, c = 0;
-    for (int64_t j = lane; j < b.np; j += 32) {
-      const double m = row[j];
-      a += m * x0[j];
-      c += m * x1[j];
+#pragma unroll 2
+    for (int64_t j = lane; j < h; j += 32) {
+      const double2 m = row[j], p = u0[j], r = u1[j];
+      a += m.x * p.x;
+      a += m.y * p.y;
+      c += m.x * r.x;
+      c += m.y * r.y;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {

@@ -595,13 +595,24 @@ __device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t 
   const int sh = 7 * S - e;
   const bool one_factor = sh <= 1000;
   const double scale = one_factor ? ldexp(1.0, sh) : 0.0;
-  for (int64_t k0 = (int64_t)lane * 4; k0 < K; k0 += 128) {
+  // Second pass: the next step's values are loaded before this step's digits are cut, so
+  // that every lane has two loads in flight.
+  double cur[2][4] = {}, nxt[2][4] = {};
+  int64_t k0 = (int64_t)lane * 4;
+  if (k0 < K) {
+    load4<TI>(rre, k0, K, vec, cur[0]);
+    if (rim) load4<TI>(rim, k0, K, vec, cur[1]);
+  }
+  for (; k0 < K; k0 += 128) {
+    if (k0 + 128 < K) {
+      load4<TI>(rre, k0 + 128, K, vec, nxt[0]);
+      if (rim) load4<TI>(rim, k0 + 128, K, vec, nxt[1]);
+    }
 #pragma unroll
     for (int plane = 0; plane < 2; ++plane) {
       const TI* src = plane == 0 ? rre : rim;
       if (!src) continue;
-      double x[4];
-      load4<TI>(src, k0, K, vec, x);
+      double* x = cur[plane];
       uint32_t packed[kMaxSlices] = {0, 0, 0, 0, 0}, packed_neg[kMaxSlices] = {0, 0, 0, 0, 0};
       const bool neg = NEG && plane == 1;
 #pragma unroll
@@ -635,11 +646,16 @@ __device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t 
         if (neg && out.neg_im[q]) *reinterpret_cast<uint32_t*>(out.neg_im[q] + orow * out.ld + k0) = packed_neg[q];
       }
     }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      cur[0][j] = nxt[0][j];
+      cur[1][j] = nxt[1][j];
+    }
   }
 }
 
 template <typename TI, bool NEG>
-__global__ void __launch_bounds__(256, 3) k_slice_rows(const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K, int S,
+__global__ void __launch_bounds__(256, 2) k_slice_rows(const TI* re, const TI* im, int64_t ld, int64_t rows, int64_t K, int S,
                              I8Slices out) {
   const int lane = threadIdx.x & 31;
   const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
@@ -649,7 +665,7 @@ __global__ void __launch_bounds__(256, 3) k_slice_rows(const TI* re, const TI* i
 
 // Grouped slicing: warp per stacked row; the slab is found by binary search on row0.
 template <typename TI, bool NEG>
-__global__ void __launch_bounds__(256, 3) k_slice_rows_grouped(const GSlab* slabs, int nslabs, int64_t total_rows, int S, I8Slices out) {
+__global__ void __launch_bounds__(256, 2) k_slice_rows_grouped(const GSlab* slabs, int nslabs, int64_t total_rows, int S, I8Slices out) {
   const int lane = threadIdx.x & 31;
   const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   if (row >= total_rows) return;
