@@ -36,7 +36,8 @@ using namespace tc;
 
 constexpr int kBM = 128, kBK = 64;  // kBK in int8 elements (= bytes)
 constexpr int kMaxSlices = 5;
-constexpr int kThreads = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+constexpr int kEpiWarps = 16;   // epilogue warps: kEpiWarps / 4 per TMEM lane quarter
+constexpr int kThreads = 64 + 32 * kEpiWarps;   // warp 0 TMA, warp 1 MMA, then the epilogue
 constexpr int kMaxTerms = 2;
 constexpr int kStages = 3;
 
@@ -95,6 +96,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* v) {
       : "r"(taddr));
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = (int)r[i];
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int* v) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = (int)r[i];
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -239,7 +248,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
       mbar_init(&empty_bar[s], 1);
     }
     mbar_init(&tfull_bar, 1);
-    mbar_init(&tempty_bar, 256);
+    mbar_init(&tempty_bar, 32 * kEpiWarps);
     mbar_init(&drain_bar, 1);
     s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -354,10 +363,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
       }
     }
   } else {
-    // Two epilogue warps per TMEM lane quarter (warp % 4), each draining half of the columns.
+    // kEpiWarps / 4 epilogue warps per TMEM lane quarter (warp % 4), each draining an equal share
+    // of the columns in chunks of kW.
     const int q = warp & 3;
-    const int half = (warp - 2) >> 2;
-    constexpr int kChunks = kBN / 32;   // 16-column chunks per half
+    const int half = (warp - 2) >> 2;        // this warp's share of the columns
+    constexpr int kParts = kEpiWarps / 4;
+    constexpr int kCols = kBN / kParts;       // columns per warp
+    constexpr int kW = kEpiWarps == 16 ? 8 : 16;
+    constexpr int kChunks = kCols / kW;
+    static_assert(kCols % kW == 0, "epilogue chunks");
+    // drain all of a warp's columns before handing TMEM back when they fit in registers
+    constexpr bool kEarly = kCols <= (kEpiWarps == 16 ? 24 : 48);
     int it = 0;
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++it) {
       if constexpr (G) {
@@ -374,7 +390,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
       // Columns col0 .. col0 + 15 of this thread's row from the folded levels x: scaling,
       // diagonal split terms, alpha / beta C / gamma I, stores.  The launch's or the problem's
       // parameters are read here, after the TMEM reads, to keep them out of the fold's registers.
-      auto finish = [&](const double (&x)[16], int64_t col0) {
+      auto finish = [&](const auto& x, int64_t col0) {
+        constexpr int W = (int)(sizeof(x) / sizeof(double));
         double alpha = p.alpha, beta = p.beta, gamma = p.gamma;
         const TO* Cq = Cp;
         TO* Dq = Dp;
@@ -419,7 +436,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
         // may be C.  split 1: the thread's A row segment in 16-byte loads (the lanes hold
         // different rows); split 2: A symmetric, read down the columns across the lanes.
 #pragma unroll
-        for (int h = 0; h < 16; h += 8) {
+        for (int h = 0; h < W; h += 8) {
           const int64_t c0 = col0 + h;
           double arow[8];
           if (split == 1) {
@@ -475,17 +492,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
       };
       // x = sum_l 2^(-7 l) L_l of 16 columns, from the top level down, the levels read two at a
       // time (for |L_l| < 2^31 every step but the last of five levels is exact in FP64).
-      auto fold = [&](uint32_t ta, double (&x)[16]) {
+      auto fold = [&](uint32_t ta, auto& x) {
+        constexpr int W = (int)(sizeof(x) / sizeof(double));
 #pragma unroll
-        for (int i = 0; i < 16; ++i) x[i] = 0.0;
+        for (int i = 0; i < W; ++i) x[i] = 0.0;
 #pragma unroll
         for (int l = S - 1; l >= 0; l -= 2) {
-          int hi[16], lo[16];
-          tmem_ld16(ta + l * kBN, hi);
-          if (l >= 1) tmem_ld16(ta + (l - 1) * kBN, lo);
+          int hi[W], lo[W];
+          if constexpr (W == 16) {
+            tmem_ld16(ta + l * kBN, hi);
+            if (l >= 1) tmem_ld16(ta + (l - 1) * kBN, lo);
+          } else {
+            tmem_ld8(ta + l * kBN, hi);
+            if (l >= 1) tmem_ld8(ta + (l - 1) * kBN, lo);
+          }
           tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
+          for (int i = 0; i < W; ++i) {
             double t = x[i] * 0x1p-7 + (double)hi[i];
             if (l >= 1) t = t * 0x1p-7 + (double)lo[i];
             x[i] = t;
@@ -493,26 +516,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
         }
       };
       const uint32_t tq = tmem_base + ((uint32_t)(q * 32) << 16);
-      if constexpr (kChunks <= 3) {
-        // All of this half's columns fit in registers once folded: drain TMEM first and hand it
+      if constexpr (kEarly) {
+        // All of this warp's columns fit in registers once folded: drain TMEM first and hand it
         // back to the MMA warp, so that the next tile's products overlap the rest of the epilogue.
-        double xv[kChunks][16];
+        double xv[kChunks][kW];
 #pragma unroll
-        for (int c = 0; c < kChunks; ++c) fold(tq + (uint32_t)((half * kChunks + c) * 16), xv[c]);
+        for (int c = 0; c < kChunks; ++c) fold(tq + (uint32_t)((half * kChunks + c) * kW), xv[c]);
         tc_fence_before();
         mbar_arrive(&tempty_bar);
         if (row_ok) {
 #pragma unroll
           for (int c = 0; c < kChunks; ++c) {
-            const int64_t col0 = (int64_t)jb.nb * kBN + (half * kChunks + c) * 16;
+            const int64_t col0 = (int64_t)jb.nb * kBN + (half * kChunks + c) * kW;
             if (col0 < jb.N) finish(xv[c], col0);
           }
         }
       } else {
         for (int cc = half * kChunks; cc < (half + 1) * kChunks; ++cc) {
-          double x[16];
-          fold(tq + (uint32_t)(cc * 16), x);
-          const int64_t col0 = (int64_t)jb.nb * kBN + cc * 16;
+          double x[kW];
+          fold(tq + (uint32_t)(cc * kW), x);
+          const int64_t col0 = (int64_t)jb.nb * kBN + cc * kW;
           if (row_ok && col0 < jb.N) finish(x, col0);
         }
         tc_fence_before();
