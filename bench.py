@@ -213,13 +213,14 @@ def bench_batch(args, dev):
 
     plain_batch_ms = None
     if args.selector != "plain":
-        bpl = WalkBatch(ns)
+        bpl = WalkBatch(ns, autotune=True)
         plain_batch_ms = timed(bpl)
         _, s_plain = bpl.selection()
         bpl.close()
-    b = WalkBatch(ns, selector=args.selector)
+    b = WalkBatch(ns, selector=args.selector, autotune=True)   # schedule tuned in the warm-up
     batch_ms = timed(b)
     info = b.info()
+    sched = b.schedule()
     m, s = b.selection()
     outcome = b.details()["outcome"]
     # accuracy on the largest walks: FP64 eigendecomposition of A on the device
@@ -270,6 +271,8 @@ def bench_batch(args, dev):
         "s_max": int(s.max()), "s_mean": round(float(s.mean()), 2),
         "worst_infidelity_4_largest": worst,
         "norm_deviation_max": norm_dev,
+        "schedule": {"tile_group": sched["tile_group"], "tile_order": sched["tile_order"],
+                     "tuned_ms": [[g, o, round(ms, 2)] for g, o, ms in sched["tuned"]]},
     }
 
 

@@ -78,6 +78,8 @@ SIGNATURES = {
     "fx_probabilities": [ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                          ctypes.c_void_p, ctypes.c_void_p],
     "fx_graph_error": [],
+    "fx_batch_schedule": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)],
     "fx_product_f32_noalloc": [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
                                ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int64,

@@ -21,6 +21,7 @@ from . import _native
 from ._native import check, lib
 
 OPT_GRAPH, OPT_TIMEOUT_MS, OPT_FORCE_M, OPT_SELECTOR, OPT_ANALYZE_ONLY, OPT_DIAG_SPLIT = 0, 1, 2, 3, 4, 5
+OPT_AUTOTUNE, OPT_TILE_GROUP, OPT_TILE_ORDER = 6, 7, 8
 OUTCOMES = {0: "plain", 1: "certified", 2: "learned", -1: "learned rejected by the bound",
             -2: "failed an a-posteriori check, redone with the plain (m, s)"}
 
@@ -48,7 +49,7 @@ class WalkBatch:
     """Owner of one ``fx_batch`` handle: device workspace for walks of sizes ``ns``."""
 
     def __init__(self, ns, dtype=np.complex64, graph: bool = True, selector: str = "plain",
-                 analyze_only: bool = False, diag_split: int = 3) -> None:
+                 analyze_only: bool = False, diag_split: int = 3, autotune: bool = False) -> None:
         self.ns = [int(n) for n in ns]
         self.dtype = np.dtype(dtype)
         if self.dtype not in (np.dtype(np.complex64), np.dtype(np.complex128)):
@@ -65,6 +66,8 @@ class WalkBatch:
             self.set_option(OPT_ANALYZE_ONLY, 1)
         if int(diag_split) != 3:
             self.set_option(OPT_DIAG_SPLIT, int(diag_split))
+        if autotune:
+            self.set_option(OPT_AUTOTUNE, 1)
 
     def set_option(self, key: int, value: float) -> None:
         _check(lib().fx_batch_set_option(self._h, int(key), float(value)), self._h)
@@ -108,6 +111,19 @@ class WalkBatch:
         s = (ctypes.c_int32 * len(self.ns))()
         _check(lib().fx_batch_selection(self._h, m, s), self._h)
         return np.array(m[:], dtype=np.int32), np.array(s[:], dtype=np.int32)
+
+    def schedule(self) -> dict:
+        """Schedule of the post-selection products (tile group, tile order) and, after an
+        autotuned run, the candidates tried with their times."""
+        g, o, n = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        t = (ctypes.c_double * 48)()
+        _check(lib().fx_batch_schedule(self._h, ctypes.byref(g), ctypes.byref(o), t, ctypes.byref(n)), self._h)
+        return {"tile_group": g.value, "tile_order": o.value,
+                "tuned": [(int(t[3 * i]), int(t[3 * i + 1]), t[3 * i + 2]) for i in range(n.value)]}
+
+    def set_schedule(self, tile_group: int, tile_order: int) -> None:
+        self.set_option(OPT_TILE_GROUP, tile_group)
+        self.set_option(OPT_TILE_ORDER, tile_order)
 
     def details(self) -> dict:
         """Per walk of the last run: selector features (n x 8), the Al-Mohy & Higham (m, s),

@@ -832,6 +832,18 @@ class BatchPipeline {
   void set_selector(int k) { selector_ = k; }
   // Stop after the selection (statistics, norms, estimates, features; no exponential).
   void set_analyze_only(bool a) { analyze_only_ = a; }
+  // Phase-2 schedule: tune it at the next run, or set it.
+  void set_autotune(bool a) { autotune_ = a; }
+  void set_schedule(int group, int order) {
+    tile_group_ = group;
+    tile_order_ = order;
+    key2_.clear();
+  }
+  void schedule(int* group, int* order) const {
+    *group = tile_group_;
+    *order = tile_order_;
+  }
+  const std::vector<std::array<double, 3>>& tuned() const { return tuned_; }
   // Diagonal split of the solve's products, a mask: 1 V^2, W^2, VW; 2 the complex products
   // P2 L^-T and Z L^-1 (default 3); changing it re-records both phases.
   void set_diag_split(int v) {
@@ -1006,6 +1018,10 @@ class BatchPipeline {
     // Pade denominator fails to factor, or whose state loses its norm, is redone alone with the
     // plain (m, s) in a pipeline of its own (its outputs are overwritten; the other walks keep
     // theirs).  A failure under the plain choice is an error.
+    if (autotune_) {
+      autotune_phase2(tab);
+      autotune_ = false;
+    }
     FX_CUDA(cudaMemsetAsync(walk_err(), 0, sizeof(int) * W, s));
     run_phase2(tab);
     std::vector<int> werr(W), own(W, 0);
@@ -1136,6 +1152,9 @@ class BatchPipeline {
   int selector_ = 0;
   bool analyze_only_ = false;
   int split_ = 3;
+  int tile_group_ = 8, tile_order_ = 0;   // phase-2 schedule of the grouped products
+  bool autotune_ = false;
+  std::vector<std::array<double, 3>> tuned_;   // (group, order, ms) of the last tuning
   DevArena sel_io_, ver_io_;
   cudaStream_t stream_ = nullptr;
   unsigned timeout_ms_ = 2000;
@@ -1377,18 +1396,81 @@ class BatchPipeline {
   }
 
   // ---- recorded grouped operations --------------------------------------------------
-  // Tile order of one problem: 8 x 8 blocks of tiles, row-major inside a block and over the
-  // blocks.  The ~148 tiles in flight then cover two or three blocks, so every A row panel
-  // and Bt column panel of a K step is fetched from HBM once and served to up to eight CTAs
-  // from L2 (a row-major order would stream a distinct Bt panel for every CTA).
+  // Tile order of one problem: G x G blocks of tiles (G = tile_group_, 8 unless tuned),
+  // row-major inside a block and over the blocks.  The ~148 tiles in flight then cover a few
+  // blocks, so every A row panel and Bt column panel of a K step is fetched from HBM once and
+  // served to up to G CTAs from L2 (a row-major order would stream a distinct Bt panel for every
+  // CTA).
   template <typename F>
-  static void for_tiles(int tm, int tn, F&& f) {
-    constexpr int G = 8;
+  void for_tiles(int tm, int tn, F&& f) const {
+    const int G = tile_group_;
     for (int bm = 0; bm < tm; bm += G)
       for (int bn = 0; bn < tn; bn += G)
         for (int mb = bm; mb < std::min(tm, bm + G); ++mb)
           for (int nb = bn; nb < std::min(tn, bn + G); ++nb) f(mb, nb);
   }
+  // Launch order of a grouped product's tiles (tile_order_): 0, the longest K ranges first (the
+  // persistent CTAs then finish close together); 1, problems by decreasing K with the tiles of a
+  // problem kept together in their blocked order (the CTAs working at the same time share its
+  // panels in L2).
+  void order_tiles(std::vector<GTile>& tiles, const std::vector<GProblem>& pr) const {
+    if (tile_order_ == 0)
+      std::stable_sort(tiles.begin(), tiles.end(),
+                       [](const GTile& x, const GTile& y) { return (x.kb1 - x.kb0) > (y.kb1 - y.kb0); });
+    else
+      std::stable_sort(tiles.begin(), tiles.end(),
+                       [&](const GTile& x, const GTile& y) { return pr[x.prob].K > pr[y.prob].K; });
+  }
+
+  // Autotuning of the phase-2 schedule (tile_group_, tile_order_): every candidate is recorded,
+  // replayed once to warm up and once timed on this batch, and the fastest is kept.  Phase 2
+  // overwrites the powers that phase 1 left in the arenas, so phase 1 is replayed before every
+  // phase-2 run (and once more before the real one); only phase 2 is timed.  The schedule
+  // changes only the order in which tiles run, never a tile's arithmetic, so the results do not
+  // depend on it.
+  void autotune_phase2(const std::vector<const void*>& tab) {
+    static const int cand[][2] = {{8, 0}, {8, 1}, {4, 0}, {16, 0}, {16, 1}};
+    tuned_.clear();
+    double best = 1e300;
+    int bg = tile_group_, bo = tile_order_;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    FX_CUDA(cudaEventCreate(&e0));
+    FX_CUDA(cudaEventCreate(&e1));
+    try {
+      for (const auto& c : cand) {
+        tile_group_ = c[0];
+        tile_order_ = c[1];
+        key2_.clear();
+        replay_phase1();
+        run_phase2(tab);
+        replay_phase1();
+        FX_CUDA(cudaEventRecord(e0, stream_));
+        run_phase2(tab);
+        FX_CUDA(cudaEventRecord(e1, stream_));
+        FX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        FX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        tuned_.push_back({(double)c[0], (double)c[1], (double)ms});
+        if (ms < best) {
+          best = ms;
+          bg = c[0];
+          bo = c[1];
+        }
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    tile_group_ = bg;
+    tile_order_ = bo;
+    key2_.clear();
+    replay_phase1();
+  }
+  void replay_phase1() { run_recorded(desc1_, st1_, r1_, graph1_, use_graph_ && !profile_); }
+
   // Real multiply-adds x 2 that the listed tiles compute (tile-level: 128 x BN x 64 per K step
   // and term); the int8 MMA operations issued are S(S+1)/2 times that.
   static double tile_ops(const std::vector<GTile>& tiles, int nterms) {
@@ -1458,9 +1540,7 @@ class BatchPipeline {
         tiles.push_back(GTile{i, mb, nb, kb0, kb1, 0});
       });
     }
-    // Largest K ranges first: the persistent CTAs then finish close together.
-    std::stable_sort(tiles.begin(), tiles.end(),
-                     [](const GTile& x, const GTile& y) { return (x.kb1 - x.kb0) > (y.kb1 - y.kb0); });
+    order_tiles(tiles, pr);
     std::vector<GSlab> a_sorted = sa, b_sorted = sb ? *sb : std::vector<GSlab>();
     auto by_row = [](const GSlab& x, const GSlab& y) { return x.row0 < y.row0; };
     std::sort(a_sorted.begin(), a_sorted.end(), by_row);
@@ -1790,8 +1870,7 @@ class BatchPipeline {
           if ((long long)nb * bn + bn - 1 >= (long long)mb * 128) tiles.push_back(GTile{i, mb, nb, 0, prr[i].K / 64, 0});
         });
       }
-      std::stable_sort(tiles.begin(), tiles.end(),
-                       [](const GTile& x, const GTile& y) { return (x.kb1 - x.kb0) > (y.kb1 - y.kb0); });
+      order_tiles(tiles, prr);
       std::sort(sa.begin(), sa.end(), [](const GSlab& x, const GSlab& y) { return x.row0 < y.row0; });
       const size_t o_sa = st.put(sa), o_r = st.put(prr), o_i = st.put(pri), o_t = st.put(tiles);
       const int nsa = (int)sa.size(), nt = (int)tiles.size();
@@ -2120,6 +2199,20 @@ int fx_batch_destroy(fx_batch_handle b) {
   return FX_OK;
 }
 
+int fx_batch_schedule(fx_batch_handle b, int32_t* tile_group, int32_t* tile_order, double* tuned, int32_t* ntuned) {
+  if (!b || !tile_group || !tile_order) return bfail(b, fx::Error{FX_ERR_VALUE, "null argument"});
+  int g = 0, o = 0;
+  b->p->schedule(&g, &o);
+  *tile_group = g;
+  *tile_order = o;
+  const auto& t = b->p->tuned();
+  if (ntuned) *ntuned = (int32_t)t.size();
+  if (tuned)
+    for (size_t i = 0; i < t.size(); ++i)
+      for (int k = 0; k < 3; ++k) tuned[3 * i + k] = t[i][k];
+  return FX_OK;
+}
+
 int fx_batch_set_option(fx_batch_handle b, int key, double value) {
   if (!b) return bfail(nullptr, fx::Error{FX_ERR_VALUE, "null handle"});
   switch (key) {
@@ -2135,6 +2228,22 @@ int fx_batch_set_option(fx_batch_handle b, int key, double value) {
       b->p->set_selector((int)value);
       return FX_OK;
     case FX_BATCH_OPT_ANALYZE_ONLY: b->p->set_analyze_only(value != 0.0); return FX_OK;
+    case FX_BATCH_OPT_AUTOTUNE: b->p->set_autotune(value != 0.0); return FX_OK;
+    case FX_BATCH_OPT_TILE_GROUP: {
+      int g = 0, o = 0;
+      b->p->schedule(&g, &o);
+      if (value != 4 && value != 8 && value != 16)
+        return bfail(b, fx::Error{FX_ERR_VALUE, "tile group must be 4, 8 or 16"});
+      b->p->set_schedule((int)value, o);
+      return FX_OK;
+    }
+    case FX_BATCH_OPT_TILE_ORDER: {
+      int g = 0, o = 0;
+      b->p->schedule(&g, &o);
+      if (value != 0 && value != 1) return bfail(b, fx::Error{FX_ERR_VALUE, "tile order must be 0 or 1"});
+      b->p->set_schedule(g, (int)value);
+      return FX_OK;
+    }
     case FX_BATCH_OPT_DIAG_SPLIT:
       if (value != 0 && value != 1 && value != 2 && value != 3)
         return bfail(b, fx::Error{FX_ERR_VALUE, "diagonal split must be a mask of 1 and 2"});

@@ -174,9 +174,13 @@ enum fx_batch_option {
   FX_BATCH_OPT_FORCE_M = 2,     /* diagnostics: force the Pade degree (-1 automatic)            */
   FX_BATCH_OPT_SELECTOR = 3,    /* as FX_OPT_SELECTOR                                           */
   FX_BATCH_OPT_ANALYZE_ONLY = 4, /* 1: stop after the selection (features and (m, s) only)      */
-  FX_BATCH_OPT_DIAG_SPLIT = 5    /* mask, default 3: products of the solve that take their       */
+  FX_BATCH_OPT_DIAG_SPLIT = 5,   /* mask, default 3: products of the solve that take their       */
                                  /* operands' diagonals out of the int8 slices and add those    */
                                  /* terms in FP64; 1 V^2, W^2, VW; 2 P2 L^-T and Z L^-1          */
+  FX_BATCH_OPT_AUTOTUNE = 6,     /* 1: at the next run, time the candidate schedules of the     */
+                                 /* post-selection products on this batch and keep the fastest */
+  FX_BATCH_OPT_TILE_GROUP = 7,   /* schedule: tiles in G x G blocks, G = 4, 8 (default) or 16    */
+  FX_BATCH_OPT_TILE_ORDER = 8    /* schedule: 0 (default) longest K ranges first, 1 by problem   */
 };
 /* count walks of sizes n[0..count); dtype FX_C64 or FX_C128 (of X, psi0 and psi). */
 int fx_batch_create(size_t count, const int64_t* n, int dtype, fx_batch_handle* out);
@@ -202,6 +206,10 @@ int fx_batch_details(fx_batch_handle b, double* features, int32_t* plain_m, int3
 /* Weights of the learned selector for every handle of the process (5126 floats, host
  * pointer; copied to the current device). */
 int fx_selector_set_weights(const float* w, int64_t n);
+/* The phase-2 schedule in use and, after an autotuned run, the candidates tried: ntuned rows
+ * of (tile group, tile order, ms) in tuned (3 doubles each, at most 16 rows). */
+int fx_batch_schedule(fx_batch_handle b, int32_t* tile_group, int32_t* tile_order, double* tuned,
+                      int32_t* ntuned);
 const char* fx_batch_last_error(fx_batch_handle b);
 
 /* ---- Learned (m, s) selector: MLP 8 -> 64 -> 64 -> (5 Pade-degree logits + s), ReLU.

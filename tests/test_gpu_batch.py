@@ -107,3 +107,24 @@ def test_large_scaling_walks_keep_double_level_accuracy():
     for k in range(len(Xs)):
         assert s[k] >= 9, (m, s)
         assert eo.infidelity(psis[k], refs[k]) <= 5e-12, (k, eo.infidelity(psis[k], refs[k]), s[k])
+
+
+def test_autotuned_schedule_keeps_the_states_bitwise():
+    """The autotuner times the candidate schedules of the post-selection products on the batch
+    and keeps the fastest; a schedule orders the tiles, never changes their arithmetic."""
+    from fastctqw_b200.batch import WalkBatch
+    _, Xs, p0 = _family(12, seed=10, nmin=64, nmax=600)
+    ns = [X.shape[0] for X in Xs]
+    ref = WalkBatch(ns).run(Xs, p0)
+    b = WalkBatch(ns, autotune=True)
+    got = b.run(Xs, p0)
+    sch = b.schedule()
+    assert len(sch["tuned"]) == 5 and all(ms > 0 for _, _, ms in sch["tuned"])
+    best = min(sch["tuned"], key=lambda r: r[2])
+    assert (sch["tile_group"], sch["tile_order"]) == best[:2]
+    again = b.run(Xs, p0)                  # the kept schedule, no tuning
+    c = WalkBatch(ns)
+    c.set_schedule(16, 1)
+    other = c.run(Xs, p0)
+    for x, y, z, w in zip(ref, got, again, other):
+        assert np.array_equal(x, y) and np.array_equal(x, z) and np.array_equal(x, w)
