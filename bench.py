@@ -221,6 +221,7 @@ def bench_batch(args, dev):
     batch_ms = timed(b)
     info = b.info()
     sched = b.schedule()
+    sampled = b.sample_check()
     m, s = b.selection()
     outcome = b.details()["outcome"]
     # accuracy on the largest walks: FP64 eigendecomposition of A on the device
@@ -271,6 +272,7 @@ def bench_batch(args, dev):
         "s_max": int(s.max()), "s_mean": round(float(s.mean()), 2),
         "worst_infidelity_4_largest": worst,
         "norm_deviation_max": norm_dev,
+        "sampled_plain_check": sampled,
         "schedule": {"tile_group": sched["tile_group"], "tile_order": sched["tile_order"],
                      "tuned_ms": [[g, o, round(ms, 2)] for g, o, ms in sched["tuned"]]},
     }

@@ -78,6 +78,7 @@ SIGNATURES = {
     "fx_probabilities": [ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                          ctypes.c_void_p, ctypes.c_void_p],
     "fx_graph_error": [],
+    "fx_batch_sample_check": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)],
     "fx_batch_schedule": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)],
     "fx_product_f32_noalloc": [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,

@@ -21,7 +21,7 @@ from . import _native
 from ._native import check, lib
 
 OPT_GRAPH, OPT_TIMEOUT_MS, OPT_FORCE_M, OPT_SELECTOR, OPT_ANALYZE_ONLY, OPT_DIAG_SPLIT = 0, 1, 2, 3, 4, 5
-OPT_AUTOTUNE, OPT_TILE_GROUP, OPT_TILE_ORDER = 6, 7, 8
+OPT_AUTOTUNE, OPT_TILE_GROUP, OPT_TILE_ORDER, OPT_SAMPLE_WALKS = 6, 7, 8, 9
 OUTCOMES = {0: "plain", 1: "certified", 2: "learned", -1: "learned rejected by the bound",
             -2: "failed an a-posteriori check, redone with the plain (m, s)"}
 
@@ -111,6 +111,13 @@ class WalkBatch:
         s = (ctypes.c_int32 * len(self.ns))()
         _check(lib().fx_batch_selection(self._h, m, s), self._h)
         return np.array(m[:], dtype=np.int32), np.array(s[:], dtype=np.int32)
+
+    def sample_check(self) -> dict:
+        """The last run's sampled comparison with the plain method: walks re-run, largest
+        infidelity between the two states."""
+        c, m = ctypes.c_int32(), ctypes.c_double()
+        _check(lib().fx_batch_sample_check(self._h, ctypes.byref(c), ctypes.byref(m)), self._h)
+        return {"sampled": c.value, "max_infidelity": m.value}
 
     def schedule(self) -> dict:
         """Schedule of the post-selection products (tile group, tile order) and, after an

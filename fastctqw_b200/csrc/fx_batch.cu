@@ -1037,6 +1037,7 @@ class BatchPipeline {
       any = true;
     }
     any = verify_states(tab, own) || any;
+    any = sample_compare(tab, own) || any;
     if (any) {
       if (herr & kDevTimeout) throw Error{FX_ERR_TIMEOUT, "a device-side wait timed out"};
       FX_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int) * 8, s));
@@ -1100,6 +1101,95 @@ class BatchPipeline {
   // the plain choice shares (up to ~2e-4 after 13 squarings for walks dominated by one
   // eigenvalue, where the int8 slices hold that mode's off-diagonal entries to ~1e-8).  Returns
   // true when a walk failed.
+  // Sampled comparison with the plain method: up to sample_walks_ of the walks that ran a
+  // non-plain (m, s) (the smallest, so that the check stays cheap; ties to the lower index) are
+  // run again with the plain (m, s) in a side pipeline, and the two states compared.  An
+  // infidelity above kSampleInfid marks every non-plain walk of the batch for the plain redo.
+  bool sample_compare(const std::vector<const void*>& tab, std::vector<int>& own) {
+    constexpr double kSampleInfid = 1e-10;
+    const int W = count();
+    sample_count_ = 0;
+    sample_max_infid_ = 0.0;
+    std::vector<int> cand;
+    for (int w = 0; w < W; ++w)
+      if (outcome_[w] > 0 && !own[w] && tab[W + w] && tab[2 * W + w] &&
+          (sel_m_[w] != plain_m_[w] || sel_s_[w] != plain_s_[w]))
+        cand.push_back(w);
+    if (cand.empty() || sample_walks_ <= 0) return false;
+    std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) { return walks_[a].n < walks_[b].n; });
+    if ((int)cand.size() > sample_walks_) cand.resize(sample_walks_);
+    std::vector<int64_t> ns;
+    for (int w : cand) ns.push_back(walks_[w].n);
+    if (!sample_pipe_ || ns != sample_ns_) {
+      sample_pipe_.reset(new BatchPipeline(ns, dtype_));
+      sample_ns_ = ns;
+    }
+    sample_pipe_->set_timeout(timeout_ms_);
+    const size_t elem = dtype_ == FX_C64 ? 8 : 16;
+    size_t total = 0;
+    for (int64_t n : ns) total += (size_t)n * elem;
+    if (sample_io_.bytes < total) sample_io_.alloc(total);
+    std::vector<const void*> x, p0;
+    std::vector<void*> p1, u(cand.size(), nullptr);
+    size_t off = 0;
+    for (int w : cand) {
+      x.push_back(tab[w]);
+      p0.push_back(tab[W + w]);
+      p1.push_back((unsigned char*)sample_io_.p + off);
+      off += (size_t)walks_[w].n * elem;
+    }
+    sample_pipe_->run(x.data(), p0.data(), p1.data(), u.data(), stream_);
+    launches_ += sample_pipe_->launches();
+    // both states to the host, compared in FP64
+    std::vector<unsigned char> a(total), b(total);
+    off = 0;
+    for (size_t i = 0; i < cand.size(); ++i) {
+      const size_t bytes = (size_t)walks_[cand[i]].n * elem;
+      FX_CUDA(cudaMemcpyAsync(a.data() + off, tab[2 * W + cand[i]], bytes, cudaMemcpyDeviceToHost, stream_));
+      FX_CUDA(cudaMemcpyAsync(b.data() + off, p1[i], bytes, cudaMemcpyDeviceToHost, stream_));
+      off += bytes;
+    }
+    FX_CUDA(cudaStreamSynchronize(stream_));
+    off = 0;
+    for (size_t i = 0; i < cand.size(); ++i) {
+      const int64_t n = walks_[cand[i]].n;
+      std::complex<double> ov(0.0, 0.0);
+      double na = 0.0, nb = 0.0;
+      for (int64_t k = 0; k < n; ++k) {
+        std::complex<double> va, vb;
+        if (dtype_ == FX_C64) {
+          const float* fa = (const float*)(a.data() + off);
+          const float* fb = (const float*)(b.data() + off);
+          va = {fa[2 * k], fa[2 * k + 1]};
+          vb = {fb[2 * k], fb[2 * k + 1]};
+        } else {
+          const double* da = (const double*)(a.data() + off);
+          const double* db = (const double*)(b.data() + off);
+          va = {da[2 * k], da[2 * k + 1]};
+          vb = {db[2 * k], db[2 * k + 1]};
+        }
+        ov += std::conj(vb) * va;
+        na += std::norm(va);
+        nb += std::norm(vb);
+      }
+      const double inf = (na > 0 && nb > 0) ? 1.0 - std::norm(ov) / (na * nb) : 1.0;
+      sample_max_infid_ = std::max(sample_max_infid_, inf);
+      off += (size_t)n * elem;
+    }
+    sample_count_ = (int)cand.size();
+    if (!(sample_max_infid_ <= kSampleInfid)) {
+      for (int w = 0; w < W; ++w)
+        if (outcome_[w] > 0) own[w] = 1;
+      return true;
+    }
+    return false;
+  }
+  void set_sample_walks(int k) { sample_walks_ = k; }
+  void sample_check(int* count, double* max_infid) const {
+    *count = sample_count_;
+    *max_infid = sample_max_infid_;
+  }
+
   bool verify_states(const std::vector<const void*>& tab, std::vector<int>& own) {
     const int W = count();
     std::vector<int> list;
@@ -1153,6 +1243,11 @@ class BatchPipeline {
   bool analyze_only_ = false;
   int split_ = 3;
   int tile_group_ = 8, tile_order_ = 0;   // phase-2 schedule of the grouped products
+  int sample_walks_ = 2, sample_count_ = 0;   // sampled comparison with the plain method
+  double sample_max_infid_ = 0.0;
+  std::unique_ptr<BatchPipeline> sample_pipe_;
+  std::vector<int64_t> sample_ns_;
+  DevArena sample_io_;
   bool autotune_ = false;
   std::vector<std::array<double, 3>> tuned_;   // (group, order, ms) of the last tuning
   DevArena sel_io_, ver_io_;
@@ -2199,6 +2294,16 @@ int fx_batch_destroy(fx_batch_handle b) {
   return FX_OK;
 }
 
+int fx_batch_sample_check(fx_batch_handle b, int32_t* sampled, double* max_infidelity) {
+  if (!b || !sampled || !max_infidelity) return bfail(b, fx::Error{FX_ERR_VALUE, "null argument"});
+  int c = 0;
+  double m = 0.0;
+  b->p->sample_check(&c, &m);
+  *sampled = c;
+  *max_infidelity = m;
+  return FX_OK;
+}
+
 int fx_batch_schedule(fx_batch_handle b, int32_t* tile_group, int32_t* tile_order, double* tuned, int32_t* ntuned) {
   if (!b || !tile_group || !tile_order) return bfail(b, fx::Error{FX_ERR_VALUE, "null argument"});
   int g = 0, o = 0;
@@ -2229,6 +2334,10 @@ int fx_batch_set_option(fx_batch_handle b, int key, double value) {
       return FX_OK;
     case FX_BATCH_OPT_ANALYZE_ONLY: b->p->set_analyze_only(value != 0.0); return FX_OK;
     case FX_BATCH_OPT_AUTOTUNE: b->p->set_autotune(value != 0.0); return FX_OK;
+    case FX_BATCH_OPT_SAMPLE_WALKS:
+      if (value < 0 || value > 64) return bfail(b, fx::Error{FX_ERR_VALUE, "sampled walks must be 0..64"});
+      b->p->set_sample_walks((int)value);
+      return FX_OK;
     case FX_BATCH_OPT_TILE_GROUP: {
       int g = 0, o = 0;
       b->p->schedule(&g, &o);

@@ -180,7 +180,9 @@ enum fx_batch_option {
   FX_BATCH_OPT_AUTOTUNE = 6,     /* 1: at the next run, time the candidate schedules of the     */
                                  /* post-selection products on this batch and keep the fastest */
   FX_BATCH_OPT_TILE_GROUP = 7,   /* schedule: tiles in G x G blocks, G = 4, 8 (default) or 16    */
-  FX_BATCH_OPT_TILE_ORDER = 8    /* schedule: 0 (default) longest K ranges first, 1 by problem   */
+  FX_BATCH_OPT_TILE_ORDER = 8,   /* schedule: 0 (default) longest K ranges first, 1 by problem   */
+  FX_BATCH_OPT_SAMPLE_WALKS = 9  /* walks (default 2, 0..64) of a non-plain selection re-run with */
+                                 /* the plain (m, s) and compared after every run               */
 };
 /* count walks of sizes n[0..count); dtype FX_C64 or FX_C128 (of X, psi0 and psi). */
 int fx_batch_create(size_t count, const int64_t* n, int dtype, fx_batch_handle* out);
@@ -206,6 +208,10 @@ int fx_batch_details(fx_batch_handle b, double* features, int32_t* plain_m, int3
 /* Weights of the learned selector for every handle of the process (5126 floats, host
  * pointer; copied to the current device). */
 int fx_selector_set_weights(const float* w, int64_t n);
+/* Sampled comparison of the last run: how many non-plain walks were re-run with the plain
+ * (m, s), and the largest infidelity between the two states.  Above 1e-10 every non-plain
+ * walk was redone with the plain (m, s) (outcome -2). */
+int fx_batch_sample_check(fx_batch_handle b, int32_t* sampled, double* max_infidelity);
 /* The phase-2 schedule in use and, after an autotuned run, the candidates tried: ntuned rows
  * of (tile group, tile order, ms) in tuned (3 doubles each, at most 16 rows). */
 int fx_batch_schedule(fx_batch_handle b, int32_t* tile_group, int32_t* tile_order, double* tuned,

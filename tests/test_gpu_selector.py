@@ -166,3 +166,24 @@ def test_mixed_degree_batches_twice():
         ref = V @ (np.exp(1j * lam) * (V.T @ p0))
         assert _inf(first[k], ref) <= 1e-10, (k, m[k], s[k])
         assert np.array_equal(first[k], second[k])
+
+
+def test_sampled_plain_comparison_checks_non_plain_walks():
+    """After a learned run, the smallest walks that took a non-plain (m, s) are re-run with the
+    plain (m, s) and compared; on sound proposals the states agree to far below 1e-10."""
+    from fastctqw_b200 import selector
+    from fastctqw_b200.batch import OPT_SAMPLE_WALKS, WalkBatch
+    selector.set_weights()
+    Xs, psi0, refs = _walks(16, 14)
+    ns = [X.shape[0] for X in Xs]
+    b = WalkBatch(ns, selector="learned")
+    b.run(Xs, psi0)
+    d = b.details()
+    m, s = b.selection()
+    nonplain = int(((m != d["plain_m"]) | (s != d["plain_s"])).sum())
+    chk = b.sample_check()
+    assert chk["sampled"] == min(2, nonplain), (chk, nonplain)
+    assert chk["max_infidelity"] <= 1e-10
+    b.set_option(OPT_SAMPLE_WALKS, 5)
+    b.run(Xs, psi0)
+    assert b.sample_check()["sampled"] == min(5, nonplain)
