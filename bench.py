@@ -213,11 +213,11 @@ def bench_batch(args, dev):
 
     plain_batch_ms = None
     if args.selector != "plain":
-        bpl = WalkBatch(ns, autotune=True)
+        bpl = WalkBatch(ns, autotune=not args.no_autotune)
         plain_batch_ms = timed(bpl)
         _, s_plain = bpl.selection()
         bpl.close()
-    b = WalkBatch(ns, selector=args.selector, autotune=True)   # schedule tuned in the warm-up
+    b = WalkBatch(ns, selector=args.selector, autotune=not args.no_autotune)   # tuned in the warm-up
     batch_ms = timed(b)
     info = b.info()
     sched = b.schedule()
@@ -402,6 +402,7 @@ def main():
     ap.add_argument("--no-batch-loop", action="store_true", help="skip the per-walk loop of the batch leg")
     ap.add_argument("--batch-only", action="store_true", help="run only the uneven-batch leg")
     ap.add_argument("--no-setup", action="store_true", help="skip the device set-up / time-curve leg")
+    ap.add_argument("--no-autotune", action="store_true", help="batch leg: default schedule, no autotuning")
     ap.add_argument("--batch-shard", action="store_true",
                     help="with N > 1 ranks: also run the uneven batch sharded over the ranks")
     ap.add_argument("--batch-count", type=int, default=512)
