@@ -1105,6 +1105,7 @@ class BatchPipeline {
   // non-plain (m, s) (the smallest, so that the check stays cheap; ties to the lower index) are
   // run again with the plain (m, s) in a side pipeline, and the two states compared.  An
   // infidelity above kSampleInfid marks every non-plain walk of the batch for the plain redo.
+  // The sample is taken only if it costs at most a tenth of the batch.
   bool sample_compare(const std::vector<const void*>& tab, std::vector<int>& own) {
     constexpr double kSampleInfid = 1e-10;
     const int W = count();
@@ -1118,6 +1119,12 @@ class BatchPipeline {
     if (cand.empty() || sample_walks_ <= 0) return false;
     std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) { return walks_[a].n < walks_[b].n; });
     if ((int)cand.size() > sample_walks_) cand.resize(sample_walks_);
+    // skipped when the re-runs would cost more than a tenth of the batch (by N^3): a batch of
+    // one walk (a single structured walk) would otherwise be computed twice
+    double all_n3 = 0.0, cand_n3 = 0.0;
+    for (int w = 0; w < W; ++w) all_n3 += std::pow((double)walks_[w].n, 3);
+    for (int w : cand) cand_n3 += std::pow((double)walks_[w].n, 3);
+    if (cand_n3 > 0.1 * all_n3) return false;
     std::vector<int64_t> ns;
     for (int w : cand) ns.push_back(walks_[w].n);
     if (!sample_pipe_ || ns != sample_ns_) {
