@@ -29,6 +29,15 @@ from numpy.typing import NDArray
 from .fastexpm import ExpMatComplex64, ExpMatComplex128
 
 
+def is_uniform_grid(times) -> bool:
+    """True when times are t_k = (k + 1) t_0 (k = 0, 1, ...) with t_0 > 0, to 1e-12 relative:
+    the grid on which one propagator U(t_0) can be stepped."""
+    times = np.asarray(times, dtype=np.float64).reshape(-1)
+    if times.size == 0 or not times[0] > 0:
+        return False
+    return bool(np.allclose(times, times[0] * np.arange(1, times.size + 1), rtol=1e-12, atol=0.0))
+
+
 def _check_device(device: str) -> None:
     if device != "cuda":
         raise ValueError("fastctqw_b200 computes on the B200 only: use device='cuda'")
@@ -144,7 +153,7 @@ class Operator:
         K = times.shape[0]
         if K == 0:
             return np.zeros((0, self._n if nodes is None else len(nodes)))
-        uniform = bool(times[0] > 0 and np.allclose(times, times[0] * np.arange(1, K + 1), rtol=1e-12, atol=0.0))
+        uniform = is_uniform_grid(times)
         if method not in ("auto", "steps", "batch"):
             raise ValueError(f"unknown method {method!r}")
         if method == "steps" and not uniform:
