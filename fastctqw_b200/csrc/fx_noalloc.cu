@@ -28,6 +28,9 @@
 // All calls on a device share the one array and it keeps the previous call's contents.  Calls
 // whose work overlaps on the GPU (different streams, or different host threads) race on it;
 // order them on one stream or synchronise between them.
+//
+// Every call waits for its stream before it returns: it copies the kernel's error word (the
+// bounded-wait status) back into a host variable and synchronises the stream to read it.
 #include <mutex>
 #include <string>
 
@@ -38,6 +41,10 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
 constexpr int kNoAllocSlices = 4;
 constexpr int kMaxDevices = 64;
+// Per-size limits checked before any size arithmetic: a row count above the array's byte size
+// can never fit, and the int8 level sums are exact in int32 only up to K = 32768.
+constexpr int64_t kMaxRows = (int64_t)kNoAllocScratchBytes;
+constexpr int64_t kMaxK = 32768;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -78,6 +85,14 @@ int fx_product_f32_noalloc(int64_t M, int64_t N, int64_t K, const float* A, int6
     if (M % 16 || N % 16 || K % 64)
       throw fx::Error{FX_ERR_VALUE, "noalloc product: M, N must be multiples of 16 and K of 64"};
     if (!A || !Bt || !D || (beta != 0.f && !C)) throw fx::Error{FX_ERR_VALUE, "noalloc product: null operand"};
+    // Bound each size before the scratch arithmetic so that 4 (M + N) K cannot wrap: a huge M or
+    // N would otherwise give a small product and pass the check below.  K <= 32768 is also the
+    // exactness bound of the int32 level sums.
+    if (M > kMaxRows || N > kMaxRows || K > kMaxK)
+      throw fx::Error{FX_ERR_VALUE, "noalloc product: M, N must be at most " + std::to_string(kMaxRows) +
+                                        " and K at most " + std::to_string(kMaxK) +
+                                        " (the fixed scratch array holds " +
+                                        std::to_string(kNoAllocScratchBytes) + " bytes)"};
     const size_t exp_bytes = round256(sizeof(int) * (size_t)(M + N));
     const size_t need = 256 + exp_bytes + (size_t)kNoAllocSlices * (size_t)(M + N) * (size_t)K;
     if (need > kNoAllocScratchBytes)

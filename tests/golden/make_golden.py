@@ -1,8 +1,9 @@
 """Generate the golden fixtures from the reference's own CPU path.
 
-Run in a container where the reference checkout exists (it is read, never modified):
+Run where a checkout of the reference exists (it is read, never modified), passing its root
+directory as the argument or in the environment variable FASTCTQW_REFERENCE_ROOT:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 The reference package ``FastCTQW`` imports matplotlib/seaborn eagerly
 (FastCTQW/__init__.py:3 via Plot.py:1-2) and the compiled ``_fastexpm_core``
@@ -154,4 +155,7 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FASTCTQW_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout> (or set FASTCTQW_REFERENCE_ROOT)")
+    main(root)

@@ -45,9 +45,11 @@ def test_noalloc_matches_allocating_product_twice():
     stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
     gen = torch.Generator(device="cpu").manual_seed(11)
     cases = [
-        # (M, N, K, alpha, beta, gamma): two different shapes in a row
-        (256, 384, 640, 1.0, 0.0, 0.0),
+        # (M, N, K, alpha, beta, gamma), one call after another on the shared array:
+        (256, 384, 640, 1.0, 0.0, 0.0),        # whole 128-row tiles
         (512, 512, 1024, -0.75, 2.0, 1.5),
+        (144, 208, 64, 1.25, -0.5, 0.25),      # partial tiles: clipped rows and columns, one K step
+        (1408, 1408, 1408, 1.0, 1.0, -2.0),    # the largest square size the array holds
     ]
     for M, N, K, alpha, beta, gamma in cases:
         A = torch.randn(M, K, generator=gen).to(dev)
@@ -89,3 +91,24 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     assert b"scratch" in lib.fx_product_error()
     torch.cuda.synchronize()
     assert bool((D == 3.0).all())          # nothing was launched
+
+
+def test_noalloc_rejects_sizes_whose_scratch_arithmetic_would_wrap():
+    """Sizes far beyond the array are rejected before any arithmetic on them: with M = 2^60 the
+    scratch size 4 (M + N) K wraps around 64 bits to a small number, which a check of the product
+    alone would let through.  Nothing is launched, so the small operands are never read."""
+    import torch
+    lib = _native.lib()
+    dev = torch.device("cuda", 0)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    A = torch.zeros(16, 64, device=dev)
+    Bt = torch.zeros(16, 64, device=dev)
+    D = torch.full((16, 16), 3.0, device=dev)
+    for M, N, K in [(1 << 60, 16, 64), (16, 1 << 60, 64), (16, 16, 1 << 40)]:
+        assert (4 * (M + N) * K) % (1 << 64) < SCRATCH_BYTES or K > 32768
+        rc = lib.fx_product_f32_noalloc(M, N, K, _p(A), 64, _p(Bt), 64, 1.0, 0.0, None, 0, 0.0,
+                                        _p(D), 16, stream)
+        assert rc == _native.ERR_VALUE, (M, N, K)
+        assert b"at most" in lib.fx_product_error()
+    torch.cuda.synchronize()
+    assert bool((D == 3.0).all())
