@@ -33,6 +33,19 @@ sys.path.insert(0, REPO)
 METRIC = "expm(-iHt) ms at N=10k c64; batched walks/s; chosen vs plain @ infid<=1e-10"
 
 
+def product_traffic_per_launch():
+    """DRAM bytes (read + write) per k_gemm_i8 launch of the benchmark walk, from the committed ncu
+    capture of one walk's product launches (dram__bytes_read.sum + dram__bytes_write.sum), or None
+    when no capture for this workload is committed."""
+    path = os.path.join(REPO, "profiles", "k_gemm_i8_walk_n10000_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return {"bytes": d["dram_bytes_per_launch"], "source": d["summary"]}
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -132,30 +145,57 @@ def threads_used():
         return os.cpu_count()
 
 
+def reference_walks(n: int, seed: int, t: float, steps: int, budget_s: float):
+    """Full-size runs of the reference's CPU path on this host: X = -1j H t of the benchmark walk,
+    U = scipy.linalg.expm(X) (FastCTQW/Operator.py:74-76), psi = U psi0 (FastCTQW/Ctqw.py:94).
+    At least one run; more (up to `steps`) only while the runs so far stay within `budget_s`.
+    Returns (seconds of every timed run, (m, s) the algorithm picks)."""
+    from oracle import expm_oracle as eo
+    _, _, X = workload(n, seed, t)
+    psi0 = np.zeros(n, dtype=np.complex64)
+    psi0[0] = 1.0
+    times = []
+    while True:
+        t0 = time.perf_counter()
+        U = eo.reference_cpu_expm(X)
+        psi = U @ psi0
+        times.append(time.perf_counter() - t0)
+        del U, psi
+        if len(times) >= max(1, steps) or sum(times) * (len(times) + 1) / len(times) > budget_s:
+            break
+    sel = eo.select_pade(X.astype(np.complex128)) if n <= 4096 else None
+    return times, sel
+
+
 def run_reference(args, rank, world):
-    """--impl reference: the reference's CPU path (scipy.linalg.expm) on this host's cores."""
+    """--impl reference: the reference's CPU path (scipy.linalg.expm) on this host's cores, on
+    the benchmark's own N.  A full N = 10000 expm takes tens of seconds, so the run times as many
+    full walks as fit the step budget (at least one) and reports those steps; no warm-up run (a
+    second full run would only double the time)."""
     if rank != 0:
         return
-    n_sample = args.ref_sample_n
-    for _ in range(args.warmup):
-        cpu_reference_sample(n_sample, args.seed, args.t, 1)
-    sec, Xs = cpu_reference_sample(n_sample, args.seed, args.t, max(1, args.steps))
-    full_sec, sel_s, sel_full = scale_to_full(sec, Xs, args.n)
-    v = full_sec * 1e3
+    times, _ = reference_walks(args.n, args.seed, args.t, args.steps, args.ref_budget_s)
+    v = 1e3 * statistics.median(times)
     cores = threads_used()
-    sample = (f"scipy.linalg.expm (the reference CPU path, FastCTQW/Operator.py:76) on the same "
-              f"family at N={n_sample} (m={sel_s[0]}, s={sel_s[1]}), best of {max(1, args.steps)}, "
-              f"scaled to N={args.n} (m={sel_full[0]}, s={sel_full[1]}, s grown by log2 of the size ratio) "
-              f"by the flop model 8N^3(pi_m+s)+(8/3)N^3+8N^3")
+    # labelled cross-check: the earlier flop-model extrapolation from a small sample
+    sec, Xs = cpu_reference_sample(args.ref_sample_n, args.seed, args.t, 2)
+    model_sec, sel_s, sel_full = scale_to_full(sec, Xs, args.n)
+    sample = (f"scipy.linalg.expm + U psi0 (the reference CPU path, FastCTQW/Operator.py:74-76, Ctqw.py:94) "
+              f"on the full N={args.n} walk, {len(times)} run(s) timed ({args.steps} requested; runs are "
+              f"added only within a {args.ref_budget_s:.0f} s budget), median; OpenBLAS/MKL threads={cores}")
     print(json.dumps({
         "metric": METRIC, "value": round(v, 3), "unit": "ms", "impl": "reference", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+        "steps": len(times), "warmup": 0, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": round(v, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded G(n,0.5) Laplacian)",
         "config": {"workload": f"dense ER G(n={args.n}, p=0.5) Laplacian, t={args.t}, complex64 expm + U psi0",
                    "n": args.n, "t": args.t},
         "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": cores, "kind": "reference",
-                         "sample": sample},
+                         "sample": sample, "runs_s": [round(x, 2) for x in times]},
         "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "flop_model_cross_check": {"ms": round(model_sec * 1e3, 1),
+                                   "from": f"N={args.ref_sample_n} (m={sel_s[0]}, s={sel_s[1]}) scaled to "
+                                           f"(m={sel_full[0]}, s={sel_full[1]}) by 8N^3(pi_m+s)+(8/3)N^3+8N^3"},
     }), flush=True)
 
 
@@ -165,6 +205,37 @@ def full_size_selection(n_full, n_sample, sel_sample):
     from the sample's s (scipy picks s = 10, 11, 12 at N = 1024, 2048, 4096 here)."""
     import math
     return (13, sel_sample[1] + int(round(math.log2(n_full / n_sample))))
+
+
+def accuracy_vs_eigh(H: np.ndarray, t: float, dU, psi_e0, psi_e0_plain, dev, seed: int) -> dict:
+    """Accuracy of the timed walk against the FP64 eigendecomposition propagator
+    U_ref = V diag(exp(-i lambda t)) V^T of the real symmetric H (torch FP64 on the device):
+    the relative Frobenius error of the stored complex64 U, and the infidelity of the states of
+    |0> (the walk's own psi), of the uniform superposition and of a seeded random state (psi = U
+    psi0 in complex128 from the stored U)."""
+    import torch
+    from fastctqw_b200 import graphs
+    from oracle import expm_oracle as eo
+    n = H.shape[0]
+    lam, V = torch.linalg.eigh(torch.from_numpy(H).to(dev))
+    Vc = V.to(torch.complex128)
+    del V
+    Uref = (Vc * torch.exp(-1j * lam * t)) @ Vc.T
+    del Vc
+    torch.cuda.empty_cache()
+    out = {"oracle": "FP64 eigendecomposition of H on the device (torch.linalg.eigh)"}
+    ref0 = Uref[:, 0].cpu().numpy()
+    out["infidelity_e0"] = eo.infidelity(psi_e0.cpu().numpy(), ref0)
+    if psi_e0_plain is not None:
+        out["infidelity_e0_plain"] = eo.infidelity(psi_e0_plain.cpu().numpy(), ref0)
+    U = dU.to(torch.complex128)
+    out["u_rel_error"] = float(torch.linalg.matrix_norm(U - Uref) / torch.linalg.matrix_norm(Uref))
+    for kind, p0 in (("uniform", graphs.uniform_state(n)), ("random", graphs.random_state(n, seed))):
+        p = torch.from_numpy(p0).to(dev).to(torch.complex128)
+        out[f"infidelity_{kind}"] = eo.infidelity((U @ p).cpu().numpy(), (Uref @ p).cpu().numpy())
+    del U, Uref
+    torch.cuda.empty_cache()
+    return out
 
 
 def batch_workload(count: int, seed: int, nmin: int, nmax: int):
@@ -394,7 +465,10 @@ def main():
     ap.add_argument("--form", default="plain", choices=["plain", "mixed", "simt"])
     ap.add_argument("--selector", default="learned", choices=["plain", "certified", "learned"],
                     help="(m, s) selection of the timed walk; the plain selection is timed beside it")
-    ap.add_argument("--ref-sample-n", type=int, default=1024)
+    ap.add_argument("--ref-sample-n", type=int, default=1024,
+                    help="size of the small sample behind the flop-model cross-check of the reference arm")
+    ap.add_argument("--ref-budget-s", type=float, default=240.0,
+                    help="reference arm: full-size runs are added while their total stays within this")
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 infidelity check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) leg")
@@ -403,8 +477,8 @@ def main():
     ap.add_argument("--batch-only", action="store_true", help="run only the uneven-batch leg")
     ap.add_argument("--no-setup", action="store_true", help="skip the device set-up / time-curve leg")
     ap.add_argument("--no-autotune", action="store_true", help="batch leg: default schedule, no autotuning")
-    ap.add_argument("--batch-shard", action="store_true",
-                    help="with N > 1 ranks: also run the uneven batch sharded over the ranks")
+    ap.add_argument("--batch-shard", action=argparse.BooleanOptionalAction, default=True,
+                    help="with N > 1 ranks: also run the uneven batch sharded over the ranks (default on)")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-nmin", type=int, default=64)
     ap.add_argument("--batch-nmax", type=int, default=2048)
@@ -495,19 +569,30 @@ def main():
     step()
     torch.cuda.synchronize()
     pst = eng.stats()
+    stages = {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in eng.product_profile().items()}
     eng.configure(profile=False)
     pk, pk_kind = peaks()
-    int8_peak = 2.0 * pk["bf16_tflops"]        # B200 int8 dense rate = 2x the BF16 rate
+    from fastctqw_b200 import _native
+    i8 = _native.tensor_peak("int8")
+    bf = _native.tensor_peak("bf16")
+    int8_peak = i8["tops"]
     achieved = pst["prod_ops"] / (pst["prod_ms"] * 1e-3) / 1e12 if pst["prod_ms"] > 0 else None
+    traffic = product_traffic_per_launch()
     roofline = {
         "bound": "tensor", "kernel": "k_gemm_i8<5,double> (int8 Ozaki-slice product, exact accumulation)",
         "achieved": round(achieved, 1) if achieved else None, "peak": round(int8_peak, 1), "unit": "TOP/s (int8)",
         "frac": round(achieved / int8_peak, 3) if achieved else None,
-        "peak_source": f"2 x bf16_tflops of MEASURED_PEAKS.json ({pk_kind})",
-        "traffic": None,
+        "peak_source": "measured on this GPU by fx_tensor_peak (tcgen05.mma kind::i8 M128 N256, operands in "
+                       "shared memory, one CTA per SM, median of 5 launches)",
+        "traffic": traffic["bytes"] if traffic else None,
+        "traffic_source": traffic["source"] if traffic else None,
         "launches": pst["prod_launches"], "kernel_ms_per_walk": round(pst["prod_ms"], 3),
         "kernel_share_of_walk": round(pst["prod_ms"] / ms_per_step, 3),
         "useful_real_tflops": round(pst["prod_flops"] / (pst["prod_ms"] * 1e-3) / 1e12, 2) if pst["prod_ms"] else None,
+        "frac_of_2x_bf16": round(achieved / (2.0 * pk["bf16_tflops"]), 3) if achieved else None,
+        "bf16_peak_measured_here": round(bf["tops"], 1),
+        "bf16_peak_measured_peaks_json": pk.get("bf16_tflops"), "peaks_json": pk_kind,
+        "stages": stages,
     }
 
     # ---- the plain (Al-Mohy & Higham) selection on the same walk, timed the same way
@@ -532,17 +617,8 @@ def main():
     # ---- accuracy of both against the FP64 eigendecomposition propagator
     accuracy = None
     if not args.no_check and rank == 0:
-        from oracle import expm_oracle as eo
-        Hd = torch.from_numpy(H).to(dev)
-        lam, V = torch.linalg.eigh(Hd)
-        Vc = V.to(torch.complex128)
-        ref = (Vc @ (torch.exp(-1j * lam * args.t) * Vc[0])).cpu().numpy()
-        accuracy = {"infidelity_e0": eo.infidelity(psi_chosen.cpu().numpy(), ref),
-                    "unitarity_residual": unitarity}
-        if psi_plain is not None:
-            accuracy["infidelity_e0_plain"] = eo.infidelity(psi_plain.cpu().numpy(), ref)
-        del Hd, V, lam, Vc
-        torch.cuda.empty_cache()
+        accuracy = accuracy_vs_eigh(H, args.t, dU, psi_chosen, psi_plain, dev, args.seed)
+        accuracy["unitarity_residual"] = unitarity
 
     # ---- end to end through the drop-in API (host ndarray in, host ndarray out)
     e2e = None
@@ -556,18 +632,27 @@ def main():
         for _ in range(e_steps):
             Uh = em.run(X_pinned)
         e2e_ms = (time.perf_counter() - t0) * 1e3 / e_steps
+        del Uh
+        # the same call with an ordinary (pageable) numpy input, as most callers pass it
+        em.run(X)
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            Uh = em.run(X)
+        e2e_pageable_ms = (time.perf_counter() - t0) * 1e3 / e_steps
         em.free()
         e2e = {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(X.nbytes),
-               "d2h_bytes_per_step": int(Uh.nbytes), "api": "fastexpm.ExpMatComplex64.run"}
+               "d2h_bytes_per_step": int(Uh.nbytes), "api": "fastexpm.ExpMatComplex64.run",
+               "input": "page-locked numpy array; output a new (pageable) numpy array per call",
+               "steps": e_steps, "pageable_input_ms": round(e2e_pageable_ms, 3)}
+        del Uh, X_pinned
 
     # ---- CPU baseline (reference CPU path on this host, bounded sample, rank 0, N=1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        sec, Xs = cpu_reference_sample(args.ref_sample_n, args.seed, args.t, 2)
-        full_sec, sel_s, sel_full = scale_to_full(sec, Xs, n)
-        cpu = {"value": round(full_sec * 1e3, 1), "unit": "ms", "cores": threads_used(), "kind": "reference",
-               "sample": f"scipy.linalg.expm at N={args.ref_sample_n} (m={sel_s[0]}, s={sel_s[1]}), best of 2, "
-                         f"scaled to N={n} (m={sel_full[0]}, s={sel_full[1]}) by 8N^3(pi_m+s)+(8/3)N^3+8N^3"}
+        times, _ = reference_walks(n, args.seed, args.t, 1, args.ref_budget_s)
+        cpu = {"value": round(1e3 * times[0], 1), "unit": "ms", "cores": threads_used(), "kind": "reference",
+               "sample": f"one full N={n} walk of the reference CPU path: scipy.linalg.expm(X) + U psi0 "
+                         f"(FastCTQW/Operator.py:74-76, Ctqw.py:94) on this host"}
 
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:

@@ -21,7 +21,8 @@ CODE_DTYPE = {v: k for k, v in DTYPE_CODE.items()}
 
 FORM_PLAIN, FORM_MIXED, FORM_SIMT, FORM_FP64 = 0, 1, 2, 3
 FORMS = {"plain": FORM_PLAIN, "mixed": FORM_MIXED, "simt": FORM_SIMT, "fp64": FORM_FP64}
-OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE, OPT_DEBUG_STAGE, OPT_PROFILE, OPT_SELECTOR = range(11)
+(OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE,
+ OPT_DEBUG_STAGE, OPT_PROFILE, OPT_SELECTOR, OPT_INJECT_STALL) = range(12)
 SELECTORS = {"plain": 0, "certified": 1, "learned": 2}
 
 OK, ERR_TYPE, ERR_VALUE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_NONFINITE, ERR_SINGULAR, ERR_NODEV, ERR_FREED = range(10)
@@ -57,6 +58,8 @@ SIGNATURES = {
     "fx_get_n": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)],
     "fx_set_option": [ctypes.c_void_p, ctypes.c_int, ctypes.c_double],
     "fx_get_stats": [ctypes.c_void_p, ctypes.POINTER(FxStats)],
+    "fx_product_profile": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double),
+                           ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)],
     "fx_last_error": [ctypes.c_void_p],
     "fx_run_host": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "fx_run_device": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
@@ -69,6 +72,8 @@ SIGNATURES = {
                        ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int64,
                        ctypes.c_float, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
     "fx_product_error": [],
+    "fx_tensor_peak": [ctypes.c_int, ctypes.c_int64, ctypes.POINTER(ctypes.c_double),
+                       ctypes.POINTER(ctypes.c_double), ctypes.c_void_p],
     "fx_build_generator": [ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int,
                            ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     "fx_check_hermitian": [ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
@@ -173,6 +178,22 @@ def product_f32(form: str, A, Bt, alpha=1.0, beta=0.0, C=None, gamma=0.0, D=None
     return D
 
 
+def tensor_peak(kind: str = "int8", iters: int = 50000, reps: int = 5, stream=None) -> dict:
+    """Measured dense tensor-core rate (fx_tensor_peak): the median of `reps` launches, in
+    tera-ops per second (2 M N K per instruction)."""
+    k = {"int8": 0, "bf16": 1}[kind]
+    tops, ms = ctypes.c_double(), ctypes.c_double()
+    vals = []
+    for _ in range(reps + 1):   # the first launch warms up
+        rc = lib().fx_tensor_peak(k, int(iters), ctypes.byref(tops), ctypes.byref(ms), stream)
+        if rc != OK:
+            raise RuntimeError(lib().fx_product_error().decode())
+        vals.append((tops.value, ms.value))
+    vals = sorted(vals[1:])
+    return {"tops": vals[len(vals) // 2][0], "ms": vals[len(vals) // 2][1], "reps": reps,
+            "all_tops": [round(v[0], 1) for v in vals]}
+
+
 def device_ok() -> bool:
     return bool(lib().fx_device_ok())
 
@@ -200,7 +221,8 @@ class Engine:
                   structure: bool | None = None, force_m: int | None = None,
                   force_s: int | None = None, ipe: bool | None = None,
                   timeout_ms: float | None = None, debug_stage: int | None = None,
-                  profile: bool | None = None, selector: str | None = None) -> None:
+                  profile: bool | None = None, selector: str | None = None,
+                  inject_stall: int | None = None) -> None:
         if form is not None:
             if form not in FORMS:
                 raise ValueError(f"form must be one of {sorted(FORMS)}")
@@ -225,11 +247,34 @@ class Engine:
             if selector not in SELECTORS:
                 raise ValueError(f"selector must be one of {sorted(SELECTORS)}")
             self.set_option(OPT_SELECTOR, SELECTORS[selector])
+        if inject_stall is not None:
+            self.set_option(OPT_INJECT_STALL, inject_stall)
 
     def stats(self) -> dict:
         st = FxStats()
         check(lib().fx_get_stats(self._h, ctypes.byref(st)), self._h)
         return st.as_dict()
+
+    PRODUCT_STAGES = ("powers", "pade", "solve", "cholesky", "inverse", "triangular", "squarings",
+                      "diagnostics")
+
+    def product_profile(self) -> dict:
+        """Per-stage product time of the last profiled walk-generator run (configure(profile=True)):
+        {stage: {"launches", "ms", "ops"}}."""
+        cnt = ctypes.c_int32()
+        check(lib().fx_product_profile(self._h, None, None, None, 0, ctypes.byref(cnt)), self._h)
+        n = cnt.value
+        tags = (ctypes.c_int32 * max(n, 1))()
+        ms = (ctypes.c_double * max(n, 1))()
+        ops = (ctypes.c_double * max(n, 1))()
+        check(lib().fx_product_profile(self._h, tags, ms, ops, n, ctypes.byref(cnt)), self._h)
+        out: dict = {}
+        for i in range(n):
+            d = out.setdefault(self.PRODUCT_STAGES[tags[i]], {"launches": 0, "ms": 0.0, "ops": 0.0})
+            d["launches"] += 1
+            d["ms"] += ms[i]
+            d["ops"] += ops[i]
+        return out
 
     # -- host buffers
     def _host_in(self, A) -> np.ndarray:

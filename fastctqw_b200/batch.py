@@ -113,7 +113,8 @@ class WalkBatch:
         return np.array(m[:], dtype=np.int32), np.array(s[:], dtype=np.int32)
 
     def sample_check(self) -> dict:
-        """The last run's sampled comparison with the plain method: walks re-run, largest
+        """The last run's sampled comparison with the plain method: walks re-run (0 when no
+        walk took a non-plain (m, s), -1 when skipped for a batch of one walk), largest
         infidelity between the two states."""
         c, m = ctypes.c_int32(), ctypes.c_double()
         _check(lib().fx_batch_sample_check(self._h, ctypes.byref(c), ctypes.byref(m)), self._h)

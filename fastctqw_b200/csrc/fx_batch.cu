@@ -858,6 +858,9 @@ class BatchPipeline {
     key2_.clear();
   }
   int selector() const { return selector_; }
+  // Diagnostics of the failure path: product launch k (k >= 0) of every run leaves the loads of
+  // its first K step out, so that its bounded waits run out; runs are then replayed eagerly.
+  void set_inject_stall(int k) { inject_ = k; }
   void details(int w, double* feat, int* pm, int* ps, int* cm, int* cs, int* outcome) const {
     for (int k = 0; k < 8; ++k) feat[k] = features_.empty() ? 0.0 : features_[8 * w + k];
     *pm = plain_m_.empty() ? 0 : plain_m_[w];
@@ -886,6 +889,8 @@ class BatchPipeline {
     st->prod_launches = prod_launches_;
   }
   int gemm_launches() const { return gemm_launches_; }
+  // Skip-tile argument of the next product launch (the injected stall hits tile 0 of launch k).
+  int next_skip() { return (inject_ >= 0 && prod_index_++ == inject_) ? 0 : -1; }
 
   // psi_w = expm(X_w) psi0_w and/or U_w = expm(X_w); any of dpsi0 / dpsi / dU may be null (a
   // null table, or a null entry, skips that output for that walk).
@@ -894,6 +899,7 @@ class BatchPipeline {
     stream_ = s;
     launches_ = 0;
     gemm_launches_ = 0;
+    prod_index_ = 0;
     prof_reset();
     std::vector<const void*> tab(4 * W, nullptr);
     for (int w = 0; w < W; ++w) {
@@ -907,7 +913,7 @@ class BatchPipeline {
     FX_CUDA(cudaMemsetAsync(flags(), 0, sizeof(int) * W, s));
 
     // ---- phase 1: statistics and shifts, powers, exact norms, estimates (one host round trip)
-    run_recorded(desc1_, st1_, r1_, graph1_, use_graph_ && !profile_);
+    run_recorded(desc1_, st1_, r1_, graph1_, use_graph_ && !profile_ && inject_ < 0);
     std::vector<double>& h_wo = walkrec_;
     h_wo.assign(kWO * W, 0.0);
     std::vector<int> h_flags(W);
@@ -1029,6 +1035,8 @@ class BatchPipeline {
     FX_CUDA(cudaMemcpyAsync(werr.data(), walk_err(), sizeof(int) * W, cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaMemcpyAsync(&herr, err_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaStreamSynchronize(s));
+    // a wait that ran out leaves every later result meaningless: report it before anything else
+    if (herr & kDevTimeout) throw Error{FX_ERR_TIMEOUT, "a device-side wait timed out"};
     bool any = false;
     for (int w = 0; w < W; ++w) {
       if (!werr[w]) continue;
@@ -1092,7 +1100,7 @@ class BatchPipeline {
       FX_CUDA(cudaMemcpyAsync(desc2_.p, st2_.buf.data(), st2_.buf.size(), cudaMemcpyHostToDevice, stream_));
       key2_ = profile_ ? std::vector<double>() : key;
     }
-    run_recorded(desc2_, st2_, r2_, graph2_, use_graph_ && !profile_, false);
+    run_recorded(desc2_, st2_, r2_, graph2_, use_graph_ && !profile_ && inject_ < 0, false);
   }
 
   // A-posteriori unitarity check of the walks that did not take the plain (m, s): ||psi|| must
@@ -1105,7 +1113,9 @@ class BatchPipeline {
   // non-plain (m, s) (the smallest, so that the check stays cheap; ties to the lower index) are
   // run again with the plain (m, s) in a side pipeline, and the two states compared.  An
   // infidelity above kSampleInfid marks every non-plain walk of the batch for the plain redo.
-  // The sample is taken only if it costs at most a tenth of the batch.
+  // Walks are dropped from the sample (largest first) while it costs more than a tenth of the
+  // batch by N^3, but one walk is always sampled; only a batch of one walk (a single structured
+  // walk, which would be computed twice) skips the comparison (sample_count_ = -1).
   bool sample_compare(const std::vector<const void*>& tab, std::vector<int>& own) {
     constexpr double kSampleInfid = 1e-10;
     const int W = count();
@@ -1117,14 +1127,19 @@ class BatchPipeline {
           (sel_m_[w] != plain_m_[w] || sel_s_[w] != plain_s_[w]))
         cand.push_back(w);
     if (cand.empty() || sample_walks_ <= 0) return false;
+    if (W == 1) {
+      sample_count_ = -1;
+      return false;
+    }
     std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) { return walks_[a].n < walks_[b].n; });
     if ((int)cand.size() > sample_walks_) cand.resize(sample_walks_);
-    // skipped when the re-runs would cost more than a tenth of the batch (by N^3): a batch of
-    // one walk (a single structured walk) would otherwise be computed twice
     double all_n3 = 0.0, cand_n3 = 0.0;
     for (int w = 0; w < W; ++w) all_n3 += std::pow((double)walks_[w].n, 3);
     for (int w : cand) cand_n3 += std::pow((double)walks_[w].n, 3);
-    if (cand_n3 > 0.1 * all_n3) return false;
+    while (cand.size() > 1 && cand_n3 > 0.1 * all_n3) {
+      cand_n3 -= std::pow((double)walks_[cand.back()].n, 3);
+      cand.pop_back();
+    }
     std::vector<int64_t> ns;
     for (int w : cand) ns.push_back(walks_[w].n);
     if (!sample_pipe_ || ns != sample_ns_) {
@@ -1262,15 +1277,27 @@ class BatchPipeline {
   unsigned timeout_ms_ = 2000;
   bool use_graph_ = true, profile_ = false;
   int force_m_ = -1, force_s_ = -1;
+  int inject_ = -1, prod_index_ = 0;   // stall injection (diagnostics), product launches so far
   int launches_ = 0, gemm_launches_ = 0;
   double flops_ = 0;
   cudaGraphExec_t graph1_ = nullptr, graph2_ = nullptr;
   unsigned char* desc_base_ = nullptr;
   // product-launch timing (profile mode)
   std::vector<cudaEvent_t> ev_pool_;
-  std::vector<std::pair<double, double>> ev_work_;
+  struct ProdWork {
+    double ops, flops;
+    int tag;
+  };
+  std::vector<ProdWork> ev_work_;
   double prod_ms_ = 0, prod_ops_ = 0, prod_flops_ = 0;
   int prod_launches_ = 0;
+  int tag_ = kTagPowers;                  // stage of the products being recorded
+  std::vector<ProdRecord> prod_list_;    // per product launch of the last profiled run
+
+ public:
+  const std::vector<ProdRecord>& prod_list() const { return prod_list_; }
+
+ private:
 
  public:
   void force(int m, int s) {
@@ -1347,6 +1374,7 @@ class BatchPipeline {
 
   void prof_reset() {
     ev_work_.clear();
+    prod_list_.clear();
     prod_ms_ = prod_ops_ = prod_flops_ = 0;
     prod_launches_ = 0;
   }
@@ -1362,10 +1390,10 @@ class BatchPipeline {
     FX_CUDA(cudaEventRecord(ev_pool_[2 * i], stream_));
     return i;
   }
-  void prof_end(size_t i, double ops, double fl) {
+  void prof_end(size_t i, double ops, double fl, int tag) {
     if (!profile_) return;
     FX_CUDA(cudaEventRecord(ev_pool_[2 * i + 1], stream_));
-    ev_work_.push_back({ops, fl});
+    ev_work_.push_back({ops, fl, tag});
   }
   void prof_collect() {
     if (!profile_) return;
@@ -1373,8 +1401,9 @@ class BatchPipeline {
       float t = 0;
       FX_CUDA(cudaEventElapsedTime(&t, ev_pool_[2 * i], ev_pool_[2 * i + 1]));
       prod_ms_ += t;
-      prod_ops_ += ev_work_[i].first;
-      prod_flops_ += ev_work_[i].second;
+      prod_ops_ += ev_work_[i].ops;
+      prod_flops_ += ev_work_[i].flops;
+      prod_list_.push_back(ProdRecord{ev_work_[i].tag, (double)t, ev_work_[i].ops, ev_work_[i].flops});
     }
     prod_launches_ = (int)ev_work_.size();
   }
@@ -1446,6 +1475,7 @@ class BatchPipeline {
       FX_LAUNCH_CHECK();
     });
     r.launches += 3;
+    tag_ = kTagPowers;
     product(st, r, all, kY, kY, -1.0, -1, 0.0, 0.0, kA2, true);
     product(st, r, all, kA2, kA2, 1.0, -1, 0.0, 0.0, kA4, true);
     product(st, r, all, kA4, kA2, 1.0, -1, 0.0, 0.0, kA6, true);
@@ -1655,6 +1685,7 @@ class BatchPipeline {
     for (const GSlab& g : b_sorted) b_span = std::max<int64_t>(b_span, (int64_t)g.row0 + g.rows);
     r.launches += same ? 2 : 3;
     r.gemms += 1;
+    const int tag = tag_;
     r.ops.push_back([=]() {
       I8Slices outa{}, outb{};
       for (int q = 0; q < kS; ++q) {
@@ -1679,8 +1710,8 @@ class BatchPipeline {
       launch_gemm_i8_grouped<double>(kS, &t, 1, pitch_, a_rows_, same ? a_rows_ : rows_, aexp(),
                                      same ? aexp() : bexp(), dev<GProblem>(o_pr), dev<GTile>(o_t), nt,
                                      (int*)err_.p, timeout_ms_, stream_, split ? adiag() : nullptr,
-                                     split ? (same ? adiag() : bdiag()) : nullptr);
-      prof_end(pi, ops * kS * (kS + 1) / 2, ops);
+                                     split ? (same ? adiag() : bdiag()) : nullptr, next_skip());
+      prof_end(pi, ops * kS * (kS + 1) / 2, ops, tag);
     });
   }
 
@@ -1781,6 +1812,7 @@ class BatchPipeline {
     std::vector<double> al(W, 1.0), ga(W, 0.0);
     auto cs = [&](int w, int p) { return std::ldexp(1.0, -p * sel_s_[w]); };
     // m = 9: A8 = A4 A4 -> T2
+    tag_ = kTagPade;
     product(st, r, m9, kA4, kA4, 1.0, -1, 0.0, 0.0, kT2, true);
     // m = 13: T1 = b13 A6 + b11 A4 + b9 A2 (scaled), T2 = A6 T1 (scaled)
     for (int w : m13) {
@@ -1832,6 +1864,7 @@ class BatchPipeline {
 
     // ---- solve: G = V^2 + W^2 = L L^T, P2 = (V + iW)^2, R = G^-1 P2
     // V ~ b_0 I once scaled: these products and the complex ones below split the diagonals off
+    tag_ = kTagSolve;
     product(st, r, all, kV, kV, 1.0, -1, 0.0, 0.0, kT1, true, nullptr, nullptr, true);    // VV
     product(st, r, all, kW, kW, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, true);    // WW
     product(st, r, all, kV, kW, 1.0, -1, 0.0, 0.0, kA2, true, nullptr, nullptr, true);    // VW
@@ -1843,10 +1876,13 @@ class BatchPipeline {
     combo(st, r, all, kA6, m_12, cf);                             // P2 re -> A6
     for (int w = 0; w < W; ++w) cf[w] = {2.0, 0.0, 0.0, 0.0, 0.0};
     combo(st, r, all, kY, m_a2, cf);                              // P2 im -> Y
+    tag_ = kTagCholesky;
     cholesky(st, r, kA4);
     transpose(st, r, all, kA4, kT1);                              // L^T -> T1
+    tag_ = kTagInverse;
     inverse(st, r, kT1, kT2, kW, kA2);                            // X = L^-1 -> T2, X^T -> W (scratch A2)
     // Z = P2 X^T (re -> V, im -> T1); R^T = Z X (re -> A4, im -> A2)
+    tag_ = kTagTriangular;
     complex_by_real(st, r, all, kA6, kY, kT2, kV, kT1, 1, true);    // P2 symmetric
     complex_by_real(st, r, all, kV, kT1, kW, kA4, kA2, 2, false);
     symmetrize(st, r, all, kA4);
@@ -1999,8 +2035,9 @@ class BatchPipeline {
         }
         size_t pi = prof_begin();
         launch_gemm_i8_grouped<double>(kS, t, 2, pitch_, rows_, rows_, aexp(), aexp(), dev<GProblem>(o_r),
-                                       dev<GTile>(o_t), nt, (int*)err_.p, timeout_ms_, stream_);
-        prof_end(pi, ops * kS * (kS + 1) / 2, ops);
+                                       dev<GTile>(o_t), nt, (int*)err_.p, timeout_ms_, stream_, nullptr, nullptr,
+                                       next_skip());
+        prof_end(pi, ops * kS * (kS + 1) / 2, ops, kTagSquare);
         // imaginary: Re Im + Im Re
         for (int q = 0; q < kS; ++q) {
           t[0].a[q] = out.re[q];
@@ -2010,8 +2047,9 @@ class BatchPipeline {
         }
         pi = prof_begin();
         launch_gemm_i8_grouped<double>(kS, t, 2, pitch_, rows_, rows_, aexp(), aexp(), dev<GProblem>(o_i),
-                                       dev<GTile>(o_t), nt, (int*)err_.p, timeout_ms_, stream_);
-        prof_end(pi, ops * kS * (kS + 1) / 2, ops);
+                                       dev<GTile>(o_t), nt, (int*)err_.p, timeout_ms_, stream_, nullptr, nullptr,
+                                       next_skip());
+        prof_end(pi, ops * kS * (kS + 1) / 2, ops, kTagSquare);
       });
     }
   }
@@ -2198,17 +2236,19 @@ class BatchPipeline {
 // ---- interface used by the per-walk engine (fx_engine.cu) for structured walks
 BatchPipeline* batch_pipeline_create(int64_t n, int dtype) { return new BatchPipeline({n}, dtype); }
 void batch_pipeline_destroy(BatchPipeline* p) { delete p; }
-void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU, bool profile,
-                        unsigned timeout_ms, int selector, cudaStream_t s) {
-  p->set_selector(selector);
+void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU,
+                        const PipeOpts& o, cudaStream_t s) {
+  p->set_selector(o.selector);
   const void* x[1] = {dX};
   const void* p0[1] = {dpsi0};
   void* p1[1] = {dpsi};
   void* u[1] = {dU};
-  p->set_profile(profile);
-  p->set_timeout(timeout_ms);
+  p->set_profile(o.profile);
+  p->set_timeout(o.timeout_ms);
+  p->set_inject_stall(o.inject_stall);
   p->run(x, p0, p1, u, s);
 }
+const std::vector<ProdRecord>& batch_pipeline_products(const BatchPipeline* p) { return p->prod_list(); }
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st) {
   p->walk_stats(0, st);
   double f[8];
@@ -2234,6 +2274,7 @@ struct fx_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double ms = 0;
   std::vector<void*> h_in;   // device staging of host runs (X, psi0, psi per walk)
+  fx::HostStage stage;       // page-locked chunks for the copies of the host matrices
   std::string last_error;
 };
 
@@ -2400,7 +2441,7 @@ int fx_batch_walk_host(fx_batch_handle b, const void* const* X, const void* cons
     }
     for (size_t w = 0; w < W; ++w) {
       const size_t n = (size_t)b->ns[w];
-      FX_CUDA(cudaMemcpyAsync(b->h_in[w], X[w], n * n * es, cudaMemcpyHostToDevice, b->stream));
+      b->stage.h2d(b->h_in[w], X[w], n * n * es, b->stream);
       FX_CUDA(cudaMemcpyAsync(b->h_in[W + w], psi0[w], n * es, cudaMemcpyHostToDevice, b->stream));
     }
     b->p->run((const void* const*)b->h_in.data(), (const void* const*)(b->h_in.data() + W),

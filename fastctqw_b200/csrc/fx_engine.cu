@@ -88,6 +88,7 @@ struct RunOpts {
   int debug_stage;   // 0: normal output; k > 0: output an intermediate (diagnostics)
   int profile;       // 1: time every int8 product launch with CUDA events
   int selector;      // (m, s) selection of the grouped path: 0 plain, 1 certified, 2 learned
+  int inject_stall;  // diagnostics of the grouped path: product launch that skips a K step (-1 off)
 };
 
 // Planar complex matrix view over owned storage; a missing plane is identically zero.
@@ -1040,7 +1041,8 @@ struct fx_engine {
   size_t elem = 8;
   fx::BatchPipeline* grouped = nullptr;   // grouped pipeline for walk generators (lazy)
   void* check_buf = nullptr;              // input statistics of the routing check
-  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0, 0};
+  fx::HostStage stage;                    // page-locked chunks for copies of host buffers
+  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0, 0, -1};
   fx_stats stats{};
   std::string last_error;
 };
@@ -1124,8 +1126,12 @@ void run_device(fx_handle h, const void* dA, void* dU, const void* dpsi0, void* 
   if (grouped_eligible(h) && fx_device_ok() && input_is_walk_generator(h, dA, s)) {
     if (!h->grouped) h->grouped = fx::batch_pipeline_create(h->n, h->dtype);
     FX_CUDA(cudaEventRecord(h->ev0, s));
-    fx::batch_pipeline_run(h->grouped, dA, dpsi0, dpsi, dU, h->opts.profile != 0, h->opts.timeout_ms,
-                           h->opts.selector, s);
+    fx::PipeOpts po;
+    po.profile = h->opts.profile != 0;
+    po.timeout_ms = h->opts.timeout_ms;
+    po.selector = h->opts.selector;
+    po.inject_stall = h->opts.inject_stall;
+    fx::batch_pipeline_run(h->grouped, dA, dpsi0, dpsi, dU, po, s);
     FX_CUDA(cudaEventRecord(h->ev1, s));
     FX_CUDA(cudaEventSynchronize(h->ev1));
     float ms = 0;
@@ -1217,6 +1223,7 @@ int fx_free(fx_handle h) {
     if (h->h_out) cudaFree(h->h_out);
     if (h->h_psi) cudaFree(h->h_psi);
     h->h_in = h->h_out = h->h_psi = nullptr;
+    h->stage.release();
     h->freed = true;
   });
 }
@@ -1275,8 +1282,26 @@ int fx_set_option(fx_handle h, int key, double value) {
       if (v < 0 || v > 2) return fail(h, fx::Error{FX_ERR_VALUE, "selector must be 0, 1 or 2"});
       h->opts.selector = v;
       return FX_OK;
+    case FX_OPT_INJECT_STALL:
+      if (v < -1) return fail(h, fx::Error{FX_ERR_VALUE, "stall injection takes a launch index >= 0, or -1"});
+      h->opts.inject_stall = v;
+      return FX_OK;
   }
   return fail(h, fx::Error{FX_ERR_VALUE, "unknown option"});
+}
+
+int fx_product_profile(fx_handle h, int32_t* tags, double* ms, double* ops, int32_t cap, int32_t* count) {
+  if (!h || !count || (cap > 0 && (!tags || !ms || !ops))) return fail(h, fx::Error{FX_ERR_VALUE, "null argument"});
+  *count = 0;
+  if (!h->grouped) return FX_OK;
+  const std::vector<fx::ProdRecord>& v = fx::batch_pipeline_products(h->grouped);
+  for (int32_t i = 0; i < cap && i < (int32_t)v.size(); ++i) {
+    tags[i] = v[i].tag;
+    ms[i] = v[i].ms;
+    ops[i] = v[i].ops;
+  }
+  *count = (int32_t)v.size();
+  return FX_OK;
 }
 
 int fx_get_stats(fx_handle h, fx_stats* out) {
@@ -1315,11 +1340,10 @@ int fx_run_host(fx_handle h, const void* A, void* U) {
     const size_t bytes = (size_t)h->n * h->n * h->elem;
     if (!h->h_in) FX_CUDA(cudaMalloc(&h->h_in, bytes));
     if (!h->h_out) FX_CUDA(cudaMalloc(&h->h_out, bytes));
-    FX_CUDA(cudaMemcpyAsync(h->h_in, A, bytes, cudaMemcpyHostToDevice, h->stream));
+    h->stage.h2d(h->h_in, A, bytes, h->stream);
     h->u_valid = false;
     run_device(h, h->h_in, h->h_out, nullptr, nullptr, h->stream);
-    FX_CUDA(cudaMemcpyAsync(U, h->h_out, bytes, cudaMemcpyDeviceToHost, h->stream));
-    FX_CUDA(cudaStreamSynchronize(h->stream));
+    h->stage.d2h(U, h->h_out, bytes, h->stream);
   });
 }
 
@@ -1335,7 +1359,7 @@ int fx_walk_host(fx_handle h, const void* A, const void* psi0, void* psi) {
     if (!h->h_psi) FX_CUDA(cudaMalloc(&h->h_psi, 2 * vbytes));
     char* dpsi0 = (char*)h->h_psi;
     char* dpsi = dpsi0 + vbytes;
-    FX_CUDA(cudaMemcpyAsync(h->h_in, A, bytes, cudaMemcpyHostToDevice, h->stream));
+    h->stage.h2d(h->h_in, A, bytes, h->stream);
     FX_CUDA(cudaMemcpyAsync(dpsi0, psi0, vbytes, cudaMemcpyHostToDevice, h->stream));
     h->u_valid = false;
     run_device(h, h->h_in, h->h_out, dpsi0, dpsi, h->stream);
@@ -1352,8 +1376,7 @@ int fx_fetch_u(fx_handle h, void* U) {
     if (h->n == 0) return;
     if (!h->u_valid || !h->h_out) throw fx::Error{FX_ERR_VALUE, "no walk result on the device"};
     const size_t bytes = (size_t)h->n * h->n * h->elem;
-    FX_CUDA(cudaMemcpyAsync(U, h->h_out, bytes, cudaMemcpyDeviceToHost, h->stream));
-    FX_CUDA(cudaStreamSynchronize(h->stream));
+    h->stage.d2h(U, h->h_out, bytes, h->stream);
   });
 }
 

@@ -72,6 +72,7 @@ struct I8Params {
   const GTile* tiles;
   const double* adg;   // diagonal split: removed diagonals by stacked row
   const double* bdg;
+  int skip_tile;       // diagnostics: the producer skips the first K step's loads of this tile
 };
 
 __host__ __device__ constexpr uint32_t idesc_i8(int m, int n) {
@@ -285,6 +286,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
               ok = false;
               break;
             }
+            // Failure-path diagnostics: leave one stage unfilled, so that the MMA warp's bounded
+            // wait runs out and every role takes its timeout exit.
+            if (tile == p.skip_tile && t == 0 && kb == jb.kb0) continue;
             uint8_t* st = smem + (size_t)s * kStage;
             mbar_expect_tx(&full_bar[s], kStage);
             for (int q = 0; q < S; ++q) {
@@ -857,6 +861,7 @@ void launch_gemm_i8(int S, int64_t M, int64_t N, int64_t K, const I8Term* terms,
   p.ldd = ldd;
   p.err = err;
   p.timeout_ns = (unsigned long long)timeout_ms * 1000000ull;
+  p.skip_tile = -1;
   if (S == 4)
     launch_i8_cfg<4, TO>(p, terms, nterms, M, N, K, lda, ldb, s);
   else if (S == 5)
@@ -914,7 +919,8 @@ void prepare_gemm_i8_grouped(int S) {
 template <typename TO>
 void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitch, int64_t a_rows, int64_t b_rows,
                             const int* aexp, const int* bexp, const GProblem* probs, const GTile* tiles, int ntiles,
-                            int* err, unsigned timeout_ms, cudaStream_t s, const double* adg, const double* bdg) {
+                            int* err, unsigned timeout_ms, cudaStream_t s, const double* adg, const double* bdg,
+                            int skip_tile) {
   if (nterms < 1 || nterms > kMaxTerms) throw Error{FX_ERR_VALUE, "int8 product: 1 or 2 terms"};
   if (ntiles <= 0) return;
   if (pitch % kBK || pitch <= 0 || pitch > 32768) throw Error{FX_ERR_VALUE, "grouped int8 product: bad pitch"};
@@ -929,6 +935,7 @@ void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitc
   p.tiles = tiles;
   p.adg = adg;
   p.bdg = bdg;
+  p.skip_tile = skip_tile;
   if (S == 4)
     launch_i8_grouped_cfg<4, TO>(p, terms, nterms, pitch, a_rows, b_rows, ntiles, s);
   else if (S == 5)
@@ -938,9 +945,9 @@ void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitc
 }
 template void launch_gemm_i8_grouped<float>(int, const I8Term*, int, int64_t, int64_t, int64_t, const int*,
                                             const int*, const GProblem*, const GTile*, int, int*, unsigned,
-                                            cudaStream_t, const double*, const double*);
+                                            cudaStream_t, const double*, const double*, int);
 template void launch_gemm_i8_grouped<double>(int, const I8Term*, int, int64_t, int64_t, int64_t, const int*,
                                              const int*, const GProblem*, const GTile*, int, int*, unsigned,
-                                             cudaStream_t, const double*, const double*);
+                                             cudaStream_t, const double*, const double*, int);
 
 }  // namespace fx

@@ -3,6 +3,8 @@
 // the given stream.  Matrices are planar complex: separate real and imaginary planes,
 // row-major with leading dimension `ld`; an imaginary plane of nullptr means "zero".
 #pragma once
+#include <vector>
+
 #include "fx_common.cuh"
 
 namespace fx {
@@ -220,11 +222,53 @@ void prepare_gemm_i8_grouped(int S);
 // generators X = i*(real symmetric), plain form (int8 slices on FP64 masters).  Any of dpsi0 /
 // dpsi / dU may be null.  Throws fx::Error (FX_ERR_VALUE when X is not of that form).
 class BatchPipeline;
+// Stage of a product launch, for the per-launch timing of a profiled run.
+enum ProdTag {
+  kTagPowers = 0,      // A2, A4, A6 (and A8)
+  kTagPade = 1,        // Pade numerator / denominator products
+  kTagSolve = 2,       // V^2, W^2, VW of the solve
+  kTagCholesky = 3,    // Cholesky panel and trailing updates
+  kTagInverse = 4,     // explicit inverse of the Cholesky factor
+  kTagTriangular = 5,  // Z = P2 L^-T, R^T = Z L^-1
+  kTagSquare = 6,      // squarings
+  kTagDrift = 7        // diagnostic unitarity products
+};
+struct ProdRecord {
+  int tag;
+  double ms, ops, flops;
+};
 BatchPipeline* batch_pipeline_create(int64_t n, int dtype);
 void batch_pipeline_destroy(BatchPipeline* p);
-void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU, bool profile,
-                        unsigned timeout_ms, int selector, cudaStream_t s);
+// Options of one run of the one-walk pipeline.
+struct PipeOpts {
+  bool profile = false;      // CUDA-event timing of every product launch
+  unsigned timeout_ms = 2000;
+  int selector = 0;          // 0 Al-Mohy & Higham, 1 certified bound, 2 learned
+  int inject_stall = -1;     // diagnostics: k >= 0 makes product launch k of every run skip the
+                             // operand loads of its first K step, so that the bounded waits run out
+};
+void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU,
+                        const PipeOpts& o, cudaStream_t s);
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st);
+const std::vector<ProdRecord>& batch_pipeline_products(const BatchPipeline* p);
+// Host <-> device copies of large host buffers (fx_hostcopy.cu): a buffer the driver knows as
+// page-locked is copied by DMA directly; any other goes through two page-locked chunk buffers,
+// the host side of a chunk (split over threads) overlapping the DMA of the previous one.
+bool host_is_pinned(const void* p);
+struct HostStage {
+  void* buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  HostStage() = default;
+  HostStage(const HostStage&) = delete;
+  HostStage& operator=(const HostStage&) = delete;
+  ~HostStage();
+  void release();
+  void ensure();
+  // device dst <- host src, ordered on s; src may be reused once it returns.
+  void h2d(void* dst, const void* src, size_t bytes, cudaStream_t s);
+  // host dst <- device src after the work already on s; dst holds the data when it returns.
+  void d2h(void* dst, const void* src, size_t bytes, cudaStream_t s);
+};
 // Learned selector inference (fx_selector.cu): out[n x 6] = MLP(x[n x 8]), device pointers.
 void launch_mlp_infer(const float* w, const float* x, int n, float* out, cudaStream_t s);
 // Records the message returned by fx_product_error (fx_debug.cu).
@@ -236,7 +280,7 @@ template <typename TO>
 void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitch, int64_t a_rows,
                             int64_t b_rows, const int* aexp, const int* bexp, const GProblem* probs,
                             const GTile* tiles, int ntiles, int* err, unsigned timeout_ms, cudaStream_t s,
-                            const double* adg = nullptr, const double* bdg = nullptr);
+                            const double* adg = nullptr, const double* bdg = nullptr, int skip_tile = -1);
 // Grouped slicing: slab k copies rows [0, rows_k) of a planar (re, im) source with leading
 // dimension ld_k, K_k columns, into stacked rows [row0_k, row0_k + rows_k).  Slabs are sorted
 // by row0 and do not overlap; rows between slabs are left alone.

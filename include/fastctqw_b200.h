@@ -78,11 +78,15 @@ enum fx_option {
                              squarings) and stop                                       */
   FX_OPT_PROFILE = 9,     /* 1: CUDA-event timing of every tensor-core product launch
                              (fx_stats.prod_*)                                         */
-  FX_OPT_SELECTOR = 10    /* (m, s) selection for walk generators X = i*(real symmetric):
+  FX_OPT_SELECTOR = 10,   /* (m, s) selection for walk generators X = i*(real symmetric):
                              0 Al-Mohy & Higham (default), 1 the cheapest (m, s) the
                              truncation bound certifies at phase error 1e-6, 2 the learned
                              MLP proposal, accepted only when the bound certifies it and
                              the result passes the unitarity check (else option 0)     */
+  FX_OPT_INJECT_STALL = 11 /* diagnostics of the failure path (walk generators): k >= 0 makes
+                             the k-th product launch of every run leave out the operand
+                             loads of one K step, so that its bounded waits run out and
+                             the run returns FX_ERR_TIMEOUT; -1 (default) off          */
 };
 
 /* What the last run did. */
@@ -122,6 +126,14 @@ int fx_set_option(fx_handle h, int key, double value);
 int fx_get_stats(fx_handle h, fx_stats* out);
 const char* fx_last_error(fx_handle h);
 
+/* Per product launch of the last run made with FX_OPT_PROFILE = 1 through the walk-generator
+ * pipeline: its stage (0 powers, 1 Pade numerator / denominator, 2 the solve's V^2, W^2, VW,
+ * 3 Cholesky, 4 triangular inverse, 5 triangular products, 6 squarings, 7 diagnostic unitarity
+ * products), its CUDA-event duration in ms and the int8 tensor ops it issued.  Writes
+ * min(cap, launches) records and the launch count to *count (0 when no such run was profiled).
+ * Diagnostics; no counterpart in the reference. */
+int fx_product_profile(fx_handle h, int32_t* tags, double* ms, double* ops, int32_t cap, int32_t* count);
+
 /* U = expm(A), both host buffers of n*n elements of the handle's dtype. */
 int fx_run_host(fx_handle h, const void* A, void* U);
 /* Same with device buffers; the work is ordered on `stream` (a cudaStream_t or NULL). */
@@ -145,16 +157,25 @@ int fx_product_f32(int form, int64_t M, int64_t N, int64_t K, const float* A, in
                    int64_t ldc, float gamma, float* D, int64_t ldd, void* stream);
 const char* fx_product_error(void);
 
+/* Measured dense tensor-core rate of the current GPU (diagnostics; no counterpart in the
+ * reference): one CTA per SM issues `iters` (1..2^20) x 2 tcgen05.mma of M = 128, N = 256, K = 32 bytes
+ * (kind 0: int8 x int8 -> int32; kind 1: BF16 x BF16 -> FP32) on operand tiles resident in
+ * shared memory, timed with CUDA events on `stream`.  *tops = tensor ops (2 M N K per
+ * instruction) per second / 1e12, *ms = the launch's duration.  Messages through
+ * fx_product_error. */
+int fx_tensor_peak(int kind, int64_t iters, double* tops, double* ms, void* stream);
+
 /* Allocation-free form of fx_product_f32 with FX_FORM_PLAIN (4 int8 slices, exact int32
  * accumulation on the tensor cores); no counterpart in the reference.  For callers that must
  * not allocate device memory once they are running (a pool that owns the device, an
  * allocator callback, a host that sizes all GPU memory at start-up): the slice scratch lives
  * in one fixed 16 MiB array of device memory inside the library, present on every GPU that
  * loads it until the process exits.  Needs 4 (M + N) K + 4 (M + N) + 512 bytes of it (M, N
- * multiples of 16, K of 64) and returns FX_ERR_VALUE beyond that.  The first call on a device
- * looks the array's device address up (make it before any stream capture).  All calls share
- * the array: calls that overlap on the GPU race; order them on one stream.  Messages through
- * fx_product_error. */
+ * multiples of 16, K of 64 and at most 32768) and returns FX_ERR_VALUE beyond that.  The first
+ * call on a device looks the array's device address up (make it before any stream capture).
+ * All calls share the array: calls that overlap on the GPU race; order them on one stream.
+ * Each call synchronises its stream before it returns (it reads the kernel's error word back).
+ * Messages through fx_product_error. */
 int fx_product_f32_noalloc(int64_t M, int64_t N, int64_t K, const float* A, int64_t lda,
                            const float* Bt, int64_t ldb, float alpha, float beta, const float* C,
                            int64_t ldc, float gamma, float* D, int64_t ldd, void* stream);
@@ -209,8 +230,11 @@ int fx_batch_details(fx_batch_handle b, double* features, int32_t* plain_m, int3
  * pointer; copied to the current device). */
 int fx_selector_set_weights(const float* w, int64_t n);
 /* Sampled comparison of the last run: how many non-plain walks were re-run with the plain
- * (m, s), and the largest infidelity between the two states.  Above 1e-10 every non-plain
- * walk was redone with the plain (m, s) (outcome -2). */
+ * (m, s) (the smallest ones, at most FX_BATCH_OPT_SAMPLE_WALKS, trimmed to a tenth of the
+ * batch's N^3 but never below one; 0 when no walk took a non-plain (m, s); -1 when the
+ * comparison was skipped because the batch holds a single walk), and the largest infidelity
+ * between the two states.  Above 1e-10 every non-plain walk was redone with the plain (m, s)
+ * (outcome -2). */
 int fx_batch_sample_check(fx_batch_handle b, int32_t* sampled, double* max_infidelity);
 /* The phase-2 schedule in use and, after an autotuned run, the candidates tried: ntuned rows
  * of (tile group, tile order, ms) in tuned (3 doubles each, at most 16 rows). */
