@@ -238,6 +238,74 @@ def accuracy_vs_eigh(H: np.ndarray, t: float, dU, psi_e0, psi_e0_plain, dev, see
     return out
 
 
+def bench_stress(args, dev) -> dict:
+    """The large-norm stress workload: dense symmetric weighted graph, N = 16384, weights uniform
+    in [0, 1) from a fixed seed (zero diagonal), H = weighted Laplacian D - W, t = 100, X = -1j H t
+    (FastCTQW/Operator.py:49-56).  Runs complex64 in the plain and mixed forms and complex128
+    (int8 slices on FP64 masters), each timed with CUDA events, with the unitarity residual
+    ||U_k^H U_k - I||_F / sqrt(N) after every squaring k (FX_OPT_DRIFT) and the final accuracy
+    against the FP64 eigendecomposition of the same generator (the complex64 input is itself a
+    rounding of X, so its oracle is the exact propagator of that rounded X)."""
+    import torch
+    from fastctqw_b200 import graphs
+    from fastctqw_b200._native import Engine
+    from oracle import expm_oracle as eo
+    n, t = args.stress_n, args.stress_t
+    Wt = graphs.weighted_complete(n, seed=args.seed, dtype=np.float64)
+    L = np.diag(Wt.sum(axis=1)) - Wt
+    del Wt
+    out = {"workload": f"dense U[0,1)-weighted complete graph N={n}, H = D - W, t={t}",
+           "oracle": "FP64 eigendecomposition of the (rounded) generator on the device"}
+    stream = torch.cuda.current_stream(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for dt, forms in ((np.complex64, ("plain", "mixed")), (np.complex128, ("plain",))):
+        X = np.asarray(-1j * (-1.0 * L) * t, dtype=dt)
+        lam, V = torch.linalg.eigh(torch.from_numpy(np.ascontiguousarray(X.imag, dtype=np.float64)).to(dev))
+        Vc = V.to(torch.complex128)
+        del V
+        Uref = (Vc * torch.exp(1j * lam)) @ Vc.T
+        del Vc, lam
+        torch.cuda.empty_cache()
+        dX = torch.from_numpy(X).to(dev)
+        del X
+        p0 = torch.zeros(n, dtype=dX.dtype, device=dev)
+        p0[0] = 1.0
+        dp = torch.empty_like(p0)
+        dU = torch.empty_like(dX)
+        eng = Engine(n, dt)
+        for form in forms:
+            eng.configure(form=form, drift=False)
+            eng.walk_device(dX, p0, dp, dU, stream)
+            torch.cuda.synchronize()
+            ev[0].record(stream)
+            eng.walk_device(dX, p0, dp, dU, stream)
+            ev[1].record(stream)
+            torch.cuda.synchronize()
+            st = eng.stats()
+            rec = {"ms": round(ev[0].elapsed_time(ev[1]), 2), "m": st["m"], "s": st["s"]}
+            U = dU.to(torch.complex128)
+            rec["u_rel_error"] = float(torch.linalg.matrix_norm(U - Uref) / torch.linalg.matrix_norm(Uref))
+            rec["infidelity_e0"] = eo.infidelity(dp.cpu().numpy(), Uref[:, 0].cpu().numpy())
+            for kind, v in (("uniform", graphs.uniform_state(n)), ("random", graphs.random_state(n, args.seed))):
+                pv = torch.from_numpy(v).to(dev).to(torch.complex128)
+                rec[f"infidelity_{kind}"] = eo.infidelity((U @ pv).cpu().numpy(), (Uref @ pv).cpu().numpy())
+            G = U.conj().T @ U
+            G.diagonal().sub_(1.0)
+            rec["unitarity_residual_final"] = float(torch.linalg.matrix_norm(G) / np.sqrt(n))
+            del U, G
+            torch.cuda.empty_cache()
+            eng.configure(drift=True)
+            eng.walk_device(dX, p0, dp, dU, stream)
+            torch.cuda.synchronize()
+            rec["drift_per_squaring"] = [float("%.4g" % x) for x in eng.unitarity_drift()]
+            eng.configure(drift=False)
+            out[f"{np.dtype(dt).name}_{form}"] = rec
+        eng.close()
+        del dX, dU, Uref
+        torch.cuda.empty_cache()
+    return out
+
+
 def batch_workload(count: int, seed: int, nmin: int, nmax: int):
     """The uneven batch: `count` walks, N ~ U{nmin..nmax}, alternating random d-regular
     (d ~ U{3..16}) and G(N, p) (p ~ U[0.05, 0.5]) adjacency graphs, t log-uniform in [0.5, 50],
@@ -476,6 +544,9 @@ def main():
     ap.add_argument("--no-batch-loop", action="store_true", help="skip the per-walk loop of the batch leg")
     ap.add_argument("--batch-only", action="store_true", help="run only the uneven-batch leg")
     ap.add_argument("--no-setup", action="store_true", help="skip the device set-up / time-curve leg")
+    ap.add_argument("--no-stress", action="store_true", help="skip the large-norm stress leg (N=16384, t=100)")
+    ap.add_argument("--stress-n", type=int, default=16384)
+    ap.add_argument("--stress-t", type=float, default=100.0)
     ap.add_argument("--no-autotune", action="store_true", help="batch leg: default schedule, no autotuning")
     ap.add_argument("--batch-shard", action=argparse.BooleanOptionalAction, default=True,
                     help="with N > 1 ranks: also run the uneven batch sharded over the ranks (default on)")
@@ -665,6 +736,12 @@ def main():
             eng.close()
         torch.cuda.empty_cache()
         batch = bench_batch_sharded(args, dev, rank, world)
+    stress = None
+    if rank == 0 and world == 1 and not args.no_stress:
+        if not eng._freed:
+            eng.close()
+        torch.cuda.empty_cache()
+        stress = bench_stress(args, dev)
     setup = None
     if rank == 0 and world == 1 and not args.no_setup:
         if not eng._freed:
@@ -687,7 +764,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "clocks": clk, "e2e": e2e, "gpu_launches": int(st["launches"]) * args.steps,
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "batch": batch,
-            "device_setup": setup,
+            "device_setup": setup, "stress": stress,
             "plain_selection": plain,
             "chosen_vs_plain_speedup": round(plain["ms"] / ms_per_step, 3) if plain else None,
             "algorithmic_tflops": round(st["flops"] / (ms_per_step * 1e-3) / 1e12, 2),

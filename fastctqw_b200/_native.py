@@ -22,7 +22,7 @@ CODE_DTYPE = {v: k for k, v in DTYPE_CODE.items()}
 FORM_PLAIN, FORM_MIXED, FORM_SIMT, FORM_FP64 = 0, 1, 2, 3
 FORMS = {"plain": FORM_PLAIN, "mixed": FORM_MIXED, "simt": FORM_SIMT, "fp64": FORM_FP64}
 (OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE,
- OPT_DEBUG_STAGE, OPT_PROFILE, OPT_SELECTOR, OPT_INJECT_STALL) = range(12)
+ OPT_DEBUG_STAGE, OPT_PROFILE, OPT_SELECTOR, OPT_INJECT_STALL, OPT_SQ_N4, OPT_SQ_N3, OPT_DRIFT) = range(15)
 SELECTORS = {"plain": 0, "certified": 1, "learned": 2}
 
 OK, ERR_TYPE, ERR_VALUE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_NONFINITE, ERR_SINGULAR, ERR_NODEV, ERR_FREED = range(10)
@@ -58,6 +58,10 @@ SIGNATURES = {
     "fx_get_n": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)],
     "fx_set_option": [ctypes.c_void_p, ctypes.c_int, ctypes.c_double],
     "fx_get_stats": [ctypes.c_void_p, ctypes.POINTER(FxStats)],
+    "fx_unitarity_drift": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int32,
+                           ctypes.POINTER(ctypes.c_int32)],
+    "fx_batch_drift": [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double), ctypes.c_int32,
+                       ctypes.POINTER(ctypes.c_int32)],
     "fx_product_profile": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double),
                            ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)],
     "fx_last_error": [ctypes.c_void_p],
@@ -222,7 +226,8 @@ class Engine:
                   force_s: int | None = None, ipe: bool | None = None,
                   timeout_ms: float | None = None, debug_stage: int | None = None,
                   profile: bool | None = None, selector: str | None = None,
-                  inject_stall: int | None = None) -> None:
+                  inject_stall: int | None = None, sq_n4: int | None = None, sq_n3: int | None = None,
+                  drift: bool | None = None) -> None:
         if form is not None:
             if form not in FORMS:
                 raise ValueError(f"form must be one of {sorted(FORMS)}")
@@ -249,6 +254,20 @@ class Engine:
             self.set_option(OPT_SELECTOR, SELECTORS[selector])
         if inject_stall is not None:
             self.set_option(OPT_INJECT_STALL, inject_stall)
+        if sq_n4 is not None:
+            self.set_option(OPT_SQ_N4, sq_n4)
+        if sq_n3 is not None:
+            self.set_option(OPT_SQ_N3, sq_n3)
+        if drift is not None:
+            self.set_option(OPT_DRIFT, int(bool(drift)))
+
+    def unitarity_drift(self) -> list:
+        """||U_k^H U_k - I||_F / sqrt(n) after every squaring k = 0..s of the last run made with
+        configure(drift=True) (walk generators)."""
+        cnt = ctypes.c_int32()
+        buf = (ctypes.c_double * 64)()
+        check(lib().fx_unitarity_drift(self._h, buf, 64, ctypes.byref(cnt)), self._h)
+        return list(buf[:min(cnt.value, 64)])
 
     def stats(self) -> dict:
         st = FxStats()

@@ -22,6 +22,7 @@ from ._native import check, lib
 
 OPT_GRAPH, OPT_TIMEOUT_MS, OPT_FORCE_M, OPT_SELECTOR, OPT_ANALYZE_ONLY, OPT_DIAG_SPLIT = 0, 1, 2, 3, 4, 5
 OPT_AUTOTUNE, OPT_TILE_GROUP, OPT_TILE_ORDER, OPT_SAMPLE_WALKS = 6, 7, 8, 9
+OPT_FORM, OPT_SQ_N4, OPT_SQ_N3, OPT_DRIFT = 10, 11, 12, 13
 OUTCOMES = {0: "plain", 1: "certified", 2: "learned", -1: "learned rejected by the bound",
             -2: "failed an a-posteriori check, redone with the plain (m, s)"}
 
@@ -49,7 +50,9 @@ class WalkBatch:
     """Owner of one ``fx_batch`` handle: device workspace for walks of sizes ``ns``."""
 
     def __init__(self, ns, dtype=np.complex64, graph: bool = True, selector: str = "plain",
-                 analyze_only: bool = False, diag_split: int = 3, autotune: bool = False) -> None:
+                 analyze_only: bool = False, diag_split: int = 3, autotune: bool = False,
+                 form: str = "plain", sq_n4: int | None = None, sq_n3: int | None = None,
+                 drift: bool = False) -> None:
         self.ns = [int(n) for n in ns]
         self.dtype = np.dtype(dtype)
         if self.dtype not in (np.dtype(np.complex64), np.dtype(np.complex128)):
@@ -68,6 +71,24 @@ class WalkBatch:
             self.set_option(OPT_DIAG_SPLIT, int(diag_split))
         if autotune:
             self.set_option(OPT_AUTOTUNE, 1)
+        if sq_n4 is not None:
+            self.set_option(OPT_SQ_N4, sq_n4)
+        if sq_n3 is not None:
+            self.set_option(OPT_SQ_N3, sq_n3)
+        if form != "plain":
+            if form != "mixed":
+                raise ValueError("batched walks take form 'plain' or 'mixed'")
+            self.set_option(OPT_FORM, _native.FORM_MIXED)
+        if drift:
+            self.set_option(OPT_DRIFT, 1)
+
+    def drift(self, w: int) -> list:
+        """||U_k^H U_k - I||_F / sqrt(n) after every squaring of walk w in the last run (needs
+        drift=True)."""
+        cnt = ctypes.c_int32()
+        buf = (ctypes.c_double * 64)()
+        _check(lib().fx_batch_drift(self._h, int(w), buf, 64, ctypes.byref(cnt)), self._h)
+        return list(buf[:min(cnt.value, 64)])
 
     def set_option(self, key: int, value: float) -> None:
         _check(lib().fx_batch_set_option(self._h, int(key), float(value)), self._h)

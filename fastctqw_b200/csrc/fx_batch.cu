@@ -253,6 +253,37 @@ __global__ void kb_rowsums(const double* P, const int* list, const BWalk* wk, do
     if (lane == 0) rs[b.row0 + i] = s;
   }
 }
+// Unitarity residual of a symmetric complex iterate U = I + E (diagnostics): with Eh = conj(E),
+// U^H U - I = 2 Re E + (Er Er + Ei Ei) + i (Er Ei - Ei Er).  D1 = Er Er + Ei Ei and D2 = Er Ei
+// are products over the walk's np x np block (zero padding); every chunk adds its share of
+// ||2 Er + D1||_F^2 + ||D2 - D2^T||_F^2 to out[w * kDriftMax + slot[w]].
+constexpr int kDriftMax = 64;
+__global__ void kb_drift(const double* const* Er, const double* D1, const double* D2, const RChunk* ch,
+                         const BWalk* wk, const int* slot, double* out) {
+  const RChunk q = ch[blockIdx.x];
+  const BWalk b = wk[q.w];
+  const double* er = Er[q.w];
+  const double* d1 = D1 + b.off;
+  const double* d2 = D2 + b.off;
+  const int64_t np = b.np, total = (int64_t)(q.r1 - q.r0) * np;
+  double acc = 0.0;
+  for (int64_t t = threadIdx.x; t < total; t += blockDim.x) {
+    const int64_t i = q.r0 + t / np, j = t - (t / np) * np;
+    const double v1 = 2.0 * er[i * np + j] + d1[i * np + j];
+    const double v2 = d2[i * np + j] - d2[j * np + i];
+    acc += v1 * v1 + v2 * v2;
+  }
+  __shared__ double sh[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x / 32] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x / 32); ++k) t += sh[k];
+    atomicAdd(out + (int64_t)q.w * kDriftMax + slot[q.w], t);
+  }
+}
 // One CTA per walk: out[w * stride + slot] = max (mode 0) or sum (mode 1) of v[row0 .. row0 + len).
 __global__ void kb_walk_vec_reduce(const double* v, const int* list, const BWalk* wk, int use_np, int mode,
                                    double* out, int stride, int slot) {
@@ -861,6 +892,33 @@ class BatchPipeline {
   // Diagnostics of the failure path: product launch k (k >= 0) of every run leaves the loads of
   // its first K step out, so that its bounded waits run out; runs are then replayed eagerly.
   void set_inject_stall(int k) { inject_ = k; }
+  // Precision form of the squarings: 0 plain (every squaring the exact complex square, 4 real
+  // products at 5 slices); 1 mixed (each squaring as the two real products (Er + Ei)(Er - Ei)
+  // and 2 Er Ei, 5 slices except the last n4 + n3 squarings: n4 at 4 slices, then n3 at 3).
+  void set_form(int form, int n4, int n3) {
+    if (form == form_ && n4 == sq_n4_ && n3 == sq_n3_) return;
+    form_ = form;
+    sq_n4_ = n4;
+    sq_n3_ = n3;
+    key2_.clear();
+  }
+  int form() const { return form_; }
+  // Diagnostics: the unitarity residual ||U_k^H U_k - I||_F / sqrt(n) of the iterate after every
+  // squaring k = 0..s (k = 0: the Pade result), from two extra 5-slice products per squaring.
+  void set_drift(bool d) {
+    if (d == drift_) return;
+    drift_ = d;
+    key2_.clear();
+  }
+  // Residuals of walk w in the last run with drift on (s + 1 values; empty otherwise).
+  std::vector<double> drift_curve(int w) const {
+    std::vector<double> out;
+    if (!drift_ || drift_host_.empty()) return out;
+    const int cnt = std::min(sel_s_[w], kDriftMax - 1) + 1;
+    for (int k = 0; k < cnt; ++k)
+      out.push_back(std::sqrt(std::max(0.0, drift_host_[(size_t)w * kDriftMax + k])) / std::sqrt((double)walks_[w].n));
+    return out;
+  }
   void details(int w, double* feat, int* pm, int* ps, int* cm, int* cs, int* outcome) const {
     for (int k = 0; k < 8; ++k) feat[k] = features_.empty() ? 0.0 : features_[8 * w + k];
     *pm = plain_m_.empty() ? 0 : plain_m_[w];
@@ -1075,6 +1133,10 @@ class BatchPipeline {
     FX_CUDA(cudaStreamSynchronize(s));
     check_err();
     prof_collect();
+    if (drift_ && drift_buf_.p) {
+      drift_host_.assign((size_t)W * kDriftMax, 0.0);
+      FX_CUDA(cudaMemcpy(drift_host_.data(), drift_buf_.p, sizeof(double) * drift_host_.size(), cudaMemcpyDeviceToHost));
+    }
   }
 
   // Phase 2: Pade, solve, squarings, outputs.  The recorded launch sequence (and its CUDA graph)
@@ -1278,6 +1340,10 @@ class BatchPipeline {
   bool use_graph_ = true, profile_ = false;
   int force_m_ = -1, force_s_ = -1;
   int inject_ = -1, prod_index_ = 0;   // stall injection (diagnostics), product launches so far
+  int form_ = 0, sq_n4_ = 0, sq_n3_ = 0;   // squaring form and slice schedule
+  bool drift_ = false;                     // per-squaring unitarity residual (diagnostics)
+  DevArena drift_buf_;
+  std::vector<double> drift_host_;
   int launches_ = 0, gemm_launches_ = 0;
   double flops_ = 0;
   cudaGraphExec_t graph1_ = nullptr, graph2_ = nullptr;
@@ -1444,6 +1510,8 @@ class BatchPipeline {
   }
   // Kernel attributes (dynamic shared memory) are set outside any stream capture.
   void warm_attributes() {
+    prepare_gemm_i8_grouped(3);
+    prepare_gemm_i8_grouped(4);
     prepare_gemm_i8_grouped(kS);
     prepare_potrf_inv_grouped();
   }
@@ -1605,10 +1673,10 @@ class BatchPipeline {
 
   // Real multiply-adds x 2 that the listed tiles compute (tile-level: 128 x BN x 64 per K step
   // and term); the int8 MMA operations issued are S(S+1)/2 times that.
-  static double tile_ops(const std::vector<GTile>& tiles, int nterms) {
+  static double tile_ops(const std::vector<GTile>& tiles, int nterms, int S = kS) {
     double steps = 0;
     for (const GTile& t : tiles) steps += t.kb1 - t.kb0;
-    return steps * 2.0 * 128.0 * i8_tile_bn(kS) * 64.0 * nterms;
+    return steps * 2.0 * 128.0 * i8_tile_bn(S) * 64.0 * nterms;
   }
   // Real product D_w = alpha_w A_w B_w + beta_w C_w + gamma_w I on np x np blocks of the listed
   // walks (arenas; B symmetric so Bt = B); c_arena < 0: no C.
@@ -1681,6 +1749,7 @@ class BatchPipeline {
     const int nsa = (int)a_sorted.size(), nsb = (int)b_sorted.size(), nt = (int)tiles.size();
     const double ops = tile_ops(tiles, 1);
     int64_t a_span = 0, b_span = 0;
+    const int64_t ka = widest(a_sorted), kb = widest(b_sorted);
     for (const GSlab& g : a_sorted) a_span = std::max<int64_t>(a_span, (int64_t)g.row0 + g.rows);
     for (const GSlab& g : b_sorted) b_span = std::max<int64_t>(b_span, (int64_t)g.row0 + g.rows);
     r.launches += same ? 2 : 3;
@@ -1697,11 +1766,11 @@ class BatchPipeline {
       outa.dg = split ? adiag() : nullptr;
       outb.dg = split ? bdiag() : nullptr;
       outa.ld = outb.ld = pitch_;
-      launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, a_span, outa, false, stream_);
+      launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, a_span, outa, false, stream_, ka);
       I8Term t{};
       for (int q = 0; q < kS; ++q) t.a[q] = outa.re[q];
       if (!same) {
-        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sb), nsb, b_span, outb, false, stream_);
+        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sb), nsb, b_span, outb, false, stream_, kb);
         for (int q = 0; q < kS; ++q) t.b[q] = outb.re[q];
       } else {
         for (int q = 0; q < kS; ++q) t.b[q] = outa.re[q];
@@ -1715,6 +1784,11 @@ class BatchPipeline {
     });
   }
 
+  static int64_t widest(const std::vector<GSlab>& v) {
+    int64_t k = 0;
+    for (const GSlab& g : v) k = std::max<int64_t>(k, g.K);
+    return k;
+  }
   // Row chunks of the listed walks' n x n (use_n) or np x np blocks, about kChunkElems each.
   std::vector<RChunk> row_chunks(const std::vector<int>& list, bool use_n) const {
     std::vector<RChunk> ch;
@@ -1896,11 +1970,21 @@ class BatchPipeline {
     project_pair(st, r, rank1, er, ei);
     int smax = 0;
     for (int w = 0; w < W; ++w) smax = std::max(smax, sel_s_[w]);
+    if (drift_) {
+      if (!drift_buf_.p) drift_buf_.alloc(sizeof(double) * (size_t)W * kDriftMax);
+      const size_t bytes = drift_buf_.bytes;
+      r.ops.push_back([=]() { FX_CUDA(cudaMemsetAsync(drift_buf_.p, 0, bytes, stream_)); });
+    }
+    tag_ = kTagSquare;
     for (int k = 0; k < smax; ++k) {
       std::vector<int> act;
       for (int w = 0; w < W; ++w)
         if (sel_s_[w] > k) act.push_back(w);
-      square(st, r, act, er, ei, tr, ti);
+      if (drift_) drift(st, r, act, er, ei, std::vector<int>(W, std::min(k, kDriftMax - 1)));
+      if (form_ == 1)
+        square2(st, r, act, er, ei, tr, ti, k);
+      else
+        square(st, r, act, er, ei, tr, ti);
       for (int w : act) {
         std::swap(er[w], tr[w]);
         std::swap(ei[w], ti[w]);
@@ -1909,6 +1993,11 @@ class BatchPipeline {
       for (int w : act)
         if (rank1_[w]) pj.push_back(w);
       project_pair(st, r, pj, er, ei);
+    }
+    if (drift_) {
+      std::vector<int> last(W);
+      for (int w = 0; w < W; ++w) last[w] = std::min(sel_s_[w], kDriftMax - 1);
+      drift(st, r, all, er, ei, last);
     }
 
     // ---- outputs: psi = e^mu (E psi0 + psi0 + cj (1^T psi0) 1) and U = e^mu (I + E + cj J)
@@ -2012,6 +2101,7 @@ class BatchPipeline {
       std::sort(sa.begin(), sa.end(), [](const GSlab& x, const GSlab& y) { return x.row0 < y.row0; });
       const size_t o_sa = st.put(sa), o_r = st.put(prr), o_i = st.put(pri), o_t = st.put(tiles);
       const int nsa = (int)sa.size(), nt = (int)tiles.size();
+      const int64_t kw = widest(sa);
       const double ops = tile_ops(tiles, 2);
       r.launches += 3;
       r.gemms += 2;
@@ -2024,7 +2114,7 @@ class BatchPipeline {
         }
         out.exp = aexp();
         out.ld = pitch_;
-        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, rows_, out, true, stream_);
+        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, rows_, out, true, stream_, kw);
         I8Term t[2];
         // real: Re Re + Im (-Im)
         for (int q = 0; q < kS; ++q) {
@@ -2052,6 +2142,175 @@ class BatchPipeline {
         prof_end(pi, ops * kS * (kS + 1) / 2, ops, kTagSquare);
       });
     }
+  }
+
+  // Slice count of squaring k (0-based) of walk w in the mixed form.
+  int sq_slices(int w, int k) const {
+    const int rem = sel_s_[w] - k;   // 1 for the last squaring
+    return rem <= sq_n3_ ? 3 : rem <= sq_n3_ + sq_n4_ ? 4 : kS;
+  }
+  // Upper-triangle tiles of the square problems (all of the same geometry per problem index).
+  std::vector<GTile> sym_tiles(const std::vector<GProblem>& pr, int bn) const {
+    std::vector<GTile> tiles;
+    for (int i = 0; i < (int)pr.size(); ++i) {
+      const int tm = (pr[i].M + 127) / 128, tn = (pr[i].N + bn - 1) / bn;
+      for_tiles(tm, tn, [&](int mb, int nb) {
+        if ((long long)nb * bn + bn - 1 >= (long long)mb * 128) tiles.push_back(GTile{i, mb, nb, 0, pr[i].K / 64, 0});
+      });
+    }
+    return tiles;
+  }
+  // Mixed-form squaring E <- 2E + E^2 of the listed walks, E = Er + i Ei symmetric with commuting
+  // planes (a function of the walk's real symmetric generator): Re = 2 Er + (Er + Ei)(Er - Ei),
+  // Im = 2 Ei + 2 Er Ei, two real products instead of four.  The products compute the upper
+  // triangle and mirror it.  In exact arithmetic Er and Ei commute; the commutator that the
+  // rounded iterates carry is of the size of the products' own rounding error and enters the
+  // result like it.  Walks are grouped by arena pair and by their slice count for this squaring.
+  void square2(Staging& st, Rec& r, const std::vector<int>& act, const std::vector<int>& er,
+               const std::vector<int>& ei, const std::vector<int>& tr, const std::vector<int>& ti, int k) {
+    for (int pa : {kA4, kT1}) {
+      for (int S : {5, 4, 3}) {
+        std::vector<int> l;
+        for (int w : act)
+          if (er[w] == pa && sq_slices(w, k) == S) l.push_back(w);
+        if (l.empty()) continue;
+        const int re = er[l[0]], im = ei[l[0]], ore = tr[l[0]], oim = ti[l[0]];
+        std::vector<GSlab> sa;
+        std::vector<GProblem> prr, pri;
+        for (int w : l) {
+          const BWalk& b = walks_[w];
+          sa.push_back(GSlab{A(re) + b.off, A(im) + b.off, b.np, b.np, b.np, (int)b.row0, kNoDiag});
+          GProblem p{};
+          p.a_row0 = p.b_row0 = (int)b.row0;
+          p.M = p.N = p.K = b.np;
+          p.sym = 1;
+          p.alpha = 1.0;
+          p.beta = 2.0;
+          p.ldc = p.ldd = b.np;
+          p.C = A(re) + b.off;
+          p.D = A(ore) + b.off;
+          prr.push_back(p);
+          p.alpha = 2.0;
+          p.C = A(im) + b.off;
+          p.D = A(oim) + b.off;
+          pri.push_back(p);
+        }
+        std::vector<GTile> tiles = sym_tiles(prr, i8_tile_bn(S));
+        order_tiles(tiles, prr);
+        std::sort(sa.begin(), sa.end(), [](const GSlab& x, const GSlab& y) { return x.row0 < y.row0; });
+        const size_t o_sa = st.put(sa), o_r = st.put(prr), o_i = st.put(pri), o_t = st.put(tiles);
+        const int nsa = (int)sa.size(), nt = (int)tiles.size();
+        const int64_t kw = widest(sa);
+        const double ops = tile_ops(tiles, 1, S);
+        r.launches += 3;
+        r.gemms += 2;
+        r.ops.push_back([=]() {
+          SqSlices out{};
+          for (int q = 0; q < S; ++q) {
+            out.p[0][q] = slice_plane(0, q);
+            out.p[1][q] = slice_plane(0, q) + (size_t)rows_ * pitch_;
+            out.p[2][q] = slice_plane(1, q);
+            out.p[3][q] = slice_plane(2, q);
+          }
+          out.exp_sd = aexp();
+          out.exp_ri = aexp() + rows_;
+          out.ld = pitch_;
+          launch_slice_rows_sumdiff_grouped(S, dev<GSlab>(o_sa), nsa, rows_, out, stream_, kw);
+          I8Term t{};
+          for (int q = 0; q < S; ++q) {
+            t.a[q] = out.p[0][q];
+            t.b[q] = out.p[1][q];
+          }
+          size_t pi = prof_begin();
+          launch_gemm_i8_grouped<double>(S, &t, 1, pitch_, rows_, rows_, aexp(), aexp(), dev<GProblem>(o_r),
+                                         dev<GTile>(o_t), nt, (int*)err_.p, timeout_ms_, stream_, nullptr, nullptr,
+                                         next_skip());
+          prof_end(pi, ops * S * (S + 1) / 2, ops, kTagSquare);
+          for (int q = 0; q < S; ++q) {
+            t.a[q] = out.p[2][q];
+            t.b[q] = out.p[3][q];
+          }
+          pi = prof_begin();
+          launch_gemm_i8_grouped<double>(S, &t, 1, pitch_, rows_, rows_, aexp() + rows_, aexp() + rows_,
+                                         dev<GProblem>(o_i), dev<GTile>(o_t), nt, (int*)err_.p, timeout_ms_, stream_,
+                                         nullptr, nullptr, next_skip());
+          prof_end(pi, ops * S * (S + 1) / 2, ops, kTagSquare);
+        });
+      }
+    }
+  }
+
+  // Diagnostics: unitarity residual of the listed walks' iterates (planes er / ei) into slot[w]
+  // of the drift buffer: D1 = Er Er + Ei Ei (symmetric) -> arena V, D2 = Er Ei (full) -> arena W,
+  // both with 5 slices, then kb_drift.  V and W are free during the squarings.
+  void drift(Staging& st, Rec& r, const std::vector<int>& list, const std::vector<int>& er,
+             const std::vector<int>& ei, const std::vector<int>& slot) {
+    if (list.empty()) return;
+    std::vector<GSlab> sa;
+    std::vector<GProblem> p1, p2;
+    std::vector<const double*> erp(count(), nullptr);
+    for (int w : list) {
+      const BWalk& b = walks_[w];
+      sa.push_back(GSlab{A(er[w]) + b.off, A(ei[w]) + b.off, b.np, b.np, b.np, (int)b.row0, kNoDiag});
+      erp[w] = A(er[w]) + b.off;
+      GProblem p{};
+      p.a_row0 = p.b_row0 = (int)b.row0;
+      p.M = p.N = p.K = b.np;
+      p.alpha = 1.0;
+      p.ldd = b.np;
+      p.sym = 1;
+      p.D = A(kV) + b.off;
+      p1.push_back(p);
+      p.sym = 0;
+      p.D = A(kW) + b.off;
+      p2.push_back(p);
+    }
+    const int bn = i8_tile_bn(kS);
+    std::vector<GTile> t1 = sym_tiles(p1, bn), t2;
+    for (int i = 0; i < (int)p2.size(); ++i) {
+      const int tm = (p2[i].M + 127) / 128, tn = (p2[i].N + bn - 1) / bn;
+      for_tiles(tm, tn, [&](int mb, int nb) { t2.push_back(GTile{i, mb, nb, 0, p2[i].K / 64, 0}); });
+    }
+    std::sort(sa.begin(), sa.end(), [](const GSlab& x, const GSlab& y) { return x.row0 < y.row0; });
+    const std::vector<RChunk> ch = row_chunks(list, false);
+    const size_t o_sa = st.put(sa), o_p1 = st.put(p1), o_p2 = st.put(p2), o_t1 = st.put(t1), o_t2 = st.put(t2);
+    const size_t o_ch = st.put(ch), o_er = st.put(erp), o_sl = st.put(slot);
+    const int nsa = (int)sa.size(), n1 = (int)t1.size(), n2 = (int)t2.size();
+    const int64_t kw = widest(sa);
+    const unsigned nch = (unsigned)ch.size();
+    const double ops1 = tile_ops(t1, 2), ops2 = tile_ops(t2, 1);
+    r.launches += 4;
+    r.gemms += 2;
+    r.ops.push_back([=]() {
+      I8Slices out{};
+      for (int q = 0; q < kS; ++q) {
+        out.re[q] = slice_plane(0, q);
+        out.im[q] = slice_plane(1, q);
+      }
+      out.exp = aexp();
+      out.ld = pitch_;
+      launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, rows_, out, false, stream_, kw);
+      I8Term t[2];
+      for (int q = 0; q < kS; ++q) {
+        t[0].a[q] = t[0].b[q] = out.re[q];
+        t[1].a[q] = t[1].b[q] = out.im[q];
+      }
+      size_t pi = prof_begin();
+      launch_gemm_i8_grouped<double>(kS, t, 2, pitch_, rows_, rows_, aexp(), aexp(), dev<GProblem>(o_p1),
+                                     dev<GTile>(o_t1), n1, (int*)err_.p, timeout_ms_, stream_);
+      prof_end(pi, ops1 * kS * (kS + 1) / 2, ops1, kTagDrift);
+      for (int q = 0; q < kS; ++q) {
+        t[0].a[q] = out.re[q];
+        t[0].b[q] = out.im[q];
+      }
+      pi = prof_begin();
+      launch_gemm_i8_grouped<double>(kS, t, 1, pitch_, rows_, rows_, aexp(), aexp(), dev<GProblem>(o_p2),
+                                     dev<GTile>(o_t2), n2, (int*)err_.p, timeout_ms_, stream_);
+      prof_end(pi, ops2 * kS * (kS + 1) / 2, ops2, kTagDrift);
+      kb_drift<<<nch, 256, 0, stream_>>>(dev<const double*>(o_er), A(kV), A(kW), dev<RChunk>(o_ch),
+                                         (const BWalk*)d_walks_.p, dev<int>(o_sl), (double*)drift_buf_.p);
+      FX_LAUNCH_CHECK();
+    });
   }
 
   // D_re / D_im = (P_re, P_im) B^T per walk (two problems per walk, A rows side by side);
@@ -2246,9 +2505,12 @@ void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, voi
   p->set_profile(o.profile);
   p->set_timeout(o.timeout_ms);
   p->set_inject_stall(o.inject_stall);
+  p->set_form(o.form == FX_FORM_MIXED ? 1 : 0, o.sq_n4, o.sq_n3);
+  p->set_drift(o.drift);
   p->run(x, p0, p1, u, s);
 }
 const std::vector<ProdRecord>& batch_pipeline_products(const BatchPipeline* p) { return p->prod_list(); }
+std::vector<double> batch_pipeline_drift(const BatchPipeline* p) { return p->drift_curve(0); }
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st) {
   p->walk_stats(0, st);
   double f[8];
@@ -2275,6 +2537,7 @@ struct fx_batch {
   double ms = 0;
   std::vector<void*> h_in;   // device staging of host runs (X, psi0, psi per walk)
   fx::HostStage stage;       // page-locked chunks for the copies of the host matrices
+  int sq_n4 = fx::kMixedN4, sq_n3 = fx::kMixedN3;   // mixed-form slice schedule
   std::string last_error;
 };
 
@@ -2406,6 +2669,19 @@ int fx_batch_set_option(fx_batch_handle b, int key, double value) {
         return bfail(b, fx::Error{FX_ERR_VALUE, "diagonal split must be a mask of 1 and 2"});
       b->p->set_diag_split((int)value);
       return FX_OK;
+    case FX_BATCH_OPT_FORM:
+      if (value != FX_FORM_PLAIN && value != FX_FORM_MIXED)
+        return bfail(b, fx::Error{FX_ERR_VALUE, "batch form must be FX_FORM_PLAIN or FX_FORM_MIXED"});
+      b->p->set_form(value == FX_FORM_MIXED ? 1 : 0, b->sq_n4, b->sq_n3);
+      return FX_OK;
+    case FX_BATCH_OPT_SQ_N4:
+    case FX_BATCH_OPT_SQ_N3: {
+      if (value < 0 || value > 64) return bfail(b, fx::Error{FX_ERR_VALUE, "squaring counts must be 0..64"});
+      (key == FX_BATCH_OPT_SQ_N4 ? b->sq_n4 : b->sq_n3) = (int)value;
+      b->p->set_form(b->p->form(), b->sq_n4, b->sq_n3);
+      return FX_OK;
+    }
+    case FX_BATCH_OPT_DRIFT: b->p->set_drift(value != 0.0); return FX_OK;
   }
   return bfail(b, fx::Error{FX_ERR_VALUE, "unknown batch option"});
 }
@@ -2452,6 +2728,15 @@ int fx_batch_walk_host(fx_batch_handle b, const void* const* X, const void* cons
     }
     FX_CUDA(cudaStreamSynchronize(b->stream));
   });
+}
+
+int fx_batch_drift(fx_batch_handle b, int64_t w, double* out, int32_t cap, int32_t* count) {
+  if (!b || !count || (cap > 0 && !out)) return bfail(b, fx::Error{FX_ERR_VALUE, "null argument"});
+  if (w < 0 || w >= (int64_t)b->ns.size()) return bfail(b, fx::Error{FX_ERR_VALUE, "walk index out of range"});
+  const std::vector<double> v = b->p->drift_curve((int)w);
+  for (int32_t i = 0; i < cap && i < (int32_t)v.size(); ++i) out[i] = v[i];
+  *count = (int32_t)v.size();
+  return FX_OK;
 }
 
 int fx_batch_selection(fx_batch_handle b, int32_t* m, int32_t* s) {

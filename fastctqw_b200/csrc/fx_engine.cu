@@ -89,6 +89,8 @@ struct RunOpts {
   int profile;       // 1: time every int8 product launch with CUDA events
   int selector;      // (m, s) selection of the grouped path: 0 plain, 1 certified, 2 learned
   int inject_stall;  // diagnostics of the grouped path: product launch that skips a K step (-1 off)
+  int sq_n4, sq_n3;  // mixed form of the grouped path: squarings at 4 and at 3 slices
+  int drift;         // diagnostics of the grouped path: unitarity residual after every squaring
 };
 
 // Planar complex matrix view over owned storage; a missing plane is identically zero.
@@ -1042,7 +1044,7 @@ struct fx_engine {
   fx::BatchPipeline* grouped = nullptr;   // grouped pipeline for walk generators (lazy)
   void* check_buf = nullptr;              // input statistics of the routing check
   fx::HostStage stage;                    // page-locked chunks for copies of host buffers
-  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0, 0, -1};
+  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0, 0, -1, fx::kMixedN4, fx::kMixedN3, 0};
   fx_stats stats{};
   std::string last_error;
 };
@@ -1103,8 +1105,8 @@ void ensure_pipeline(fx_handle h) {
 // (general complex or real inputs, other forms or options) runs the pipeline of this file.
 bool grouped_eligible(fx_handle h) {
   const fx::RunOpts& o = h->opts;
-  return (h->dtype == FX_C64 || h->dtype == FX_C128) && o.form == FX_FORM_PLAIN && o.shift == 2 &&
-         o.structure == 1 && o.ipe == 1 && o.debug_stage == 0 && o.force_m < 0 && o.force_s < 0;
+  return (h->dtype == FX_C64 || h->dtype == FX_C128) && (o.form == FX_FORM_PLAIN || o.form == FX_FORM_MIXED) &&
+         o.shift == 2 && o.structure == 1 && o.ipe == 1 && o.debug_stage == 0 && o.force_m < 0 && o.force_s < 0;
 }
 bool input_is_walk_generator(fx_handle h, const void* dA, cudaStream_t s) {
   const int64_t n = h->n;
@@ -1131,6 +1133,10 @@ void run_device(fx_handle h, const void* dA, void* dU, const void* dpsi0, void* 
     po.timeout_ms = h->opts.timeout_ms;
     po.selector = h->opts.selector;
     po.inject_stall = h->opts.inject_stall;
+    po.form = h->opts.form;
+    po.sq_n4 = h->opts.sq_n4;
+    po.sq_n3 = h->opts.sq_n3;
+    po.drift = h->opts.drift != 0;
     fx::batch_pipeline_run(h->grouped, dA, dpsi0, dpsi, dU, po, s);
     FX_CUDA(cudaEventRecord(h->ev1, s));
     FX_CUDA(cudaEventSynchronize(h->ev1));
@@ -1138,7 +1144,7 @@ void run_device(fx_handle h, const void* dA, void* dU, const void* dpsi0, void* 
     FX_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     h->stats = fx_stats{};
     fx::batch_pipeline_stats(h->grouped, &h->stats);
-    h->stats.form = FX_FORM_PLAIN;
+    h->stats.form = h->opts.form;
     h->stats.ms_total = ms;
     return;
   }
@@ -1197,7 +1203,8 @@ int fx_create(size_t n, int dtype, fx_handle* out) {
     FX_CUDA(cudaEventCreate(&h->ev0));
     FX_CUDA(cudaEventCreate(&h->ev1));
     if (dtype == FX_C128 || dtype == FX_F64) h->opts.form = FX_FORM_FP64;
-    if (n > 0) ensure_pipeline(h);
+    // the general pipeline's workspace is allocated at the first run that needs it: walk
+    // generators run the grouped pipeline instead
   });
   if (rc != FX_OK) {
     std::string msg = h->last_error;
@@ -1286,6 +1293,12 @@ int fx_set_option(fx_handle h, int key, double value) {
       if (v < -1) return fail(h, fx::Error{FX_ERR_VALUE, "stall injection takes a launch index >= 0, or -1"});
       h->opts.inject_stall = v;
       return FX_OK;
+    case FX_OPT_SQ_N4:
+    case FX_OPT_SQ_N3:
+      if (v < 0 || v > 64) return fail(h, fx::Error{FX_ERR_VALUE, "squaring counts must be 0..64"});
+      (key == FX_OPT_SQ_N4 ? h->opts.sq_n4 : h->opts.sq_n3) = v;
+      return FX_OK;
+    case FX_OPT_DRIFT: h->opts.drift = v != 0; return FX_OK;
   }
   return fail(h, fx::Error{FX_ERR_VALUE, "unknown option"});
 }
@@ -1300,6 +1313,16 @@ int fx_product_profile(fx_handle h, int32_t* tags, double* ms, double* ops, int3
     ms[i] = v[i].ms;
     ops[i] = v[i].ops;
   }
+  *count = (int32_t)v.size();
+  return FX_OK;
+}
+
+int fx_unitarity_drift(fx_handle h, double* out, int32_t cap, int32_t* count) {
+  if (!h || !count || (cap > 0 && !out)) return fail(h, fx::Error{FX_ERR_VALUE, "null argument"});
+  *count = 0;
+  if (!h->grouped) return FX_OK;
+  const std::vector<double> v = fx::batch_pipeline_drift(h->grouped);
+  for (int32_t i = 0; i < cap && i < (int32_t)v.size(); ++i) out[i] = v[i];
   *count = (int32_t)v.size();
   return FX_OK;
 }

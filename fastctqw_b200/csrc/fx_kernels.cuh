@@ -246,11 +246,17 @@ struct PipeOpts {
   int selector = 0;          // 0 Al-Mohy & Higham, 1 certified bound, 2 learned
   int inject_stall = -1;     // diagnostics: k >= 0 makes product launch k of every run skip the
                              // operand loads of its first K step, so that the bounded waits run out
+  int form = FX_FORM_PLAIN;  // FX_FORM_MIXED: two-product squarings with the slice schedule below
+  int sq_n4 = 0, sq_n3 = 0;  // mixed form: the last sq_n3 squarings at 3 slices, the sq_n4 before at 4
+  bool drift = false;        // diagnostics: unitarity residual after every squaring
 };
+// Default slice schedule of the mixed form (see fx_batch.cu, BatchPipeline::sq_slices).
+constexpr int kMixedN4 = 4, kMixedN3 = 1;
 void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU,
                         const PipeOpts& o, cudaStream_t s);
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st);
 const std::vector<ProdRecord>& batch_pipeline_products(const BatchPipeline* p);
+std::vector<double> batch_pipeline_drift(const BatchPipeline* p);
 // Host <-> device copies of large host buffers (fx_hostcopy.cu): a buffer the driver knows as
 // page-locked is copied by DMA directly; any other goes through two page-locked chunk buffers,
 // the host side of a chunk (split over threads) overlapping the DMA of the previous one.
@@ -293,9 +299,22 @@ struct GSlab {
                         // which is left out of the slices and written to I8Slices::dg
 };
 constexpr int kNoDiag = -(1 << 30);
+// kmax: the widest slab (K) of the launch, when known (> 0): rows whose planes fit the shared
+// memory are then sliced by the shared-memory kernel (one HBM read per row).
 template <typename TI>
 void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, I8Slices out,
-                               bool want_neg_im, cudaStream_t s);
+                               bool want_neg_im, cudaStream_t s, int64_t kmax = 0, bool two_planes = true);
+// Slices of the two-product squaring (launch_slice_rows_sumdiff_grouped): p[0] = Er + Ei,
+// p[1] = Er - Ei (row exponents exp_sd), p[2] = Er, p[3] = Ei (row exponents exp_ri), S digits
+// each, stacked rows of pitch ld.
+struct SqSlices {
+  int8_t* p[4][5];
+  int* exp_sd;
+  int* exp_ri;
+  int64_t ld;
+};
+void launch_slice_rows_sumdiff_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, SqSlices out,
+                                       cudaStream_t s, int64_t kmax = 0);
 // In place A <- (A + A^T) / 2 of an n x n plane (exact symmetry of a result known to be
 // symmetric in exact arithmetic).
 template <typename T>

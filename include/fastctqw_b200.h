@@ -58,8 +58,13 @@ enum fx_status {
 enum fx_form {
   FX_FORM_PLAIN = 0,  /* int8 tensor-core products of 5 (FP64 masters) or 4 (FP32)
                          Ozaki slices, exact int32 accumulation; default for complex64 */
-  FX_FORM_MIXED = 1,  /* BF16 hi+lo split, 3 products (hi*hi, hi*lo, lo*hi), FP32
-                         accumulate, FP32 masters (complex64 / float32 handles)       */
+  FX_FORM_MIXED = 1,  /* reduced-precision products (complex64 / float32 handles).  Walk
+                         generators X = i*(real symmetric): int8 slices on FP64 masters,
+                         5 slices for the Pade and solve products, each squaring as the
+                         two real products (Re+Im)(Re-Im) and 2 Re Im, with 4 and then 3
+                         slices for the last squarings (FX_OPT_SQ_N4 / FX_OPT_SQ_N3).
+                         Other inputs: BF16 hi+lo split, 3 products (hi*hi, hi*lo,
+                         lo*hi), FP32 accumulate, FP32 masters                        */
   FX_FORM_SIMT = 2,   /* CUDA-core FP32 FMA products, FP32 masters (checker)          */
   FX_FORM_FP64 = 3    /* CUDA-core FP64 products (default for complex128 / float64)   */
 };
@@ -83,10 +88,18 @@ enum fx_option {
                              truncation bound certifies at phase error 1e-6, 2 the learned
                              MLP proposal, accepted only when the bound certifies it and
                              the result passes the unitarity check (else option 0)     */
-  FX_OPT_INJECT_STALL = 11 /* diagnostics of the failure path (walk generators): k >= 0 makes
+  FX_OPT_INJECT_STALL = 11, /* diagnostics of the failure path (walk generators): k >= 0 makes
                              the k-th product launch of every run leave out the operand
                              loads of one K step, so that its bounded waits run out and
                              the run returns FX_ERR_TIMEOUT; -1 (default) off          */
+  FX_OPT_SQ_N4 = 12,      /* mixed form, walk generators: how many squarings before the
+                             3-slice ones run at 4 slices (default 4)                  */
+  FX_OPT_SQ_N3 = 13,      /* mixed form, walk generators: how many of the last squarings run
+                             at 3 slices (default 1)                                   */
+  FX_OPT_DRIFT = 14       /* diagnostics (walk generators): 1 records the unitarity residual
+                             ||U_k^H U_k - I||_F / sqrt(n) after every squaring k = 0..s
+                             (fx_unitarity_drift), at the cost of two extra products per
+                             squaring                                                  */
 };
 
 /* What the last run did. */
@@ -133,6 +146,14 @@ const char* fx_last_error(fx_handle h);
  * min(cap, launches) records and the launch count to *count (0 when no such run was profiled).
  * Diagnostics; no counterpart in the reference. */
 int fx_product_profile(fx_handle h, int32_t* tags, double* ms, double* ops, int32_t cap, int32_t* count);
+
+/* The unitarity residuals of the last run made with FX_OPT_DRIFT = 1: out[k] =
+ * ||U_k^H U_k - I||_F / sqrt(n) for the iterate U_k = I + E_k after k squarings (k = 0: the
+ * Pade approximant of the scaled generator; k = s: the propagator before the shifts, which are
+ * unitary), computed from exact-in-int32 products on 5 slices.  Writes min(cap, s + 1) values
+ * and s + 1 to *count (0 when no such run was made).  Diagnostics; no counterpart in the
+ * reference. */
+int fx_unitarity_drift(fx_handle h, double* out, int32_t cap, int32_t* count);
 
 /* U = expm(A), both host buffers of n*n elements of the handle's dtype. */
 int fx_run_host(fx_handle h, const void* A, void* U);
@@ -202,8 +223,12 @@ enum fx_batch_option {
                                  /* post-selection products on this batch and keep the fastest */
   FX_BATCH_OPT_TILE_GROUP = 7,   /* schedule: tiles in G x G blocks, G = 4, 8 (default) or 16    */
   FX_BATCH_OPT_TILE_ORDER = 8,   /* schedule: 0 (default) longest K ranges first, 1 by problem   */
-  FX_BATCH_OPT_SAMPLE_WALKS = 9  /* walks (default 2, 0..64) of a non-plain selection re-run with */
+  FX_BATCH_OPT_SAMPLE_WALKS = 9, /* walks (default 2, 0..64) of a non-plain selection re-run with */
                                  /* the plain (m, s) and compared after every run               */
+  FX_BATCH_OPT_FORM = 10,        /* FX_FORM_PLAIN (default) or FX_FORM_MIXED (as FX_OPT_FORM)     */
+  FX_BATCH_OPT_SQ_N4 = 11,       /* mixed form: squarings at 4 slices (as FX_OPT_SQ_N4)          */
+  FX_BATCH_OPT_SQ_N3 = 12,       /* mixed form: last squarings at 3 slices (as FX_OPT_SQ_N3)     */
+  FX_BATCH_OPT_DRIFT = 13        /* diagnostics: per-squaring unitarity residual (as FX_OPT_DRIFT) */
 };
 /* count walks of sizes n[0..count); dtype FX_C64 or FX_C128 (of X, psi0 and psi). */
 int fx_batch_create(size_t count, const int64_t* n, int dtype, fx_batch_handle* out);
@@ -216,6 +241,9 @@ int fx_batch_walk_device(fx_batch_handle b, const void* const* dX, const void* c
 /* The same with host buffers (copies in and out inside the call). */
 int fx_batch_walk_host(fx_batch_handle b, const void* const* X, const void* const* psi0,
                        void* const* psi);
+/* Unitarity residuals of walk w in the last run made with FX_BATCH_OPT_DRIFT = 1 (as
+ * fx_unitarity_drift). */
+int fx_batch_drift(fx_batch_handle b, int64_t w, double* out, int32_t cap, int32_t* count);
 /* (m, s) chosen for every walk by the last run (arrays of `count`). */
 int fx_batch_selection(fx_batch_handle b, int32_t* m, int32_t* s);
 /* Device time (ms, CUDA events), algorithmic flops and kernel launches of the last run. */

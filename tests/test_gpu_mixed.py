@@ -1,0 +1,108 @@
+"""The mixed (reduced-precision) form of the walk-generator pipeline (needs a GPU).
+
+The mixed form runs every squaring as two real products, Re = 2 Er + (Er + Ei)(Er - Ei) and
+Im = 2 Ei + 2 Er Ei (the planes of the iterate commute), and cuts the operands of the last
+squarings into fewer int8 slices (4, then 3): their errors are not amplified by later squarings.
+The Pade and solve products keep 5 slices.  Checked here against the FP64 eigendecomposition
+propagator, with the tolerances of the parity tests (complex64 U within 1e-5 relative, states at
+infidelity <= 1e-10); the per-squaring unitarity residual (FX_OPT_DRIFT) against one computed
+directly from the returned U; and the reduced-slice products themselves, by running every
+squaring at 4 or at 3 slices and comparing the error with the slices' resolution.
+"""
+import numpy as np
+import pytest
+
+from oracle import expm_oracle as eo
+
+pytestmark = pytest.mark.gpu
+
+C64_REL = 1e-5
+INFID = 1e-10
+
+
+def _dense(n, t=4.5, seed=11):
+    from fastctqw_b200 import graphs
+    A = graphs.erdos_renyi(n, 0.5, seed=seed, dtype=np.float32)
+    L = np.diag(A.sum(axis=1)) - A
+    X = np.asarray(-1j * (-1.0 * L) * t, dtype=np.complex64)
+    lam, V = np.linalg.eigh(X.imag.astype(np.float64))
+    return X, (V * np.exp(1j * lam)) @ V.T
+
+
+def _walk(X, form, **kw):
+    import torch
+    from fastctqw_b200._native import Engine
+    n = X.shape[0]
+    dev = torch.device("cuda", 0)
+    dX = torch.from_numpy(X).to(dev)
+    p0 = torch.zeros(n, dtype=torch.complex64, device=dev)
+    p0[0] = 1.0
+    dp = torch.empty_like(p0)
+    dU = torch.empty_like(dX)
+    e = Engine(n, np.complex64)
+    e.configure(form=form, **kw)
+    e.walk_device(dX, p0, dp, dU)
+    torch.cuda.synchronize()
+    out = (dU.cpu().numpy(), dp.cpu().numpy(), e.stats(), e.unitarity_drift())
+    e.close()
+    return out
+
+
+@pytest.mark.parametrize("n", [1024, 2048])
+def test_mixed_form_meets_the_accuracy_bar(n):
+    from fastctqw_b200 import graphs
+    X, Uref = _dense(n)
+    U, psi, st, _ = _walk(X, "mixed")
+    assert st["form"] == 1 and st["structured"] == 1
+    assert eo.rel_error(U, Uref) <= C64_REL, eo.rel_error(U, Uref)
+    assert eo.infidelity(psi, Uref[:, 0]) <= INFID
+    for p0 in (graphs.uniform_state(n), graphs.random_state(n, 3)):
+        p = p0.astype(np.complex128)
+        assert eo.infidelity(U.astype(np.complex128) @ p, Uref @ p) <= INFID
+
+
+def test_drift_curve_matches_the_returned_propagator():
+    """The residual after the last squaring equals ||U^H U - I||_F / sqrt(n) of the returned U up
+    to its complex64 rounding; one value per squaring plus the Pade result."""
+    n = 1024
+    X, _ = _dense(n)
+    for form in ("plain", "mixed"):
+        U, _, st, drift = _walk(X, form, drift=True)
+        assert len(drift) == st["s"] + 1, (form, drift, st["s"])
+        assert all(np.isfinite(drift)) and max(drift) < 1e-4, drift
+        U128 = U.astype(np.complex128)
+        direct = eo.unitarity_residual(U128)
+        # complex64 storage adds ~1e-7 per entry: compare above that floor
+        assert abs(drift[-1] - direct) <= 0.5 * direct + 3e-7, (form, drift[-1], direct)
+
+
+@pytest.mark.parametrize("slices", [4, 3])
+def test_reduced_slice_squarings_have_the_slices_resolution(slices):
+    """Every squaring at 4 (or 3) slices: the products are right (not garbage) and their error is
+    of the size the slices resolve, far above the 5-slice error."""
+    n = 1024
+    X, Uref = _dense(n, t=2.0)
+    U5, _, st, _ = _walk(X, "mixed", sq_n4=0, sq_n3=0)
+    kw = {"sq_n4": 64, "sq_n3": 0} if slices == 4 else {"sq_n4": 0, "sq_n3": 64}
+    Ur, _, _, _ = _walk(X, "mixed", **kw)
+    e5, er = eo.rel_error(U5, Uref), eo.rel_error(Ur, Uref)
+    assert e5 <= C64_REL
+    bound = {4: 1e-5, 3: 1e-2}[slices]
+    assert er <= bound, (slices, er, st["s"])
+
+
+def test_mixed_batch_matches_plain_batch():
+    from fastctqw_b200 import graphs
+    from fastctqw_b200.batch import WalkBatch
+    specs = graphs.uneven_batch(12, seed=9, nmin=96, nmax=700)
+    Xs = [np.asarray(1j * sp.adjacency(np.float32) * np.float32(sp.t), dtype=np.complex64) for sp in specs]
+    P0 = [graphs.random_state(X.shape[0], k) for k, X in enumerate(Xs)]
+    ns = [X.shape[0] for X in Xs]
+    with WalkBatch(ns) as bp, WalkBatch(ns, form="mixed") as bm:
+        a = bp.run(Xs, P0)
+        b = bm.run(Xs, P0)
+    for k, X in enumerate(Xs):
+        lam, V = np.linalg.eigh(X.imag.astype(np.float64))
+        ref = V @ (np.exp(1j * lam) * (V.T @ P0[k].astype(np.complex128)))
+        assert eo.infidelity(b[k], ref) <= INFID, (k, ns[k])
+        assert eo.infidelity(a[k], ref) <= INFID, (k, ns[k])
