@@ -23,7 +23,7 @@ FORM_PLAIN, FORM_MIXED, FORM_SIMT, FORM_FP64 = 0, 1, 2, 3
 FORMS = {"plain": FORM_PLAIN, "mixed": FORM_MIXED, "simt": FORM_SIMT, "fp64": FORM_FP64}
 (OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE,
  OPT_DEBUG_STAGE, OPT_PROFILE, OPT_SELECTOR, OPT_INJECT_STALL, OPT_SQ_N4, OPT_SQ_N3, OPT_DRIFT) = range(15)
-SELECTORS = {"plain": 0, "certified": 1, "learned": 2}
+SELECTORS = {"plain": 0, "certified": 1, "learned": 2, "estimated": 3}
 
 OK, ERR_TYPE, ERR_VALUE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_NONFINITE, ERR_SINGULAR, ERR_NODEV, ERR_FREED = range(10)
 
@@ -58,6 +58,9 @@ SIGNATURES = {
     "fx_get_n": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)],
     "fx_set_option": [ctypes.c_void_p, ctypes.c_int, ctypes.c_double],
     "fx_get_stats": [ctypes.c_void_p, ctypes.POINTER(FxStats)],
+    "fx_spectral_radius": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+    "fx_batch_force_selection": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
+    "fx_batch_spectral": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
     "fx_unitarity_drift": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int32,
                            ctypes.POINTER(ctypes.c_int32)],
     "fx_batch_drift": [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double), ctypes.c_int32,
@@ -260,6 +263,13 @@ class Engine:
             self.set_option(OPT_SQ_N3, sq_n3)
         if drift is not None:
             self.set_option(OPT_DRIFT, int(bool(drift)))
+
+    def spectral_radius(self) -> dict:
+        """Lanczos estimate and rigorous upper bound of the shifted generator's spectral radius
+        in the last walk-generator run."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        check(lib().fx_spectral_radius(self._h, ctypes.byref(a), ctypes.byref(b)), self._h)
+        return {"lanczos": a.value, "upper_bound": b.value}
 
     def unitarity_drift(self) -> list:
         """||U_k^H U_k - I||_F / sqrt(n) after every squaring k = 0..s of the last run made with

@@ -82,6 +82,25 @@ class WalkBatch:
         if drift:
             self.set_option(OPT_DRIFT, 1)
 
+    def force_selection(self, m=None, s=None) -> None:
+        """Per-walk forced (m, s) for the next runs (m[w] <= 0: the walk's own selection); no
+        arguments clears."""
+        if m is None:
+            _check(lib().fx_batch_force_selection(self._h, None, None), self._h)
+            return
+        n = len(self.ns)
+        mm = (ctypes.c_int32 * n)(*[int(x) for x in m])
+        ss = (ctypes.c_int32 * n)(*[int(x) for x in s])
+        _check(lib().fx_batch_force_selection(self._h, mm, ss), self._h)
+
+    def spectral(self) -> dict:
+        """Per walk: Lanczos spectral-radius estimate and rigorous bound of the last run."""
+        n = len(self.ns)
+        a = (ctypes.c_double * n)()
+        b = (ctypes.c_double * n)()
+        _check(lib().fx_batch_spectral(self._h, a, b), self._h)
+        return {"lanczos": np.array(a[:]), "upper_bound": np.array(b[:])}
+
     def drift(self, w: int) -> list:
         """||U_k^H U_k - I||_F / sqrt(n) after every squaring of walk w in the last run (needs
         drift=True)."""

@@ -535,6 +535,67 @@ __global__ void kb_est_matvec(const double* M, const RChunk* ch, const BWalk* wk
     }
   }
 }
+// ---- Lanczos estimate of the spectral radius of every walk's real symmetric generator B
+// (the imaginary plane of the shifted Y): two independent runs of kLanSteps steps from
+// pseudo-random sign vectors, sharing kb_est_matvec (X0, X1 -> T0, T1), without
+// reorthogonalisation (the extreme Ritz values, all this needs, stay inside the spectrum).
+// Per walk and run, lan holds (alpha_j, beta_j) for j < kLanSteps; Y0 / Y1 keep v_{j-1}.
+constexpr int kLanSteps = 30;
+__device__ double block_reduce(double v, double* sh, bool take_max);
+__device__ __forceinline__ double probe_sign_d2(int64_t i) {
+  const uint32_t h = (uint32_t)((uint64_t)(i + 977) * 0x85EBCA6Bull) ^ 0x27D4EB2Fu;
+  return ((h * 0xC2B2AE35u) >> 31) & 1 ? -1.0 : 1.0;
+}
+__global__ void kb_lan_init(const int* list, const BWalk* wk, double* scr, double* est) {
+  const int w = list[blockIdx.x];
+  const BWalk b = wk[w];
+  double* X0 = est_vec(scr, b, kEX0);
+  double* X1 = est_vec(scr, b, kEX1);
+  double* Y0 = est_vec(scr, b, kEY0);
+  double* Y1 = est_vec(scr, b, kEY1);
+  const double inv = 1.0 / sqrt((double)b.n);
+  for (int i = threadIdx.x; i < b.np; i += blockDim.x) {
+    X0[i] = i < b.n ? probe_sign_d(i) * inv : 0.0;
+    X1[i] = i < b.n ? probe_sign_d2(i) * inv : 0.0;
+    Y0[i] = 0.0;
+    Y1[i] = 0.0;
+  }
+  if (threadIdx.x == 0) est[4 * w + 2] = 0.0;   // kb_est_matvec skips walks marked done
+}
+// After T_r = B X_r: alpha = T.v, w = T - alpha v - beta_prev v_prev, beta = |w|, v_prev <- v,
+// v <- w / beta (v <- 0 once the Krylov space is exhausted).
+__global__ void kb_lan_step(const int* list, const BWalk* wk, double* scr, double* lan, int j) {
+  const int w = list[blockIdx.x];
+  const BWalk b = wk[w];
+  __shared__ double sh[256];
+  for (int r = 0; r < 2; ++r) {
+    double* v = est_vec(scr, b, kEX0 + r);
+    const double* t = est_vec(scr, b, kET0 + r);
+    double* vp = est_vec(scr, b, kEY0 + r);
+    double* rec = lan + ((int64_t)w * 2 + r) * 2 * kLanSteps;
+    const double bprev = j > 0 ? rec[2 * (j - 1) + 1] : 0.0;
+    double a = 0.0;
+    for (int i = threadIdx.x; i < b.n; i += blockDim.x) a += t[i] * v[i];
+    a = block_reduce(a, sh, false);
+    double nn = 0.0;
+    for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
+      const double x = t[i] - a * v[i] - bprev * vp[i];
+      nn += x * x;
+    }
+    const double beta = sqrt(block_reduce(nn, sh, false));
+    const double scale = beta > 1e-300 ? 1.0 / beta : 0.0;
+    for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
+      const double x = t[i] - a * v[i] - bprev * vp[i];
+      vp[i] = v[i];
+      v[i] = x * scale;
+    }
+    if (threadIdx.x == 0) {
+      rec[2 * j] = a;
+      rec[2 * j + 1] = beta;
+    }
+    __syncthreads();
+  }
+}
 __device__ double block_reduce(double v, double* sh, bool take_max) {
   sh[threadIdx.x] = v;
   __syncthreads();
@@ -754,6 +815,52 @@ void certified_choice(double rho_up, double tol, int* m_out, int* s_out) {
 // Phase tolerance of the certified and learned selections: 1e-6 per eigenvalue keeps the
 // infidelity of any state below 1e-12 and the relative error of U below 1e-6.
 constexpr double kPhaseTol = 1e-6;
+// Spectral radius from the Lanczos coefficients of one run (alpha_j, beta_j interleaved, k
+// steps): the extreme eigenvalues of the k x k tridiagonal, by Sturm-sequence bisection inside
+// Gershgorin bounds.  Ritz values lie inside the spectrum, so this never exceeds the radius.
+double tridiag_radius(const double* ab, int k) {
+  // a run whose Krylov space ran out has beta = 0: the tridiagonal ends there
+  int kk = k;
+  for (int j = 0; j + 1 < k; ++j)
+    if (!(ab[2 * j + 1] > 0.0)) {
+      kk = j + 1;
+      break;
+    }
+  double lo = 1e300, hi = -1e300;
+  for (int i = 0; i < kk; ++i) {
+    const double off = (i > 0 ? std::fabs(ab[2 * (i - 1) + 1]) : 0.0) + (i + 1 < kk ? std::fabs(ab[2 * i + 1]) : 0.0);
+    lo = std::min(lo, ab[2 * i] - off);
+    hi = std::max(hi, ab[2 * i] + off);
+  }
+  if (!(lo <= hi)) return 0.0;
+  auto below = [&](double x) {   // eigenvalues < x
+    int cnt = 0;
+    double q = 1.0;
+    for (int i = 0; i < kk; ++i) {
+      const double b2 = i > 0 ? ab[2 * (i - 1) + 1] * ab[2 * (i - 1) + 1] : 0.0;
+      q = ab[2 * i] - x - (i > 0 ? b2 / q : 0.0);
+      if (q == 0.0) q = -1e-300;
+      if (q < 0.0) ++cnt;
+    }
+    return cnt;
+  };
+  auto kth = [&](int want) {   // the smallest x with below(x) >= want
+    double a = lo, b = hi;
+    for (int it = 0; it < 200 && b - a > 1e-14 * std::max(std::fabs(a), std::fabs(b)); ++it) {
+      const double m = 0.5 * (a + b);
+      if (below(m) >= want) b = m;
+      else a = m;
+    }
+    return 0.5 * (a + b);
+  };
+  return std::max(std::fabs(kth(1)), std::fabs(kth(kk)));
+}
+// Relative margin on the Lanczos estimate in the estimated selection (selector 3) and in the
+// gate of the learned selection.
+constexpr double kLanMargin = 0.10;
+// Phase tolerance of the learned selection's gate: a phase error phi at the spectrum's edges
+// gives an infidelity of at most sin^2(phi) for any state, so 1e-5 keeps it below 1e-10.
+constexpr double kGateTol = 1e-5;
 
 // Process-wide weights of the learned selector (device copy; fx_selector_set_weights).
 std::mutex g_sel_mu;
@@ -828,6 +935,7 @@ class BatchPipeline {
     exps_.alloc(sizeof(int) * (size_t)(a_rows_ + rows_ + 64));
     diag_.alloc(sizeof(double) * (size_t)(a_rows_ + rows_ + 64));
     linv_.alloc(sizeof(double) * (size_t)rows_ * kNb * 2);
+    lanc_.alloc(sizeof(double) * (size_t)W * 4 * kLanSteps);
     // small: rowstat (kRS per row), estimator vectors (kEstScratch per row), row sums (1 per
     // row), per-walk records (8 + 8 + 4 + 8 + W ints)
     small_.alloc(sizeof(double) * (size_t)(rows_ * (kRS + kEstScratch + 1) + (kWO + 8 + 4 + 8 + 8) * W + 64));
@@ -889,6 +997,12 @@ class BatchPipeline {
     key2_.clear();
   }
   int selector() const { return selector_; }
+  // Spectral-radius estimates of walk w in the last run: Lanczos (a lower estimate) and the
+  // rigorous upper bound min(||Y||_1, d4, d6).
+  void spectral(int w, double* rho_lanczos, double* rho_up) const {
+    *rho_lanczos = rho_lan_.empty() ? 0.0 : rho_lan_[w];
+    *rho_up = rho_up_.empty() ? 0.0 : rho_up_[w];
+  }
   // Diagnostics of the failure path: product launch k (k >= 0) of every run leaves the loads of
   // its first K step out, so that its bounded waits run out; runs are then replayed eagerly.
   void set_inject_stall(int k) { inject_ = k; }
@@ -978,8 +1092,16 @@ class BatchPipeline {
     FX_CUDA(cudaMemcpyAsync(h_wo.data(), walkout(), sizeof(double) * kWO * W, cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaMemcpyAsync(h_flags.data(), flags(), sizeof(int) * W, cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaMemcpyAsync(norms_.data(), norms(), sizeof(double) * 8 * W, cudaMemcpyDeviceToHost, s));
+    lan_host_.assign((size_t)W * 4 * kLanSteps, 0.0);
+    FX_CUDA(cudaMemcpyAsync(lan_host_.data(), lanc_.p, sizeof(double) * lan_host_.size(), cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaStreamSynchronize(s));
     check_err();
+    rho_lan_.assign(W, 0.0);
+    rho_up_.assign(W, 0.0);
+    for (int w = 0; w < W; ++w) {
+      const double* base = lan_host_.data() + (size_t)w * 4 * kLanSteps;
+      rho_lan_[w] = std::max(tridiag_radius(base, kLanSteps), tridiag_radius(base + 2 * kLanSteps, kLanSteps));
+    }
     for (int w = 0; w < W; ++w) {
       if (h_flags[w] & 4) throw Error{FX_ERR_NONFINITE, "input " + std::to_string(w) + " contains NaN or Inf"};
       if (h_flags[w] & 3)
@@ -1027,6 +1149,7 @@ class BatchPipeline {
       plain_m_[w] = m;
       plain_s_[w] = sq;
       const double rho_up = std::min(anorm, std::min(d4, d6));
+      rho_up_[w] = rho_up;
       certified_choice(rho_up, kPhaseTol, &cert_m_[w], &cert_s_[w]);
       // features of the learned selection
       const double n = walks_[w].n;
@@ -1036,7 +1159,7 @@ class BatchPipeline {
       f[1] = std::log2(anorm + 1e-300);
       f[2] = std::log2(std::sqrt(rec[8] / n) + 1e-300);
       f[3] = std::log2(1.0 + rec[9]);
-      f[4] = std::log2(1.0 + std::abs(mu_[w]));
+      f[4] = std::log2(rho_lan_[w] + 1e-300);
       f[5] = rank1_[w] ? 1.0 : 0.0;
       f[6] = std::log2(d4 + 1e-300);
       f[7] = std::log2(d6 + 1e-300);
@@ -1051,6 +1174,16 @@ class BatchPipeline {
         m = cert_m_[w];
         sq = cert_s_[w];
         outcome_[w] = 1;
+      } else if (selector_ == 3) {
+        // the phase bound at the Lanczos estimate of the spectral radius, with a margin (never
+        // above the rigorous bound rho_up)
+        int em = 13, es = 0;
+        certified_choice(std::min(rho_up, rho_lan_[w] * (1.0 + kLanMargin)), kPhaseTol, &em, &es);
+        if (pade_products(em) + es < pade_products(m) + sq) {
+          m = em;
+          sq = es;
+          outcome_[w] = 3;
+        }
       } else if (selector_ == 2) {
         const float* o = prop.data() + 6 * w;
         int c = 0;
@@ -1059,7 +1192,10 @@ class BatchPipeline {
         const int pm = kDegrees[c];
         const int ps = std::max(0, (int)std::lround(o[5]));
         if (pade_products(pm) + ps < pade_products(m) + sq) {
-          if (certified(pm, ps, rho_up, kPhaseTol)) {
+          // gate: the phase bound at the spectral radius as far as it is known -- the rigorous
+          // bound, or the Lanczos estimate with its margin -- at the phase error that keeps the
+          // infidelity of every state below 1e-10
+          if (certified(pm, ps, std::min(rho_up, rho_lan_[w] * (1.0 + kLanMargin)), kGateTol)) {
             m = pm;
             sq = ps;
             outcome_[w] = 2;
@@ -1071,6 +1207,11 @@ class BatchPipeline {
       if (force_m_ > 0) m = force_m_;
       if (force_s_ >= 0 && m == 13) sq = force_s_;
       if (m != 13 && force_s_ < 0 && outcome_[w] <= 0) sq = 0;
+      if (!pw_m_.empty() && pw_m_[w] > 0) {   // per-walk forced (m, s): measured sweeps
+        m = pw_m_[w];
+        sq = std::max(0, pw_s_[w]);
+        outcome_[w] = 4;
+      }
       sel_m_[w] = m;
       sel_s_[w] = sq;
       const double N3 = (double)walks_[w].n * walks_[w].n * walks_[w].n;
@@ -1339,8 +1480,11 @@ class BatchPipeline {
   unsigned timeout_ms_ = 2000;
   bool use_graph_ = true, profile_ = false;
   int force_m_ = -1, force_s_ = -1;
+  std::vector<int> pw_m_, pw_s_;   // per-walk forced (m, s) (diagnostics and measured sweeps)
   int inject_ = -1, prod_index_ = 0;   // stall injection (diagnostics), product launches so far
   int form_ = 0, sq_n4_ = 0, sq_n3_ = 0;   // squaring form and slice schedule
+  DevArena lanc_;                          // Lanczos coefficients (W x 2 runs x kLanSteps x 2)
+  std::vector<double> lan_host_, rho_lan_, rho_up_;
   bool drift_ = false;                     // per-squaring unitarity residual (diagnostics)
   DevArena drift_buf_;
   std::vector<double> drift_host_;
@@ -1369,6 +1513,17 @@ class BatchPipeline {
   void force(int m, int s) {
     force_m_ = m;
     force_s_ = s;
+  }
+  // Per-walk (m, s) for the next runs (m <= 0: that walk's own selection); empty clears.
+  void force_each(const int* m, const int* s) {
+    const int W = count();
+    if (!m) {
+      pw_m_.clear();
+      pw_s_.clear();
+      return;
+    }
+    pw_m_.assign(m, m + W);
+    pw_s_.assign(s, s + W);
   }
 
  private:
@@ -1560,6 +1715,32 @@ class BatchPipeline {
     r.launches += 6;
     estimate(st, r, all, kA4, kA4, 3);
     estimate(st, r, all, kA4, kA6, 4);
+    lanczos(st, r, all);
+  }
+
+  // Lanczos runs on B = Im Y (arena Y) of the listed walks into lanc_ (kLanSteps steps).
+  void lanczos(Staging& st, Rec& r, const std::vector<int>& list) {
+    const size_t o_l = st.put(list);
+    const int nl = (int)list.size();
+    std::vector<RChunk> ch;
+    for (int w : list) {
+      const int np = walks_[w].np, R = std::max(8, (kChunkElems / np) & ~7);
+      for (int r0 = 0; r0 < np; r0 += R) ch.push_back(RChunk{w, r0, std::min(np, r0 + R), 0});
+    }
+    const size_t o_ch = st.put(ch);
+    const unsigned g_rows = (unsigned)ch.size();
+    r.ops.push_back([=]() {
+      const BWalk* wk = (const BWalk*)d_walks_.p;
+      const int* l = dev<int>(o_l);
+      kb_lan_init<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), estst());
+      FX_LAUNCH_CHECK();
+      for (int j = 0; j < kLanSteps; ++j) {
+        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(kY), dev<RChunk>(o_ch), wk, est_scr(), estst(), kEX0, kET0);
+        kb_lan_step<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), (double*)lanc_.p, j);
+      }
+      FX_LAUNCH_CHECK();
+    });
+    r.launches += 1 + 2 * kLanSteps;
   }
 
   // Block 1-norm estimate of ||M0 M1||_1 for the listed walks into norms()[8 w + slot].
@@ -2511,6 +2692,9 @@ void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, voi
 }
 const std::vector<ProdRecord>& batch_pipeline_products(const BatchPipeline* p) { return p->prod_list(); }
 std::vector<double> batch_pipeline_drift(const BatchPipeline* p) { return p->drift_curve(0); }
+void batch_pipeline_spectral(const BatchPipeline* p, double* rho_lanczos, double* rho_up) {
+  p->spectral(0, rho_lanczos, rho_up);
+}
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st) {
   p->walk_stats(0, st);
   double f[8];
@@ -2639,8 +2823,9 @@ int fx_batch_set_option(fx_batch_handle b, int key, double value) {
       return FX_OK;
     case FX_BATCH_OPT_FORCE_M: b->p->force((int)value, -1); return FX_OK;
     case FX_BATCH_OPT_SELECTOR:
-      if (value != 0 && value != 1 && value != 2)
-        return bfail(b, fx::Error{FX_ERR_VALUE, "selector must be 0 (plain), 1 (certified) or 2 (learned)"});
+      if (value != 0 && value != 1 && value != 2 && value != 3)
+        return bfail(b, fx::Error{FX_ERR_VALUE,
+                                  "selector must be 0 (plain), 1 (certified), 2 (learned) or 3 (estimated)"});
       b->p->set_selector((int)value);
       return FX_OK;
     case FX_BATCH_OPT_ANALYZE_ONLY: b->p->set_analyze_only(value != 0.0); return FX_OK;
@@ -2728,6 +2913,29 @@ int fx_batch_walk_host(fx_batch_handle b, const void* const* X, const void* cons
     }
     FX_CUDA(cudaStreamSynchronize(b->stream));
   });
+}
+
+int fx_batch_force_selection(fx_batch_handle b, const int32_t* m, const int32_t* s) {
+  if (!b || (m && !s)) return bfail(b, fx::Error{FX_ERR_VALUE, "null argument"});
+  if (m) {
+    for (size_t w = 0; w < b->ns.size(); ++w) {
+      const int mw = m[w];
+      if (mw > 0 && mw != 3 && mw != 5 && mw != 7 && mw != 9 && mw != 13)
+        return bfail(b, fx::Error{FX_ERR_VALUE, "forced Pade degree must be 3, 5, 7, 9 or 13"});
+      if (mw > 0 && (s[w] < 0 || s[w] > 60)) return bfail(b, fx::Error{FX_ERR_VALUE, "forced s must be 0..60"});
+    }
+    std::vector<int> mm(m, m + b->ns.size()), ss(s, s + b->ns.size());
+    b->p->force_each(mm.data(), ss.data());
+  } else {
+    b->p->force_each(nullptr, nullptr);
+  }
+  return FX_OK;
+}
+
+int fx_batch_spectral(fx_batch_handle b, double* rho_lanczos, double* rho_up) {
+  if (!b || !rho_lanczos || !rho_up) return bfail(b, fx::Error{FX_ERR_VALUE, "null argument"});
+  for (size_t w = 0; w < b->ns.size(); ++w) b->p->spectral((int)w, rho_lanczos + w, rho_up + w);
+  return FX_OK;
 }
 
 int fx_batch_drift(fx_batch_handle b, int64_t w, double* out, int32_t cap, int32_t* count) {

@@ -1286,7 +1286,7 @@ int fx_set_option(fx_handle h, int key, double value) {
     case FX_OPT_DEBUG_STAGE: h->opts.debug_stage = v; return FX_OK;
     case FX_OPT_PROFILE: h->opts.profile = v != 0; return FX_OK;
     case FX_OPT_SELECTOR:
-      if (v < 0 || v > 2) return fail(h, fx::Error{FX_ERR_VALUE, "selector must be 0, 1 or 2"});
+      if (v < 0 || v > 3) return fail(h, fx::Error{FX_ERR_VALUE, "selector must be 0, 1, 2 or 3"});
       h->opts.selector = v;
       return FX_OK;
     case FX_OPT_INJECT_STALL:
@@ -1314,6 +1314,13 @@ int fx_product_profile(fx_handle h, int32_t* tags, double* ms, double* ops, int3
     ops[i] = v[i].ops;
   }
   *count = (int32_t)v.size();
+  return FX_OK;
+}
+
+int fx_spectral_radius(fx_handle h, double* rho_lanczos, double* rho_up) {
+  if (!h || !rho_lanczos || !rho_up) return fail(h, fx::Error{FX_ERR_VALUE, "null argument"});
+  *rho_lanczos = *rho_up = 0.0;
+  if (h->grouped) fx::batch_pipeline_spectral(h->grouped, rho_lanczos, rho_up);
   return FX_OK;
 }
 

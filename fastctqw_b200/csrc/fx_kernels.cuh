@@ -243,7 +243,7 @@ void batch_pipeline_destroy(BatchPipeline* p);
 struct PipeOpts {
   bool profile = false;      // CUDA-event timing of every product launch
   unsigned timeout_ms = 2000;
-  int selector = 0;          // 0 Al-Mohy & Higham, 1 certified bound, 2 learned
+  int selector = 0;          // 0 Al-Mohy & Higham, 1 certified bound, 2 learned, 3 estimated
   int inject_stall = -1;     // diagnostics: k >= 0 makes product launch k of every run skip the
                              // operand loads of its first K step, so that the bounded waits run out
   int form = FX_FORM_PLAIN;  // FX_FORM_MIXED: two-product squarings with the slice schedule below
@@ -257,6 +257,7 @@ void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, voi
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st);
 const std::vector<ProdRecord>& batch_pipeline_products(const BatchPipeline* p);
 std::vector<double> batch_pipeline_drift(const BatchPipeline* p);
+void batch_pipeline_spectral(const BatchPipeline* p, double* rho_lanczos, double* rho_up);
 // Host <-> device copies of large host buffers (fx_hostcopy.cu): a buffer the driver knows as
 // page-locked is copied by DMA directly; any other goes through two page-locked chunk buffers,
 // the host side of a chunk (split over threads) overlapping the DMA of the previous one.

@@ -14,16 +14,22 @@ With rho_up = min(||Y||_1, ||Y^4||_1^(1/4), ||Y^6||_1^(1/6)) >= spectral radius 
 of the powers the pipeline forms anyway), the engine *certifies* a choice (m, s) when
 2^s |phi_m(rho_up / 2^s)| <= 1e-6 (``certified``; the same test runs in C++ in fx_batch.cu).
 
+The engine also estimates the spectral radius by Lanczos (30 steps from two pseudo-random
+starts, ``rho_L``; Ritz values lie inside the spectrum, so rho_L <= rho).  On dense graphs the
+norm bound rho_up is about 1.5 rho, which costs a squaring or two.
+
 The learned selector is an MLP 8 -> 64 -> 64 -> (5 logits over m in {3, 5, 7, 9, 13} + s) with
 hand-written CUDA kernels (fx_selector.cu: BF16 inference, fused FP32 forward/backward, Adam).
-It is trained on the GPU on (features, labels) that the engine itself produces for seeded walk
-generators (``make_dataset``: the engine's analyze-only mode returns the features, the
-Al-Mohy & Higham (m, s) and the cheapest certified (m, s), which is the label).  At run time a
-proposal is used only when it is cheaper than the plain choice, the bound certifies it and the
-result passes the unitarity check; otherwise the plain (m, s) is used.
+It is trained on the GPU on labels *measured* by the engine (``make_dataset_measured``): every
+training walk runs at a grid of forced (m, s) and its result is compared with the FP64
+eigendecomposition on the state that exposes the truncation error most, the equal superposition
+of the eigenvectors at the two ends of the spectrum; the label is the cheapest (m, s) whose
+infidelity stays <= 1e-10.  At run time a proposal is used only when it is cheaper than the plain
+choice, the phase bound at min(rho_up, 1.1 rho_L) stays below 1e-5 (``gate``) and the result
+passes the a-posteriori checks; otherwise the plain (m, s) is used.
 
 Features (per walk): log2 n, log2 ||Y||_1, log2 (||X||_F / sqrt n), log2 (1 + max off-diagonal
-nonzeros of a row), log2 (1 + |trace shift|), rank-one shift flag, log2 d4, log2 d6.
+nonzeros of a row), log2 rho_L, rank-one shift flag, log2 d4, log2 d6.
 """
 from __future__ import annotations
 
@@ -39,11 +45,14 @@ from ._native import lib
 DEGREES = (3, 5, 7, 9, 13)
 PRODUCTS = {3: 2, 5: 3, 7: 4, 9: 5, 13: 6}
 PHASE_TOL = 1e-6
+GATE_TOL = 1e-5      # phase error of the learned selection's gate: infidelity <= 1e-10 for any state
+LAN_MARGIN = 0.10    # relative margin on the Lanczos estimate
+INFID_LABEL = 1e-10  # measured labels: the cheapest (m, s) at or below this infidelity
 X_LIMIT = {3: 5.0, 5: 7.2, 7: 9.3, 9: 11.4, 13: 15.6}   # half of where |phi_m| reaches pi
 N_PARAMS = 5126
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "selector_weights.npz")
 FEATURE_NAMES = ("log2 n", "log2 ||Y||_1", "log2 ||X||_F/sqrt(n)", "log2(1+max degree)",
-                 "log2(1+|mu|)", "rank-one shift", "log2 d4", "log2 d6")
+                 "log2 rho_L", "rank-one shift", "log2 d4", "log2 d6")
 
 
 def pade_coeffs(m: int) -> list[float]:
@@ -136,6 +145,106 @@ def make_dataset(count: int, seed: int, nmin: int = 64, nmax: int = 1024, tmin: 
             "cert_m": cat(cm), "cert_s": cat(cs), "meta": np.array(meta, dtype=object)}
 
 
+def min_certified_s(m: int, rho: float, tol: float = PHASE_TOL) -> int:
+    s = 0
+    while s < 60 and not certified(m, s, rho, tol):
+        s += 1
+    return s
+
+
+def make_dataset_measured(count: int, seed: int, nmin: int = 64, nmax: int = 2048, tmin: float = 0.1,
+                          tmax: float = 1000.0, chunk: int = 96, depth: int = 5) -> dict:
+    """Walks of ``make_walks`` with labels measured on the GPU.
+
+    Per chunk of walks: one analyze-only run (features, the Al-Mohy & Higham and the certified
+    (m, s)); the FP64 eigendecomposition of every B = Im X (torch on the device) gives the test
+    state psi0 = (v_max + v_min) / sqrt 2, whose output is the most sensitive one to phase errors
+    (the two ends of the spectrum rotate in opposite directions); then for every m the walks run
+    at forced s = s_m - k, k = 0 .. depth - 1, where s_m is the smallest s the rigorous bound
+    certifies for that m.  (m, s) passes when the infidelity against the FP64 state is <= 1e-10
+    (and no a-posteriori check redid the walk); the label is the cheapest (m, s) (products
+    pi_m + s, ties to the larger m) whose s and every larger tested s pass."""
+    import torch
+    from .batch import OPT_SAMPLE_WALKS, WalkBatch
+    dev = torch.device("cuda", 0)
+    feats, pm_, ps_, cm_, cs_, lm_, ls_, meta, inf_plain = [], [], [], [], [], [], [], [], []
+    it = make_walks(count, seed, nmin, nmax, tmin, tmax)
+    todo = count
+    while todo > 0:
+        k = min(chunk, todo)
+        todo -= k
+        Xs, ms = [], []
+        for _ in range(k):
+            X, mt = next(it)
+            Xs.append(X)
+            ms.append(mt)
+        ns = [X.shape[0] for X in Xs]
+        with WalkBatch(ns, analyze_only=True) as b:
+            b.run(Xs)
+            d = b.details()
+        ru = rho_up(d["features"])
+        dX = [torch.from_numpy(X).to(dev) for X in Xs]
+        p0s, refs = [], []
+        for X in Xs:
+            lam, V = torch.linalg.eigh(torch.from_numpy(np.ascontiguousarray(X.imag, dtype=np.float64)).to(dev))
+            p = (V[:, -1] + V[:, 0]) / math.sqrt(2.0)
+            ref = (torch.exp(1j * lam[-1]) * V[:, -1] + torch.exp(1j * lam[0]) * V[:, 0]) / math.sqrt(2.0)
+            p0s.append(p.to(torch.complex64))
+            refs.append(ref)
+            del lam, V
+        outs = [torch.empty_like(p) for p in p0s]
+        sweep = WalkBatch(ns)
+        sweep.set_option(OPT_SAMPLE_WALKS, 0)
+
+        def infidelities():
+            sweep.run_device(dX, p0s, outs)
+            torch.cuda.synchronize()
+            oc = sweep.details()["outcome"]
+            r = []
+            for w in range(k):
+                q = outs[w].to(torch.complex128)
+                ov = torch.vdot(refs[w], q).abs() ** 2 / (torch.vdot(q, q).real * torch.vdot(refs[w], refs[w]).real)
+                r.append(1.0 if oc[w] == -2 else float(1.0 - ov))
+            return np.array(r)
+
+        inf_plain.append(infidelities())   # the plain selection's own result
+        best = [(PRODUCTS[int(d["plain_m"][w])] + int(d["plain_s"][w]), int(d["plain_m"][w]), int(d["plain_s"][w]))
+                for w in range(k)]
+        for m in DEGREES:
+            s_top = np.array([min_certified_s(m, float(r)) for r in ru])
+            ok = np.ones(k, dtype=bool)     # every s tested so far (from the top) passed
+            for kk in range(depth):
+                s_try = s_top - kk
+                active = ok & (s_try >= 0)
+                if not active.any():
+                    break
+                sweep.force_selection(np.full(k, m), np.maximum(s_try, 0))
+                inf = infidelities()
+                for w in np.nonzero(active)[0]:
+                    if inf[w] <= INFID_LABEL:
+                        cost = PRODUCTS[m] + int(s_try[w])
+                        if cost < best[w][0] or (cost == best[w][0] and m > best[w][1]):
+                            best[w] = (cost, m, int(s_try[w]))
+                    else:
+                        ok[w] = False
+        sweep.force_selection()
+        sweep.close()
+        feats.append(d["features"])
+        pm_.append(d["plain_m"])
+        ps_.append(d["plain_s"])
+        cm_.append(d["cert_m"])
+        cs_.append(d["cert_s"])
+        lm_.append(np.array([b_[1] for b_ in best], dtype=np.int32))
+        ls_.append(np.array([b_[2] for b_ in best], dtype=np.int32))
+        meta.extend(ms)
+        del dX, p0s, refs, outs
+        torch.cuda.empty_cache()
+    cat = np.concatenate
+    return {"features": cat(feats).astype(np.float32), "plain_m": cat(pm_), "plain_s": cat(ps_),
+            "cert_m": cat(cm_), "cert_s": cat(cs_), "label_m": cat(lm_), "label_s": cat(ls_),
+            "infidelity_plain": cat(inf_plain), "meta": np.array(meta, dtype=object)}
+
+
 def merge(*sets: dict) -> dict:
     return {k: np.concatenate([d[k] for d in sets]) for k in sets[0]}
 
@@ -146,23 +255,38 @@ def rho_up(features: np.ndarray) -> np.ndarray:
     return np.exp2(np.minimum(f[:, 1], np.minimum(f[:, 6], f[:, 7])))
 
 
+def rho_gate(features: np.ndarray) -> np.ndarray:
+    """min(rho_up, 1.1 rho_L): the spectral radius as far as the engine knows it."""
+    f = np.asarray(features, dtype=np.float64)
+    return np.minimum(rho_up(f), np.exp2(f[:, 4]) * (1.0 + LAN_MARGIN))
+
+
 def gate(features, plain_m, plain_s, prop_m, prop_s) -> np.ndarray:
     """Selection outcome per walk, as the engine decides it: 2 accepted, -1 rejected by the
     bound, 0 not cheaper than the plain choice."""
-    r = rho_up(features)
+    r = rho_gate(features)
     out = np.zeros(len(r), dtype=np.int32)
     for i in range(len(r)):
         pm, ps = int(prop_m[i]), int(prop_s[i])
         if PRODUCTS[pm] + ps < PRODUCTS[int(plain_m[i])] + int(plain_s[i]):
-            out[i] = 2 if certified(pm, ps, float(r[i])) else -1
+            out[i] = 2 if certified(pm, ps, float(r[i]), GATE_TOL) else -1
     return out
 
 
+def estimated_choice(features) -> tuple[np.ndarray, np.ndarray]:
+    """The engine's estimated selection (selector 3) for every walk: the cheapest (m, s) the
+    phase bound at min(rho_up, 1.1 rho_L) certifies at 1e-6."""
+    r = rho_gate(features)
+    mm, ss = zip(*[certified_choice(float(x)) for x in r])
+    return np.array(mm, dtype=np.int32), np.array(ss, dtype=np.int32)
+
+
 def labels(ds: dict) -> tuple[np.ndarray, np.ndarray]:
-    """Class index of the certified m in DEGREES and the certified s (float)."""
+    """Class index of the label m in DEGREES and the label s (float): the measured labels when
+    the dataset has them, else the certified choice."""
+    km, ks = ("label_m", "label_s") if "label_m" in ds else ("cert_m", "cert_s")
     idx = {m: i for i, m in enumerate(DEGREES)}
-    return (np.array([idx[int(m)] for m in ds["cert_m"]], dtype=np.int32),
-            np.asarray(ds["cert_s"], dtype=np.float32))
+    return (np.array([idx[int(m)] for m in ds[km]], dtype=np.int32), np.asarray(ds[ks], dtype=np.float32))
 
 
 # ----------------------------------------------------------------------------- network

@@ -85,9 +85,14 @@ enum fx_option {
                              (fx_stats.prod_*)                                         */
   FX_OPT_SELECTOR = 10,   /* (m, s) selection for walk generators X = i*(real symmetric):
                              0 Al-Mohy & Higham (default), 1 the cheapest (m, s) the
-                             truncation bound certifies at phase error 1e-6, 2 the learned
-                             MLP proposal, accepted only when the bound certifies it and
-                             the result passes the unitarity check (else option 0)     */
+                             truncation bound certifies at phase error 1e-6 from the
+                             rigorous spectral bound min(||Y||_1, d4, d6), 2 the learned
+                             MLP proposal, accepted only when the phase bound at
+                             min(rigorous bound, 1.1 x the Lanczos estimate) stays below
+                             1e-5 (infidelity <= 1e-10 for every state) and the result
+                             passes the a-posteriori checks (else option 0), 3 the
+                             same phase bound at a Lanczos estimate of the spectral radius
+                             (30 steps, two starts) raised by 10% (estimated selection) */
   FX_OPT_INJECT_STALL = 11, /* diagnostics of the failure path (walk generators): k >= 0 makes
                              the k-th product launch of every run leave out the operand
                              loads of one K step, so that its bounded waits run out and
@@ -124,9 +129,10 @@ typedef struct fx_stats {
   int32_t prod_launches;
   int32_t reserved2;
   int32_t selector;     /* FX_OPT_SELECTOR of the run                                  */
-  int32_t sel_outcome;  /* 0 plain, 1 certified, 2 learned accepted, -1 learned rejected
-                           by the bound, -2 failed an a-posteriori check (Cholesky of
-                           Q^H Q or unitarity) and was redone with the plain (m, s)  */
+  int32_t sel_outcome;  /* 0 plain, 1 certified, 2 learned accepted, 3 estimated, -1 learned
+                           rejected by the bound, -2 failed an a-posteriori check
+                           (Cholesky of Q^H Q or unitarity) and was redone with the plain
+                           (m, s)                                                   */
   int32_t plain_m;      /* (m, s) of the Al-Mohy & Higham selection                    */
   int32_t plain_s;
 } fx_stats;
@@ -154,6 +160,11 @@ int fx_product_profile(fx_handle h, int32_t* tags, double* ms, double* ops, int3
  * and s + 1 to *count (0 when no such run was made).  Diagnostics; no counterpart in the
  * reference. */
 int fx_unitarity_drift(fx_handle h, double* out, int32_t cap, int32_t* count);
+/* Spectral-radius estimates of the shifted generator of the last walk-generator run: a Lanczos
+ * estimate (30 steps from two pseudo-random starts; Ritz values lie inside the spectrum, so it
+ * does not exceed the radius) and the rigorous upper bound min(||Y||_1, d4, d6).  Diagnostics
+ * of the (m, s) selection; no counterpart in the reference. */
+int fx_spectral_radius(fx_handle h, double* rho_lanczos, double* rho_up);
 
 /* U = expm(A), both host buffers of n*n elements of the handle's dtype. */
 int fx_run_host(fx_handle h, const void* A, void* U);
@@ -244,12 +255,19 @@ int fx_batch_walk_host(fx_batch_handle b, const void* const* X, const void* cons
 /* Unitarity residuals of walk w in the last run made with FX_BATCH_OPT_DRIFT = 1 (as
  * fx_unitarity_drift). */
 int fx_batch_drift(fx_batch_handle b, int64_t w, double* out, int32_t cap, int32_t* count);
+/* Per-walk forced (m, s) for the following runs (arrays of `count`; m[w] <= 0 leaves walk w to
+ * the selector; m NULL clears): measured (m, s, error) sweeps for the learned selector's labels.
+ * Forced walks report outcome 4.  No counterpart in the reference. */
+int fx_batch_force_selection(fx_batch_handle b, const int32_t* m, const int32_t* s);
+/* Per walk of the last run (arrays of `count`): the Lanczos spectral-radius estimate and the
+ * rigorous bound (as fx_spectral_radius). */
+int fx_batch_spectral(fx_batch_handle b, double* rho_lanczos, double* rho_up);
 /* (m, s) chosen for every walk by the last run (arrays of `count`). */
 int fx_batch_selection(fx_batch_handle b, int32_t* m, int32_t* s);
 /* Device time (ms, CUDA events), algorithmic flops and kernel launches of the last run. */
 int fx_batch_info(fx_batch_handle b, double* ms, double* flops, int32_t* launches);
 /* Per walk of the last run: the 8 selector features (features[8 w ..]: log2 n, log2 ||Y||_1,
- * log2 (||X||_F / sqrt n), log2 (1 + max off-diagonal nonzeros of a row), log2 (1 + |mu|),
+ * log2 (||X||_F / sqrt n), log2 (1 + max off-diagonal nonzeros of a row), log2 (Lanczos spectral radius),
  * rank-one shift flag, log2 d4, log2 d6), the Al-Mohy & Higham (m, s), the certified (m, s) and
  * the selection outcome (as fx_stats.sel_outcome). */
 int fx_batch_details(fx_batch_handle b, double* features, int32_t* plain_m, int32_t* plain_s,

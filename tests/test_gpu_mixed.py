@@ -106,3 +106,39 @@ def test_mixed_batch_matches_plain_batch():
         ref = V @ (np.exp(1j * lam) * (V.T @ P0[k].astype(np.complex128)))
         assert eo.infidelity(b[k], ref) <= INFID, (k, ns[k])
         assert eo.infidelity(a[k], ref) <= INFID, (k, ns[k])
+
+
+def test_estimated_selection_uses_the_lanczos_radius():
+    """Selector 3: the phase bound of the Pade approximant evaluated at the Lanczos estimate of
+    the spectral radius (+10%) instead of the rigorous norm bound.  On the dense Laplacian family
+    the estimate is within a few percent of the exact radius (below it, as Ritz values are), the
+    selection takes fewer squarings than the Al-Mohy & Higham choice, and the result still meets
+    the accuracy bar."""
+    from fastctqw_b200 import graphs
+    from fastctqw_b200._native import Engine
+    import torch
+    n = 2048
+    X, Uref = _dense(n)
+    # exact radius of the shifted generator (trace and rank-one shifts, as the engine applies)
+    B = X.imag.astype(np.float64)
+    Y = B - np.trace(B) / n * np.eye(n)
+    Y -= Y.sum() / n * np.ones((n, n)) / n
+    rho = np.abs(np.linalg.eigvalsh(Y)).max()
+    _, _, st0, _ = _walk(X, "plain")
+    U, psi, st3, _ = _walk(X, "plain", selector="estimated")
+    assert st3["sel_outcome"] == 3 and st3["s"] < st0["s"], (st0["s"], st3["s"])
+    assert eo.rel_error(U, Uref) <= C64_REL
+    assert eo.infidelity(psi, Uref[:, 0]) <= INFID
+    for p0 in (graphs.uniform_state(n), graphs.random_state(n, 4)):
+        p = p0.astype(np.complex128)
+        assert eo.infidelity(U.astype(np.complex128) @ p, Uref @ p) <= INFID
+    dev = torch.device("cuda", 0)
+    e = Engine(n, np.complex64)
+    dX = torch.from_numpy(X).to(dev)
+    p0 = torch.zeros(n, dtype=torch.complex64, device=dev)
+    p0[0] = 1.0
+    e.walk_device(dX, p0, torch.empty_like(p0))
+    sr = e.spectral_radius()
+    e.close()
+    assert 0.9 * rho <= sr["lanczos"] <= rho * (1 + 1e-9), (sr, rho)
+    assert sr["upper_bound"] >= rho * (1 - 1e-9), (sr, rho)
