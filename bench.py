@@ -535,7 +535,7 @@ def main():
                     help="(m, s) selection of the timed walk; the plain selection is timed beside it")
     ap.add_argument("--ref-sample-n", type=int, default=1024,
                     help="size of the small sample behind the flop-model cross-check of the reference arm")
-    ap.add_argument("--ref-budget-s", type=float, default=240.0,
+    ap.add_argument("--ref-budget-s", type=float, default=150.0,
                     help="reference arm: full-size runs are added while their total stays within this")
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 infidelity check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

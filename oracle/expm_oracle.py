@@ -430,3 +430,71 @@ def rel_error(U: np.ndarray, U_ref: np.ndarray) -> float:
 def flops_expm(n: int, m: int, s: int) -> float:
     """Algorithmic real flops of one complex expm: 8n^3 (pi_m + s) + (8/3) n^3 + 8 n^3."""
     return 8.0 * n ** 3 * (PADE_PRODUCTS[m] + s) + (8.0 / 3.0) * n ** 3 + 8.0 * n ** 3
+
+
+# ---------------------------------------------------------------- spectral radius (selection)
+
+def tridiag_radius(alpha, beta) -> float:
+    """Largest |eigenvalue| of the symmetric tridiagonal (alpha on the diagonal, beta beside it)
+    by Sturm-sequence bisection inside the Gershgorin interval -- the step the engine runs on the
+    host after its device Lanczos iterations (fx_batch.cu, tridiag_radius).  A zero beta_j ends
+    the matrix after row j (the Krylov space ran out)."""
+    a = [float(x) for x in alpha]
+    b = [float(x) for x in beta]
+    k = len(a)
+    for j in range(k - 1):
+        if not b[j] > 0.0:
+            k = j + 1
+            break
+    a, b = a[:k], b[:k - 1]
+    off = [(abs(b[i - 1]) if i > 0 else 0.0) + (abs(b[i]) if i + 1 < k else 0.0) for i in range(k)]
+    lo = min(a[i] - off[i] for i in range(k))
+    hi = max(a[i] + off[i] for i in range(k))
+
+    def below(x):
+        cnt, q = 0, 1.0
+        for i in range(k):
+            q = a[i] - x - (b[i - 1] ** 2 / q if i > 0 else 0.0)
+            if q == 0.0:
+                q = -1e-300
+            cnt += q < 0.0
+        return cnt
+
+    def kth(want):
+        x0, x1 = lo, hi
+        for _ in range(200):
+            if x1 - x0 <= 1e-14 * max(abs(x0), abs(x1)):
+                break
+            mid = 0.5 * (x0 + x1)
+            if below(mid) >= want:
+                x1 = mid
+            else:
+                x0 = mid
+        return 0.5 * (x0 + x1)
+
+    return max(abs(kth(1)), abs(kth(k)))
+
+
+def lanczos_radius(B: np.ndarray, steps: int = 30, starts: int = 2, seed: int = 0) -> float:
+    """Spectral-radius estimate of a real symmetric B: `starts` Lanczos runs of `steps` steps from
+    random sign vectors, no reorthogonalisation, the largest radius of their tridiagonals (the
+    algorithm of the engine's estimate; its Ritz values lie inside the spectrum)."""
+    n = B.shape[0]
+    rng = np.random.default_rng(seed)
+    best = 0.0
+    for _ in range(starts):
+        v = rng.choice([-1.0, 1.0], n) / np.sqrt(n)
+        vp = np.zeros(n)
+        bprev = 0.0
+        alpha, beta = [], []
+        for _j in range(steps):
+            t = B @ v
+            a = float(t @ v)
+            w = t - a * v - bprev * vp
+            bb = float(np.linalg.norm(w))
+            alpha.append(a)
+            beta.append(bb)
+            vp, v = v, (w / bb if bb > 1e-300 else np.zeros(n))
+            bprev = bb
+        best = max(best, tridiag_radius(alpha, beta[:-1]))
+    return best
