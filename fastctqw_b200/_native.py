@@ -22,7 +22,8 @@ CODE_DTYPE = {v: k for k, v in DTYPE_CODE.items()}
 FORM_PLAIN, FORM_MIXED, FORM_SIMT, FORM_FP64 = 0, 1, 2, 3
 FORMS = {"plain": FORM_PLAIN, "mixed": FORM_MIXED, "simt": FORM_SIMT, "fp64": FORM_FP64}
 (OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE,
- OPT_DEBUG_STAGE, OPT_PROFILE, OPT_SELECTOR, OPT_INJECT_STALL, OPT_SQ_N4, OPT_SQ_N3, OPT_DRIFT) = range(15)
+ OPT_DEBUG_STAGE, OPT_PROFILE, OPT_SELECTOR, OPT_INJECT_STALL, OPT_SQ_N4, OPT_SQ_N3, OPT_DRIFT,
+ OPT_PADE_SLICES) = range(16)
 SELECTORS = {"plain": 0, "certified": 1, "learned": 2, "estimated": 3}
 
 OK, ERR_TYPE, ERR_VALUE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_NONFINITE, ERR_SINGULAR, ERR_NODEV, ERR_FREED = range(10)
@@ -230,7 +231,7 @@ class Engine:
                   timeout_ms: float | None = None, debug_stage: int | None = None,
                   profile: bool | None = None, selector: str | None = None,
                   inject_stall: int | None = None, sq_n4: int | None = None, sq_n3: int | None = None,
-                  drift: bool | None = None) -> None:
+                  drift: bool | None = None, pade_slices: int | None = None) -> None:
         if form is not None:
             if form not in FORMS:
                 raise ValueError(f"form must be one of {sorted(FORMS)}")
@@ -263,6 +264,8 @@ class Engine:
             self.set_option(OPT_SQ_N3, sq_n3)
         if drift is not None:
             self.set_option(OPT_DRIFT, int(bool(drift)))
+        if pade_slices is not None:
+            self.set_option(OPT_PADE_SLICES, pade_slices)
 
     def spectral_radius(self) -> dict:
         """Lanczos estimate and rigorous upper bound of the shifted generator's spectral radius

@@ -1009,13 +1009,15 @@ class BatchPipeline {
   // Precision form of the squarings: 0 plain (every squaring the exact complex square, 4 real
   // products at 5 slices); 1 mixed (each squaring as the two real products (Er + Ei)(Er - Ei)
   // and 2 Er Ei, 5 slices except the last n4 + n3 squarings: n4 at 4 slices, then n3 at 3).
-  void set_form(int form, int n4, int n3) {
-    if (form == form_ && n4 == sq_n4_ && n3 == sq_n3_) return;
+  void set_form(int form, int n4, int n3, int pade_slices = kS) {
+    if (form == form_ && n4 == sq_n4_ && n3 == sq_n3_ && pade_slices == pade_S_) return;
     form_ = form;
     sq_n4_ = n4;
     sq_n3_ = n3;
+    pade_S_ = pade_slices;
     key2_.clear();
   }
+  int pade_slices() const { return pade_S_; }
   int form() const { return form_; }
   // Diagnostics: the unitarity residual ||U_k^H U_k - I||_F / sqrt(n) of the iterate after every
   // squaring k = 0..s (k = 0: the Pade result), from two extra 5-slice products per squaring.
@@ -1483,6 +1485,8 @@ class BatchPipeline {
   std::vector<int> pw_m_, pw_s_;   // per-walk forced (m, s) (diagnostics and measured sweeps)
   int inject_ = -1, prod_index_ = 0;   // stall injection (diagnostics), product launches so far
   int form_ = 0, sq_n4_ = 0, sq_n3_ = 0;   // squaring form and slice schedule
+  int pade_S_ = kS;                        // mixed form: slices of the Pade and solve products
+  int gS_ = kS;                            // slices of the grouped products being recorded
   DevArena lanc_;                          // Lanczos coefficients (W x 2 runs x kLanSteps x 2)
   std::vector<double> lan_host_, rho_lan_, rho_up_;
   bool drift_ = false;                     // per-squaring unitarity residual (diagnostics)
@@ -1907,7 +1911,8 @@ class BatchPipeline {
   void grouped(Staging& st, Rec& r, const std::vector<GSlab>& sa, const std::vector<GSlab>* sb,
                const std::vector<GProblem>& pr, bool same, int tri, bool split = false) {
     if (pr.empty()) return;
-    const int bn = i8_tile_bn(kS);
+    const int S = gS_;
+    const int bn = i8_tile_bn(S);
     std::vector<GTile> tiles;
     for (int i = 0; i < (int)pr.size(); ++i) {
       const GProblem& p = pr[i];
@@ -1928,7 +1933,7 @@ class BatchPipeline {
     std::sort(b_sorted.begin(), b_sorted.end(), by_row);
     const size_t o_sa = st.put(a_sorted), o_sb = st.put(b_sorted), o_pr = st.put(pr), o_t = st.put(tiles);
     const int nsa = (int)a_sorted.size(), nsb = (int)b_sorted.size(), nt = (int)tiles.size();
-    const double ops = tile_ops(tiles, 1);
+    const double ops = tile_ops(tiles, 1, S);
     int64_t a_span = 0, b_span = 0;
     const int64_t ka = widest(a_sorted), kb = widest(b_sorted);
     for (const GSlab& g : a_sorted) a_span = std::max<int64_t>(a_span, (int64_t)g.row0 + g.rows);
@@ -1938,7 +1943,7 @@ class BatchPipeline {
     const int tag = tag_;
     r.ops.push_back([=]() {
       I8Slices outa{}, outb{};
-      for (int q = 0; q < kS; ++q) {
+      for (int q = 0; q < S; ++q) {
         outa.re[q] = slice_plane(0, q);
         outb.re[q] = slice_plane(3, q);
       }
@@ -1947,21 +1952,21 @@ class BatchPipeline {
       outa.dg = split ? adiag() : nullptr;
       outb.dg = split ? bdiag() : nullptr;
       outa.ld = outb.ld = pitch_;
-      launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, a_span, outa, false, stream_, ka);
+      launch_slice_rows_grouped<double>(S, dev<GSlab>(o_sa), nsa, a_span, outa, false, stream_, ka);
       I8Term t{};
-      for (int q = 0; q < kS; ++q) t.a[q] = outa.re[q];
+      for (int q = 0; q < S; ++q) t.a[q] = outa.re[q];
       if (!same) {
-        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sb), nsb, b_span, outb, false, stream_, kb);
-        for (int q = 0; q < kS; ++q) t.b[q] = outb.re[q];
+        launch_slice_rows_grouped<double>(S, dev<GSlab>(o_sb), nsb, b_span, outb, false, stream_, kb);
+        for (int q = 0; q < S; ++q) t.b[q] = outb.re[q];
       } else {
-        for (int q = 0; q < kS; ++q) t.b[q] = outa.re[q];
+        for (int q = 0; q < S; ++q) t.b[q] = outa.re[q];
       }
       const size_t pi = prof_begin();
-      launch_gemm_i8_grouped<double>(kS, &t, 1, pitch_, a_rows_, same ? a_rows_ : rows_, aexp(),
+      launch_gemm_i8_grouped<double>(S, &t, 1, pitch_, a_rows_, same ? a_rows_ : rows_, aexp(),
                                      same ? aexp() : bexp(), dev<GProblem>(o_pr), dev<GTile>(o_t), nt,
                                      (int*)err_.p, timeout_ms_, stream_, split ? adiag() : nullptr,
                                      split ? (same ? adiag() : bdiag()) : nullptr, next_skip());
-      prof_end(pi, ops * kS * (kS + 1) / 2, ops, tag);
+      prof_end(pi, ops * S * (S + 1) / 2, ops, tag);
     });
   }
 
@@ -2066,6 +2071,8 @@ class BatchPipeline {
     std::vector<std::array<double, 5>> cf(W), cg(W);
     std::vector<double> al(W, 1.0), ga(W, 0.0);
     auto cs = [&](int w, int p) { return std::ldexp(1.0, -p * sel_s_[w]); };
+    // the Pade and solve products: 5 slices, or the mixed form's count
+    gS_ = form_ == 1 ? pade_S_ : kS;
     // m = 9: A8 = A4 A4 -> T2
     tag_ = kTagPade;
     product(st, r, m9, kA4, kA4, 1.0, -1, 0.0, 0.0, kT2, true);
@@ -2143,6 +2150,7 @@ class BatchPipeline {
     symmetrize(st, r, all, kA4);
     symmetrize(st, r, all, kA2);
 
+    gS_ = kS;
     // ---- squarings in I + E form: E = R - I, E <- 2E + E^2
     for (int w = 0; w < W; ++w) cf[w] = {1.0, 0.0, 0.0, 0.0, -1.0};
     const int m_a4[4] = {kA4, -1, -1, -1};
@@ -2686,7 +2694,7 @@ void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, voi
   p->set_profile(o.profile);
   p->set_timeout(o.timeout_ms);
   p->set_inject_stall(o.inject_stall);
-  p->set_form(o.form == FX_FORM_MIXED ? 1 : 0, o.sq_n4, o.sq_n3);
+  p->set_form(o.form == FX_FORM_MIXED ? 1 : 0, o.sq_n4, o.sq_n3, o.pade_slices);
   p->set_drift(o.drift);
   p->run(x, p0, p1, u, s);
 }
@@ -2722,6 +2730,7 @@ struct fx_batch {
   std::vector<void*> h_in;   // device staging of host runs (X, psi0, psi per walk)
   fx::HostStage stage;       // page-locked chunks for the copies of the host matrices
   int sq_n4 = fx::kMixedN4, sq_n3 = fx::kMixedN3;   // mixed-form slice schedule
+  int pade_slices = fx::kMixedPade;
   std::string last_error;
 };
 
@@ -2857,15 +2866,21 @@ int fx_batch_set_option(fx_batch_handle b, int key, double value) {
     case FX_BATCH_OPT_FORM:
       if (value != FX_FORM_PLAIN && value != FX_FORM_MIXED)
         return bfail(b, fx::Error{FX_ERR_VALUE, "batch form must be FX_FORM_PLAIN or FX_FORM_MIXED"});
-      b->p->set_form(value == FX_FORM_MIXED ? 1 : 0, b->sq_n4, b->sq_n3);
+      b->p->set_form(value == FX_FORM_MIXED ? 1 : 0, b->sq_n4, b->sq_n3, b->pade_slices);
       return FX_OK;
     case FX_BATCH_OPT_SQ_N4:
     case FX_BATCH_OPT_SQ_N3: {
       if (value < 0 || value > 64) return bfail(b, fx::Error{FX_ERR_VALUE, "squaring counts must be 0..64"});
       (key == FX_BATCH_OPT_SQ_N4 ? b->sq_n4 : b->sq_n3) = (int)value;
-      b->p->set_form(b->p->form(), b->sq_n4, b->sq_n3);
+      b->p->set_form(b->p->form(), b->sq_n4, b->sq_n3, b->pade_slices);
       return FX_OK;
     }
+    case FX_BATCH_OPT_PADE_SLICES:
+      if (value != 3 && value != 4 && value != 5)
+        return bfail(b, fx::Error{FX_ERR_VALUE, "Pade slice count must be 3, 4 or 5"});
+      b->pade_slices = (int)value;
+      b->p->set_form(b->p->form(), b->sq_n4, b->sq_n3, b->pade_slices);
+      return FX_OK;
     case FX_BATCH_OPT_DRIFT: b->p->set_drift(value != 0.0); return FX_OK;
   }
   return bfail(b, fx::Error{FX_ERR_VALUE, "unknown batch option"});

@@ -90,6 +90,7 @@ struct RunOpts {
   int selector;      // (m, s) selection of the grouped path: 0 plain, 1 certified, 2 learned
   int inject_stall;  // diagnostics of the grouped path: product launch that skips a K step (-1 off)
   int sq_n4, sq_n3;  // mixed form of the grouped path: squarings at 4 and at 3 slices
+  int pade_slices;   // mixed form of the grouped path: slices of the Pade and solve products
   int drift;         // diagnostics of the grouped path: unitarity residual after every squaring
 };
 
@@ -1044,7 +1045,7 @@ struct fx_engine {
   fx::BatchPipeline* grouped = nullptr;   // grouped pipeline for walk generators (lazy)
   void* check_buf = nullptr;              // input statistics of the routing check
   fx::HostStage stage;                    // page-locked chunks for copies of host buffers
-  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0, 0, -1, fx::kMixedN4, fx::kMixedN3, 0};
+  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0, 0, -1, fx::kMixedN4, fx::kMixedN3, fx::kMixedPade, 0};
   fx_stats stats{};
   std::string last_error;
 };
@@ -1136,6 +1137,7 @@ void run_device(fx_handle h, const void* dA, void* dU, const void* dpsi0, void* 
     po.form = h->opts.form;
     po.sq_n4 = h->opts.sq_n4;
     po.sq_n3 = h->opts.sq_n3;
+    po.pade_slices = h->opts.pade_slices;
     po.drift = h->opts.drift != 0;
     fx::batch_pipeline_run(h->grouped, dA, dpsi0, dpsi, dU, po, s);
     FX_CUDA(cudaEventRecord(h->ev1, s));
@@ -1299,6 +1301,10 @@ int fx_set_option(fx_handle h, int key, double value) {
       (key == FX_OPT_SQ_N4 ? h->opts.sq_n4 : h->opts.sq_n3) = v;
       return FX_OK;
     case FX_OPT_DRIFT: h->opts.drift = v != 0; return FX_OK;
+    case FX_OPT_PADE_SLICES:
+      if (v != 3 && v != 4 && v != 5) return fail(h, fx::Error{FX_ERR_VALUE, "Pade slice count must be 3, 4 or 5"});
+      h->opts.pade_slices = v;
+      return FX_OK;
   }
   return fail(h, fx::Error{FX_ERR_VALUE, "unknown option"});
 }

@@ -248,10 +248,11 @@ struct PipeOpts {
                              // operand loads of its first K step, so that the bounded waits run out
   int form = FX_FORM_PLAIN;  // FX_FORM_MIXED: two-product squarings with the slice schedule below
   int sq_n4 = 0, sq_n3 = 0;  // mixed form: the last sq_n3 squarings at 3 slices, the sq_n4 before at 4
+  int pade_slices = 5;       // mixed form: slices of the Pade and solve products
   bool drift = false;        // diagnostics: unitarity residual after every squaring
 };
 // Default slice schedule of the mixed form (see fx_batch.cu, BatchPipeline::sq_slices).
-constexpr int kMixedN4 = 4, kMixedN3 = 1;
+constexpr int kMixedN4 = 4, kMixedN3 = 1, kMixedPade = 5;
 void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU,
                         const PipeOpts& o, cudaStream_t s);
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st);

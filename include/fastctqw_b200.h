@@ -101,10 +101,12 @@ enum fx_option {
                              3-slice ones run at 4 slices (default 4)                  */
   FX_OPT_SQ_N3 = 13,      /* mixed form, walk generators: how many of the last squarings run
                              at 3 slices (default 1)                                   */
-  FX_OPT_DRIFT = 14       /* diagnostics (walk generators): 1 records the unitarity residual
+  FX_OPT_DRIFT = 14,      /* diagnostics (walk generators): 1 records the unitarity residual
                              ||U_k^H U_k - I||_F / sqrt(n) after every squaring k = 0..s
                              (fx_unitarity_drift), at the cost of two extra products per
                              squaring                                                  */
+  FX_OPT_PADE_SLICES = 15 /* mixed form, walk generators: int8 slices of the Pade and solve
+                             products (5 default, 4 or 3)                              */
 };
 
 /* What the last run did. */
@@ -239,7 +241,9 @@ enum fx_batch_option {
   FX_BATCH_OPT_FORM = 10,        /* FX_FORM_PLAIN (default) or FX_FORM_MIXED (as FX_OPT_FORM)     */
   FX_BATCH_OPT_SQ_N4 = 11,       /* mixed form: squarings at 4 slices (as FX_OPT_SQ_N4)          */
   FX_BATCH_OPT_SQ_N3 = 12,       /* mixed form: last squarings at 3 slices (as FX_OPT_SQ_N3)     */
-  FX_BATCH_OPT_DRIFT = 13        /* diagnostics: per-squaring unitarity residual (as FX_OPT_DRIFT) */
+  FX_BATCH_OPT_DRIFT = 13,       /* diagnostics: per-squaring unitarity residual (as FX_OPT_DRIFT) */
+  FX_BATCH_OPT_PADE_SLICES = 14  /* mixed form: slices of the Pade and solve products (as        */
+                                 /* FX_OPT_PADE_SLICES)                                         */
 };
 /* count walks of sizes n[0..count); dtype FX_C64 or FX_C128 (of X, psi0 and psi). */
 int fx_batch_create(size_t count, const int64_t* n, int dtype, fx_batch_handle* out);
