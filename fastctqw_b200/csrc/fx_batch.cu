@@ -2071,11 +2071,13 @@ class BatchPipeline {
     std::vector<std::array<double, 5>> cf(W), cg(W);
     std::vector<double> al(W, 1.0), ga(W, 0.0);
     auto cs = [&](int w, int p) { return std::ldexp(1.0, -p * sel_s_[w]); };
-    // the Pade and solve products: 5 slices, or the mixed form's count
+    // the Pade and solve products: 5 slices, or the mixed form's count; the mixed form also takes
+    // the (dominant) diagonals of the Pade products' operands out of their slices
     gS_ = form_ == 1 ? pade_S_ : kS;
+    const bool psplit = form_ == 1;
     // m = 9: A8 = A4 A4 -> T2
     tag_ = kTagPade;
-    product(st, r, m9, kA4, kA4, 1.0, -1, 0.0, 0.0, kT2, true);
+    product(st, r, m9, kA4, kA4, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, psplit);
     // m = 13: T1 = b13 A6 + b11 A4 + b9 A2 (scaled), T2 = A6 T1 (scaled)
     for (int w : m13) {
       const auto b = pade_coeffs(13);
@@ -2084,7 +2086,7 @@ class BatchPipeline {
     }
     const int m_642[4] = {kA6, kA4, kA2, -1};
     combo(st, r, m13, kT1, m_642, cf);
-    product(st, r, m13, kA6, kT1, 1.0, -1, 0.0, 0.0, kT2, true, &al);
+    product(st, r, m13, kA6, kT1, 1.0, -1, 0.0, 0.0, kT2, true, &al, nullptr, psplit);
     // odd part: T1 = [T2] + b7 A6 + b5 A4 + b3 A2 + b1 I  (T2 = W1 for m = 13, A8 for m = 9)
     const int m_t2642[4] = {kT2, kA6, kA4, kA2};
     for (int w = 0; w < W; ++w) {
@@ -2101,7 +2103,7 @@ class BatchPipeline {
     }
     combo(st, r, all, kT1, m_t2642, cf);
     // U = i W with W = c Yim T1
-    product(st, r, all, kY, kT1, 1.0, -1, 0.0, 0.0, kW, true, &al);
+    product(st, r, all, kY, kT1, 1.0, -1, 0.0, 0.0, kW, true, &al, nullptr, psplit);
     // even part.  m = 13: T1 = b12 A6 + b10 A4 + b8 A2, T2 = b6 A6 + b4 A4 + b2 A2,
     // V = A6 T1 + T2 + b0 I.  m < 13: V = [b8 A8] + b6 A6 + b4 A4 + b2 A2 + b0 I.
     for (int w : m13) {
@@ -2122,7 +2124,7 @@ class BatchPipeline {
       else cf[w] = {0.0, 0.0, 0.0, b[2] * cs(w, 2), b[0]};
     }
     combo(st, r, mlt13, kV, m_t2642, cf);
-    product(st, r, m13, kA6, kT1, 1.0, kT2, 1.0, 0.0, kV, true, &al, &ga);
+    product(st, r, m13, kA6, kT1, 1.0, kT2, 1.0, 0.0, kV, true, &al, &ga, psplit);
 
     // ---- solve: G = V^2 + W^2 = L L^T, P2 = (V + iW)^2, R = G^-1 P2
     // V ~ b_0 I once scaled: these products and the complex ones below split the diagonals off
@@ -2171,7 +2173,7 @@ class BatchPipeline {
         if (sel_s_[w] > k) act.push_back(w);
       if (drift_) drift(st, r, act, er, ei, std::vector<int>(W, std::min(k, kDriftMax - 1)));
       if (form_ == 1)
-        square2(st, r, act, er, ei, tr, ti, k);
+        square3(st, r, act, er, ei, tr, ti, k);
       else
         square(st, r, act, er, ei, tr, ti);
       for (int w : act) {
@@ -2349,14 +2351,20 @@ class BatchPipeline {
     }
     return tiles;
   }
-  // Mixed-form squaring E <- 2E + E^2 of the listed walks, E = Er + i Ei symmetric with commuting
-  // planes (a function of the walk's real symmetric generator): Re = 2 Er + (Er + Ei)(Er - Ei),
-  // Im = 2 Ei + 2 Er Ei, two real products instead of four.  The products compute the upper
-  // triangle and mirror it.  In exact arithmetic Er and Ei commute; the commutator that the
-  // rounded iterates carry is of the size of the products' own rounding error and enters the
-  // result like it.  Walks are grouped by arena pair and by their slice count for this squaring.
-  void square2(Staging& st, Rec& r, const std::vector<int>& act, const std::vector<int>& er,
+  // Mixed-form squaring E <- 2E + E^2 of the listed walks, E = Er + i Ei complex symmetric, as
+  // three real products that are symmetric for any symmetric operands (squares of one matrix):
+  //   t1 = Er Er, t2 = Ei Ei, t3 = (Er + Ei)(Er + Ei),
+  //   Re = 2 Er + t1 - t2,  Im = 2 Ei + t3 - t1 - t2  (= 2 Ei + Er Ei + Ei Er),
+  // three products instead of four, and no dependence on Er and Ei commuting (they do in exact
+  // arithmetic, but not the rounded iterates: a form whose products are symmetric only for
+  // commuting operands, such as (Er + Ei)(Er - Ei), turns that commutator into an error that
+  // doubles with every squaring).  Every product takes the diagonal out of its int8 slices and
+  // adds it in FP64 (diagonal split): the iterates' rows are dominated by their diagonal, which
+  // would otherwise set the row exponent and cost the off-diagonal entries as many bits.
+  // Scratch arenas (free during the squarings): V = Er + Ei, Y = t1, A6 = t2, W = t3.
+  void square3(Staging& st, Rec& r, const std::vector<int>& act, const std::vector<int>& er,
                const std::vector<int>& ei, const std::vector<int>& tr, const std::vector<int>& ti, int k) {
+    const int W = count();
     for (int pa : {kA4, kT1}) {
       for (int S : {5, 4, 3}) {
         std::vector<int> l;
@@ -2364,67 +2372,20 @@ class BatchPipeline {
           if (er[w] == pa && sq_slices(w, k) == S) l.push_back(w);
         if (l.empty()) continue;
         const int re = er[l[0]], im = ei[l[0]], ore = tr[l[0]], oim = ti[l[0]];
-        std::vector<GSlab> sa;
-        std::vector<GProblem> prr, pri;
-        for (int w : l) {
-          const BWalk& b = walks_[w];
-          sa.push_back(GSlab{A(re) + b.off, A(im) + b.off, b.np, b.np, b.np, (int)b.row0, kNoDiag});
-          GProblem p{};
-          p.a_row0 = p.b_row0 = (int)b.row0;
-          p.M = p.N = p.K = b.np;
-          p.sym = 1;
-          p.alpha = 1.0;
-          p.beta = 2.0;
-          p.ldc = p.ldd = b.np;
-          p.C = A(re) + b.off;
-          p.D = A(ore) + b.off;
-          prr.push_back(p);
-          p.alpha = 2.0;
-          p.C = A(im) + b.off;
-          p.D = A(oim) + b.off;
-          pri.push_back(p);
-        }
-        std::vector<GTile> tiles = sym_tiles(prr, i8_tile_bn(S));
-        order_tiles(tiles, prr);
-        std::sort(sa.begin(), sa.end(), [](const GSlab& x, const GSlab& y) { return x.row0 < y.row0; });
-        const size_t o_sa = st.put(sa), o_r = st.put(prr), o_i = st.put(pri), o_t = st.put(tiles);
-        const int nsa = (int)sa.size(), nt = (int)tiles.size();
-        const int64_t kw = widest(sa);
-        const double ops = tile_ops(tiles, 1, S);
-        r.launches += 3;
-        r.gemms += 2;
-        r.ops.push_back([=]() {
-          SqSlices out{};
-          for (int q = 0; q < S; ++q) {
-            out.p[0][q] = slice_plane(0, q);
-            out.p[1][q] = slice_plane(0, q) + (size_t)rows_ * pitch_;
-            out.p[2][q] = slice_plane(1, q);
-            out.p[3][q] = slice_plane(2, q);
-          }
-          out.exp_sd = aexp();
-          out.exp_ri = aexp() + rows_;
-          out.ld = pitch_;
-          launch_slice_rows_sumdiff_grouped(S, dev<GSlab>(o_sa), nsa, rows_, out, stream_, kw);
-          I8Term t{};
-          for (int q = 0; q < S; ++q) {
-            t.a[q] = out.p[0][q];
-            t.b[q] = out.p[1][q];
-          }
-          size_t pi = prof_begin();
-          launch_gemm_i8_grouped<double>(S, &t, 1, pitch_, rows_, rows_, aexp(), aexp(), dev<GProblem>(o_r),
-                                         dev<GTile>(o_t), nt, (int*)err_.p, timeout_ms_, stream_, nullptr, nullptr,
-                                         next_skip());
-          prof_end(pi, ops * S * (S + 1) / 2, ops, kTagSquare);
-          for (int q = 0; q < S; ++q) {
-            t.a[q] = out.p[2][q];
-            t.b[q] = out.p[3][q];
-          }
-          pi = prof_begin();
-          launch_gemm_i8_grouped<double>(S, &t, 1, pitch_, rows_, rows_, aexp() + rows_, aexp() + rows_,
-                                         dev<GProblem>(o_i), dev<GTile>(o_t), nt, (int*)err_.p, timeout_ms_, stream_,
-                                         nullptr, nullptr, next_skip());
-          prof_end(pi, ops * S * (S + 1) / 2, ops, kTagSquare);
-        });
+        std::vector<std::array<double, 5>> cf(W, {1.0, 1.0, 0.0, 0.0, 0.0});
+        const int m_sum[4] = {re, im, -1, -1};
+        combo(st, r, l, kV, m_sum, cf);
+        gS_ = S;
+        product(st, r, l, re, re, 1.0, -1, 0.0, 0.0, kY, true, nullptr, nullptr, true);    // t1
+        product(st, r, l, im, im, 1.0, -1, 0.0, 0.0, kA6, true, nullptr, nullptr, true);   // t2
+        product(st, r, l, kV, kV, 1.0, -1, 0.0, 0.0, kW, true, nullptr, nullptr, true);    // t3
+        gS_ = kS;
+        const int m_re[4] = {re, kY, kA6, -1};
+        std::fill(cf.begin(), cf.end(), std::array<double, 5>{2.0, 1.0, -1.0, 0.0, 0.0});
+        combo(st, r, l, ore, m_re, cf);
+        const int m_im[4] = {im, kW, kY, kA6};
+        std::fill(cf.begin(), cf.end(), std::array<double, 5>{2.0, 1.0, -1.0, -1.0, 0.0});
+        combo(st, r, l, oim, m_im, cf);
       }
     }
   }

@@ -728,11 +728,7 @@ __global__ void __launch_bounds__(256, 2) k_slice_rows_grouped(const GSlab* slab
   slice_row<TI, NEG>(re, im, sb.K, S, out, row, lane, (dcol >= 0 && dcol < sb.K) ? dcol : -1);
 }
 
-// ---- slicing for the two-product squaring of a symmetric complex iterate E = Er + i Ei whose
-// planes commute (E a function of one real symmetric matrix): Re(E^2) = (Er + Ei)(Er - Ei) and
-// Im(E^2) = 2 Er Ei.  One pass over the two FP64 rows cuts four operands into S digits each:
-// (Er + Ei) and (Er - Ei) with the row exponent of |Er| + |Ei| (the larger of the two), and Er,
-// Ei with the exponent of max(|Er|, |Ei|).  Digits as in slice_row (top down, round half even).
+// ---- digit helpers of the shared-memory slicing kernel below (the digits of slice_row).
 __device__ __forceinline__ void cut_digits(double xs, int S, int d[kMaxSlices]) {
   double r = rint(xs);
 #pragma unroll
@@ -762,88 +758,14 @@ __device__ __forceinline__ double scale_for(int S, int e, bool& one) {
   return one ? ldexp(1.0, sh) : 0.0;
 }
 
-__device__ void slice_row_sumdiff(const double* rre, const double* rim, int64_t K, int S, const SqSlices& out,
-                                  int64_t orow, int lane) {
-  const bool vec = ((reinterpret_cast<uintptr_t>(rre) | reinterpret_cast<uintptr_t>(rim)) & 15) == 0;
-  double m1 = 0.0, m2 = 0.0;
-#pragma unroll 4
-  for (int64_t k0 = (int64_t)lane * 4; k0 < K; k0 += 128) {
-    double a[4], b[4];
-    load4<double>(rre, k0, K, vec, a);
-    load4<double>(rim, k0, K, vec, b);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      m1 = fmax(m1, fabs(a[j]) + fabs(b[j]));
-      m2 = fmax(m2, fmax(fabs(a[j]), fabs(b[j])));
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
-    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
-  }
-  const int e1 = row_exponent(m1), e2 = row_exponent(m2);
-  if (lane == 0) {
-    out.exp_sd[orow] = e1;
-    out.exp_ri[orow] = e2;
-  }
-  bool one1, one2;
-  const double sc1 = scale_for(S, e1, one1), sc2 = scale_for(S, e2, one2);
-  for (int64_t k0 = (int64_t)lane * 4; k0 < K; k0 += 128) {
-    double a[4], b[4];
-    load4<double>(rre, k0, K, vec, a);
-    load4<double>(rim, k0, K, vec, b);
-    uint32_t pk[4][kMaxSlices] = {};
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const double v[4] = {a[j] + b[j], a[j] - b[j], a[j], b[j]};
-#pragma unroll
-      for (int o = 0; o < 4; ++o) {
-        const bool one = o < 2 ? one1 : one2;
-        const int e = o < 2 ? e1 : e2;
-        const double xs = one ? v[o] * (o < 2 ? sc1 : sc2) : ldexp(ldexp(v[o], -e), 7 * S);
-        int d[kMaxSlices];
-        cut_digits(xs, S, d);
-#pragma unroll
-        for (int q = 0; q < kMaxSlices; ++q)
-          if (q < S) pk[o][q] |= ((uint32_t)(uint8_t)(int8_t)d[q]) << (8 * j);
-      }
-    }
-#pragma unroll
-    for (int o = 0; o < 4; ++o)
-#pragma unroll
-      for (int q = 0; q < kMaxSlices; ++q)
-        if (q < S) *reinterpret_cast<uint32_t*>(out.p[o][q] + orow * out.ld + k0) = pk[o][q];
-  }
-}
-
-__global__ void __launch_bounds__(256, 2)
-    k_slice_rows_sumdiff_grouped(const GSlab* slabs, int nslabs, int64_t total_rows, int S, SqSlices out) {
-  const int lane = threadIdx.x & 31;
-  const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-  if (row >= total_rows) return;
-  int lo = 0, hi = nslabs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (slabs[mid].row0 <= row) lo = mid;
-    else hi = mid - 1;
-  }
-  const GSlab sb = slabs[lo];
-  const int64_t local = row - sb.row0;
-  if (local < 0 || local >= sb.rows || !sb.im) return;
-  slice_row_sumdiff((const double*)sb.re + local * sb.ld, (const double*)sb.im + local * sb.ld, sb.K, S, out, row,
-                    lane);
-}
-
 // ---- grouped slicing with the row in shared memory: one CTA per row (grid-stride over the
 // stacked rows).  The row's planes are read from HBM once, with 16-byte loads, into shared
 // memory while the row maximum is taken on the way; the digits are then cut from shared memory
 // and written as packed 4-byte words (consecutive threads, consecutive words).  The warp-per-row
 // kernels above read every row twice (the maximum first), and with many rows in flight the
 // second read misses L2.  Used when the launch's widest row fits the shared memory.
-// Modes: SD = false -- re (and im) with one shared exponent (and -im when NEG), the diagonal of
-// a single-plane slab optionally left out; SD = true -- the four operands of the two-product
-// squaring (slice_row_sumdiff).
+// re (and im) share one row exponent (with -im too when NEG); the diagonal of a single-plane
+// slab is optionally left out (the diagonal split).
 constexpr int kSmemSliceThreads = 512;
 __device__ __forceinline__ double block_max(double v, double* red) {
 #pragma unroll
@@ -856,10 +778,9 @@ __device__ __forceinline__ double block_max(double v, double* red) {
   for (int i = 0; i < nw; ++i) m = fmax(m, red[i]);
   return m;
 }
-template <bool NEG, bool SD>
+template <bool NEG>
 __global__ void __launch_bounds__(kSmemSliceThreads, 1)
-    k_slice_rows_smem(const GSlab* slabs, int nslabs, int64_t total_rows, int64_t kmax, int S, I8Slices out,
-                      SqSlices sq) {
+    k_slice_rows_smem(const GSlab* slabs, int nslabs, int64_t total_rows, int64_t kmax, int S, I8Slices out) {
   extern __shared__ __align__(16) double srow[];   // [2][kmax]
   __shared__ double red[kSmemSliceThreads / 32];
   for (int64_t row = blockIdx.x; row < total_rows; row += gridDim.x) {
@@ -875,61 +796,46 @@ __global__ void __launch_bounds__(kSmemSliceThreads, 1)
     const int64_t K = sb.K;
     const double* re = (const double*)sb.re + local * sb.ld;
     const double* im = sb.im ? (const double*)sb.im + local * sb.ld : nullptr;
-    if (SD && !im) continue;
-    const int64_t dcol = (!SD && sb.diag0 != kNoDiag && out.dg && !im) ? local + sb.diag0 : -1;
+    const int64_t dcol = (sb.diag0 != kNoDiag && out.dg && !im) ? local + sb.diag0 : -1;
     const bool has_d = dcol >= 0 && dcol < K;
     double* s0 = srow;
     double* s1 = srow + kmax;
     const bool vec = ((reinterpret_cast<uintptr_t>(re) | reinterpret_cast<uintptr_t>(im)) & 15) == 0 && (K & 1) == 0;
-    double m1 = 0.0, m2 = 0.0;
+    double m1 = 0.0;
     if (vec) {
       for (int64_t k = 2 * (int64_t)threadIdx.x; k < K; k += 2 * blockDim.x) {
         double2 a = __ldcs(reinterpret_cast<const double2*>(re + k));
         if (has_d && k == dcol) a.x = 0.0;
         if (has_d && k + 1 == dcol) a.y = 0.0;
         *reinterpret_cast<double2*>(s0 + k) = a;
+        m1 = fmax(m1, fmax(fabs(a.x), fabs(a.y)));
         if (im) {
           const double2 b = __ldcs(reinterpret_cast<const double2*>(im + k));
           *reinterpret_cast<double2*>(s1 + k) = b;
-          if (SD) {
-            m1 = fmax(m1, fmax(fabs(a.x) + fabs(b.x), fabs(a.y) + fabs(b.y)));
-            m2 = fmax(m2, fmax(fmax(fabs(a.x), fabs(b.x)), fmax(fabs(a.y), fabs(b.y))));
-          } else {
-            m1 = fmax(m1, fmax(fmax(fabs(a.x), fabs(b.x)), fmax(fabs(a.y), fabs(b.y))));
-          }
-        } else {
-          m1 = fmax(m1, fmax(fabs(a.x), fabs(a.y)));
+          m1 = fmax(m1, fmax(fabs(b.x), fabs(b.y)));
         }
       }
     } else {
       for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
         const double a = (has_d && k == dcol) ? 0.0 : re[k];
         s0[k] = a;
+        m1 = fmax(m1, fabs(a));
         if (im) {
           const double b = im[k];
           s1[k] = b;
-          m1 = fmax(m1, SD ? fabs(a) + fabs(b) : fmax(fabs(a), fabs(b)));
-          if (SD) m2 = fmax(m2, fmax(fabs(a), fabs(b)));
-        } else {
-          m1 = fmax(m1, fabs(a));
+          m1 = fmax(m1, fabs(b));
         }
       }
     }
-    m1 = block_max(m1, red);
-    if (SD) m2 = block_max(m2, red);   // also orders the shared row before the digit pass
-    const int e1 = row_exponent(m1), e2 = SD ? row_exponent(m2) : 0;
+    m1 = block_max(m1, red);   // also orders the shared row before the digit pass
+    const int e1 = row_exponent(m1);
     if (threadIdx.x == 0) {
-      if (SD) {
-        sq.exp_sd[row] = e1;
-        sq.exp_ri[row] = e2;
-      } else {
-        out.exp[row] = e1;
-        if (has_d) out.dg[row] = re[dcol];
-      }
+      out.exp[row] = e1;
+      if (has_d) out.dg[row] = re[dcol];
     }
-    bool one1, one2 = true;
-    const double sc1 = scale_for(S, e1, one1), sc2 = SD ? scale_for(S, e2, one2) : 0.0;
-    const int64_t ld = SD ? sq.ld : out.ld;
+    bool one1;
+    const double sc1 = scale_for(S, e1, one1);
+    const int64_t ld = out.ld;
     for (int64_t k0 = 4 * (int64_t)threadIdx.x; k0 < K; k0 += 4 * blockDim.x) {
       double a[4], b[4];
 #pragma unroll
@@ -937,53 +843,29 @@ __global__ void __launch_bounds__(kSmemSliceThreads, 1)
         a[j] = k0 + j < K ? s0[k0 + j] : 0.0;
         b[j] = (im && k0 + j < K) ? s1[k0 + j] : 0.0;
       }
-      if (SD) {
-        uint32_t pk[4][kMaxSlices] = {};
+#pragma unroll
+      for (int plane = 0; plane < 2; ++plane) {
+        if (plane == 1 && !im) continue;
+        const double* x = plane == 0 ? a : b;
+        uint32_t pk[kMaxSlices] = {}, pn[kMaxSlices] = {};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const double v[4] = {a[j] + b[j], a[j] - b[j], a[j], b[j]};
-#pragma unroll
-          for (int o = 0; o < 4; ++o) {
-            const bool one = o < 2 ? one1 : one2;
-            const int e = o < 2 ? e1 : e2;
-            const double xs = one ? v[o] * (o < 2 ? sc1 : sc2) : ldexp(ldexp(v[o], -e), 7 * S);
-            int d[kMaxSlices];
-            cut_digits(xs, S, d);
-#pragma unroll
-            for (int q = 0; q < kMaxSlices; ++q)
-              if (q < S) pk[o][q] |= ((uint32_t)(uint8_t)(int8_t)d[q]) << (8 * j);
-          }
-        }
-#pragma unroll
-        for (int o = 0; o < 4; ++o)
+          const double xs = one1 ? x[j] * sc1 : ldexp(ldexp(x[j], -e1), 7 * S);
+          int d[kMaxSlices];
+          cut_digits(xs, S, d);
 #pragma unroll
           for (int q = 0; q < kMaxSlices; ++q)
-            if (q < S) *reinterpret_cast<uint32_t*>(sq.p[o][q] + row * ld + k0) = pk[o][q];
-      } else {
+            if (q < S) {
+              pk[q] |= ((uint32_t)(uint8_t)(int8_t)d[q]) << (8 * j);
+              if (NEG && plane == 1) pn[q] |= ((uint32_t)(uint8_t)(int8_t)(-d[q])) << (8 * j);
+            }
+        }
 #pragma unroll
-        for (int plane = 0; plane < 2; ++plane) {
-          if (plane == 1 && !im) continue;
-          const double* x = plane == 0 ? a : b;
-          uint32_t pk[kMaxSlices] = {}, pn[kMaxSlices] = {};
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const double xs = one1 ? x[j] * sc1 : ldexp(ldexp(x[j], -e1), 7 * S);
-            int d[kMaxSlices];
-            cut_digits(xs, S, d);
-#pragma unroll
-            for (int q = 0; q < kMaxSlices; ++q)
-              if (q < S) {
-                pk[q] |= ((uint32_t)(uint8_t)(int8_t)d[q]) << (8 * j);
-                if (NEG && plane == 1) pn[q] |= ((uint32_t)(uint8_t)(int8_t)(-d[q])) << (8 * j);
-              }
-          }
-#pragma unroll
-          for (int q = 0; q < kMaxSlices; ++q) {
-            if (q >= S) continue;
-            int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
-            if (dst) *reinterpret_cast<uint32_t*>(dst + row * ld + k0) = pk[q];
-            if (NEG && plane == 1 && out.neg_im[q]) *reinterpret_cast<uint32_t*>(out.neg_im[q] + row * ld + k0) = pn[q];
-          }
+        for (int q = 0; q < kMaxSlices; ++q) {
+          if (q >= S) continue;
+          int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
+          if (dst) *reinterpret_cast<uint32_t*>(dst + row * ld + k0) = pk[q];
+          if (NEG && plane == 1 && out.neg_im[q]) *reinterpret_cast<uint32_t*>(out.neg_im[q] + row * ld + k0) = pn[q];
         }
       }
     }
@@ -1071,20 +953,19 @@ void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t to
   if (std::is_same<TI, double>::value && kmax > 0 && kmax % 4 == 0 && sm <= kSmemSliceBytes) {
     static bool attr = false;
     if (!attr) {
-      FX_CUDA(cudaFuncSetAttribute(k_slice_rows_smem<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      FX_CUDA(cudaFuncSetAttribute(k_slice_rows_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)kSmemSliceBytes));
-      FX_CUDA(cudaFuncSetAttribute(k_slice_rows_smem<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      FX_CUDA(cudaFuncSetAttribute(k_slice_rows_smem<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)kSmemSliceBytes));
       attr = true;
     }
     (void)two_planes;
-    SqSlices none{};
     if (want_neg_im)
-      k_slice_rows_smem<true, false><<<smem_slice_grid(total_rows), kSmemSliceThreads, sm, s>>>(
-          slabs, nslabs, total_rows, kmax, S, out, none);
+      k_slice_rows_smem<true><<<smem_slice_grid(total_rows), kSmemSliceThreads, sm, s>>>(slabs, nslabs, total_rows,
+                                                                                           kmax, S, out);
     else
-      k_slice_rows_smem<false, false><<<smem_slice_grid(total_rows), kSmemSliceThreads, sm, s>>>(
-          slabs, nslabs, total_rows, kmax, S, out, none);
+      k_slice_rows_smem<false><<<smem_slice_grid(total_rows), kSmemSliceThreads, sm, s>>>(slabs, nslabs, total_rows,
+                                                                                            kmax, S, out);
     FX_LAUNCH_CHECK();
     return;
   }
@@ -1099,28 +980,6 @@ template void launch_slice_rows_grouped<float>(int, const GSlab*, int, int64_t, 
 template void launch_slice_rows_grouped<double>(int, const GSlab*, int, int64_t, I8Slices, bool, cudaStream_t,
                                                 int64_t, bool);
 
-void launch_slice_rows_sumdiff_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, SqSlices out,
-                                       cudaStream_t s, int64_t kmax) {
-  if (S < 3 || S > kMaxSlices) throw Error{FX_ERR_VALUE, "slice count must be 3, 4 or 5"};
-  if (out.ld % 16 != 0) throw Error{FX_ERR_VALUE, "grouped slice: pitch must be a multiple of 16"};
-  if (nslabs <= 0 || total_rows <= 0) return;
-  const int64_t sm = (int64_t)sizeof(double) * 2 * kmax;
-  if (kmax > 0 && kmax % 4 == 0 && sm <= kSmemSliceBytes) {
-    static bool attr = false;
-    if (!attr) {
-      FX_CUDA(cudaFuncSetAttribute(k_slice_rows_smem<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)kSmemSliceBytes));
-      attr = true;
-    }
-    I8Slices none{};
-    k_slice_rows_smem<false, true><<<smem_slice_grid(total_rows), kSmemSliceThreads, sm, s>>>(
-        slabs, nslabs, total_rows, kmax, S, none, out);
-    FX_LAUNCH_CHECK();
-    return;
-  }
-  k_slice_rows_sumdiff_grouped<<<cdiv(total_rows, 8), 256, 0, s>>>(slabs, nslabs, total_rows, S, out);
-  FX_LAUNCH_CHECK();
-}
 
 namespace {
 template <int S, typename TO>

@@ -306,17 +306,6 @@ constexpr int kNoDiag = -(1 << 30);
 template <typename TI>
 void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, I8Slices out,
                                bool want_neg_im, cudaStream_t s, int64_t kmax = 0, bool two_planes = true);
-// Slices of the two-product squaring (launch_slice_rows_sumdiff_grouped): p[0] = Er + Ei,
-// p[1] = Er - Ei (row exponents exp_sd), p[2] = Er, p[3] = Ei (row exponents exp_ri), S digits
-// each, stacked rows of pitch ld.
-struct SqSlices {
-  int8_t* p[4][5];
-  int* exp_sd;
-  int* exp_ri;
-  int64_t ld;
-};
-void launch_slice_rows_sumdiff_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, SqSlices out,
-                                       cudaStream_t s, int64_t kmax = 0);
 // In place A <- (A + A^T) / 2 of an n x n plane (exact symmetry of a result known to be
 // symmetric in exact arithmetic).
 template <typename T>
