@@ -351,12 +351,13 @@ def bench_batch(args, dev):
         return ev0.elapsed_time(ev1) / reps
 
     plain_batch_ms = None
-    if args.selector != "plain":
+    if args.selector != "plain" or args.form != "plain":
         bpl = WalkBatch(ns, autotune=not args.no_autotune)
         plain_batch_ms = timed(bpl)
         _, s_plain = bpl.selection()
         bpl.close()
-    b = WalkBatch(ns, selector=args.selector, autotune=not args.no_autotune)   # tuned in the warm-up
+    b = WalkBatch(ns, selector=args.selector, form=args.form,
+                  autotune=not args.no_autotune)   # tuned in the warm-up
     batch_ms = timed(b)
     info = b.info()
     sched = b.schedule()
@@ -403,8 +404,9 @@ def bench_batch(args, dev):
         "speedup_vs_loop": round(loop_ms / batch_ms, 2) if loop_ms else None,
         "launches_per_batch": info["launches"], "algorithmic_tflops": round(info["flops"] / (batch_ms * 1e-3) / 1e12, 1),
         "selector": args.selector,
-        "plain_selection_ms": round(plain_batch_ms, 2) if plain_batch_ms else None,
-        "plain_selection_walks_per_s": round(walks / (plain_batch_ms * 1e-3), 1) if plain_batch_ms else None,
+        "form": args.form,
+        "plain_form_ms": round(plain_batch_ms, 2) if plain_batch_ms else None,
+        "plain_form_walks_per_s": round(walks / (plain_batch_ms * 1e-3), 1) if plain_batch_ms else None,
         "squarings_chosen": int(s.sum()), "squarings_plain": int(s_plain.sum()) if plain_batch_ms else None,
         "outcomes": {int(k): int(v) for k, v in zip(*np.unique(outcome, return_counts=True))},
         "m_hist": {int(k): int(v) for k, v in zip(*np.unique(m, return_counts=True))},
@@ -431,7 +433,7 @@ def bench_batch_sharded(args, dev, rank, world):
     def runner(xs, ps):
         key = tuple(X.shape[0] for X in xs)
         if key not in cache:
-            cache[key] = WalkBatch(list(key), np.complex64, selector=args.selector)
+            cache[key] = WalkBatch(list(key), np.complex64, selector=args.selector, form=args.form)
         return cache[key].run(xs, ps)
 
     if args.selector == "learned":
@@ -531,7 +533,7 @@ def main():
     ap.add_argument("--t", type=float, default=4.5)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--form", default="plain", choices=["plain", "mixed", "simt"])
-    ap.add_argument("--selector", default="learned", choices=["plain", "certified", "learned"],
+    ap.add_argument("--selector", default="learned", choices=["plain", "certified", "estimated", "learned"],
                     help="(m, s) selection of the timed walk; the plain selection is timed beside it")
     ap.add_argument("--ref-sample-n", type=int, default=1024,
                     help="size of the small sample behind the flop-model cross-check of the reference arm")
@@ -666,11 +668,12 @@ def main():
         "stages": stages,
     }
 
-    # ---- the plain (Al-Mohy & Higham) selection on the same walk, timed the same way
+    # ---- the plain form (5-slice products, exact complex squarings) with the plain (Al-Mohy &
+    # Higham) selection on the same walk, timed the same way
     plain = None
     psi_plain = None
-    if args.selector != "plain":
-        eng.configure(selector="plain")
+    if args.selector != "plain" or args.form != "plain":
+        eng.configure(form="plain", selector="plain")
         step()
         torch.cuda.synchronize()
         reps = max(1, min(args.steps, 3))
@@ -681,9 +684,9 @@ def main():
         torch.cuda.synchronize()
         pst2 = eng.stats()
         plain = {"ms": round(ev0.elapsed_time(ev1) / reps, 3), "m": pst2["m"], "s": pst2["s"],
-                 "steps": reps}
+                 "steps": reps, "form": "plain", "selector": "plain"}
         psi_plain = dpsi.clone()
-        eng.configure(selector=args.selector)
+        eng.configure(form=args.form, selector=args.selector)
 
     # ---- accuracy of both against the FP64 eigendecomposition propagator
     accuracy = None
@@ -765,7 +768,7 @@ def main():
             "clocks": clk, "e2e": e2e, "gpu_launches": int(st["launches"]) * args.steps,
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy, "batch": batch,
             "device_setup": setup, "stress": stress,
-            "plain_selection": plain,
+            "plain_form": plain,
             "chosen_vs_plain_speedup": round(plain["ms"] / ms_per_step, 3) if plain else None,
             "algorithmic_tflops": round(st["flops"] / (ms_per_step * 1e-3) / 1e12, 2),
         }

@@ -288,7 +288,7 @@ class Engine:
         return st.as_dict()
 
     PRODUCT_STAGES = ("powers", "pade", "solve", "cholesky", "inverse", "triangular", "squarings",
-                      "diagnostics")
+                      "diagnostics", "newton")
 
     def product_profile(self) -> dict:
         """Per-stage product time of the last profiled walk-generator run (configure(profile=True)):

@@ -1011,11 +1011,20 @@ class BatchPipeline {
   // and 2 Er Ei, 5 slices except the last n4 + n3 squarings: n4 at 4 slices, then n3 at 3).
   void set_form(int form, int n4, int n3, int pade_slices = kS) {
     if (form == form_ && n4 == sq_n4_ && n3 == sq_n3_ && pade_slices == pade_S_) return;
+    const bool rerecord = form != form_ || (form == 1 && pade_slices != pade_S_);
     form_ = form;
     sq_n4_ = n4;
     sq_n3_ = n3;
     pade_S_ = pade_slices;
     key2_.clear();
+    if (rerecord) {   // phase 1's powers take the form's slice count and diagonal split
+      if (graph1_) cudaGraphExecDestroy(graph1_);
+      graph1_ = nullptr;
+      st1_ = Staging();
+      r1_ = Rec();
+      desc1_.release();
+      record_phase1();
+    }
   }
   int pade_slices() const { return pade_S_; }
   int form() const { return form_; }
@@ -1292,6 +1301,8 @@ class BatchPipeline {
       key.insert(key.end(), {(double)sel_m_[w], (double)sel_s_[w], (double)rank1_[w], mu_[w].real(),
                              mu_[w].imag(), nu_[w].real(), nu_[w].imag(), tab[W + w] ? 1.0 : 0.0,
                              tab[2 * W + w] ? 1.0 : 0.0, tab[3 * W + w] ? 1.0 : 0.0});
+      // the mixed form's Newton-Schulz solve takes its step count and scaling from these
+      if (form_ == 1) key.insert(key.end(), {rho_up_[w], rho_lan_[w]});
     }
     if (key != key2_ || profile_) {
       st2_ = Staging();
@@ -1703,9 +1714,14 @@ class BatchPipeline {
     });
     r.launches += 3;
     tag_ = kTagPowers;
-    product(st, r, all, kY, kY, -1.0, -1, 0.0, 0.0, kA2, true);
-    product(st, r, all, kA2, kA2, 1.0, -1, 0.0, 0.0, kA4, true);
-    product(st, r, all, kA4, kA2, 1.0, -1, 0.0, 0.0, kA6, true);
+    // the mixed form's slice count, with the diagonals split off (the shifted generator's rows
+    // are dominated by their diagonal, and its powers' even more)
+    gS_ = form_ == 1 ? pade_S_ : kS;
+    const bool psplit = form_ == 1;
+    product(st, r, all, kY, kY, -1.0, -1, 0.0, 0.0, kA2, true, nullptr, nullptr, psplit);
+    product(st, r, all, kA2, kA2, 1.0, -1, 0.0, 0.0, kA4, true, nullptr, nullptr, psplit);
+    product(st, r, all, kA4, kA2, 1.0, -1, 0.0, 0.0, kA6, true, nullptr, nullptr, psplit);
+    gS_ = kS;
     const int arenas[3] = {kY, kA4, kA6};
     r.ops.push_back([=]() {
       const BWalk* wk = (const BWalk*)d_walks_.p;
@@ -2140,17 +2156,21 @@ class BatchPipeline {
     combo(st, r, all, kA6, m_12, cf);                             // P2 re -> A6
     for (int w = 0; w < W; ++w) cf[w] = {2.0, 0.0, 0.0, 0.0, 0.0};
     combo(st, r, all, kY, m_a2, cf);                              // P2 im -> Y
-    tag_ = kTagCholesky;
-    cholesky(st, r, kA4);
-    transpose(st, r, all, kA4, kT1);                              // L^T -> T1
-    tag_ = kTagInverse;
-    inverse(st, r, kT1, kT2, kW, kA2);                            // X = L^-1 -> T2, X^T -> W (scratch A2)
-    // Z = P2 X^T (re -> V, im -> T1); R^T = Z X (re -> A4, im -> A2)
-    tag_ = kTagTriangular;
-    complex_by_real(st, r, all, kA6, kY, kT2, kV, kT1, 1, true);    // P2 symmetric
-    complex_by_real(st, r, all, kV, kT1, kW, kA4, kA2, 2, false);
-    symmetrize(st, r, all, kA4);
-    symmetrize(st, r, all, kA2);
+    if (form_ == 1) {
+      newton_solve(st, r, all);                                   // R re -> A4, im -> A2
+    } else {
+      tag_ = kTagCholesky;
+      cholesky(st, r, kA4);
+      transpose(st, r, all, kA4, kT1);                            // L^T -> T1
+      tag_ = kTagInverse;
+      inverse(st, r, kT1, kT2, kW, kA2);                          // X = L^-1 -> T2, X^T -> W (scratch A2)
+      // Z = P2 X^T (re -> V, im -> T1); R^T = Z X (re -> A4, im -> A2)
+      tag_ = kTagTriangular;
+      complex_by_real(st, r, all, kA6, kY, kT2, kV, kT1, 1, true);    // P2 symmetric
+      complex_by_real(st, r, all, kV, kT1, kW, kA4, kA2, 2, false);
+      symmetrize(st, r, all, kA4);
+      symmetrize(st, r, all, kA2);
+    }
 
     gS_ = kS;
     // ---- squarings in I + E form: E = R - I, E <- 2E + E^2
@@ -2332,6 +2352,82 @@ class BatchPipeline {
                                        next_skip());
         prof_end(pi, ops * kS * (kS + 1) / 2, ops, kTagSquare);
       });
+    }
+  }
+
+  // Mixed form: R = G^-1 P2 by the Newton-Schulz iteration X <- X (2I - G X) for G^-1, instead of
+  // the blocked Cholesky (79 dependent 128-wide steps at N = 10000, each a latency-bound block
+  // factorisation on one SM and short-K products).  In the eigenbasis of the walk's generator G is
+  // g(x) = |q_m(ix)|^2, x = lambda / 2^s, with q_m the Pade denominator (unnormalised coefficients,
+  // as the combinations use them); over |x| <= x_max = rho / 2^s its range [g_lo, g_hi] is taken on
+  // a fine grid on the host (rho: the rigorous bound min(||Y||_1, d4, d6), or 1.25 x the Lanczos
+  // estimate when that is smaller).  X1 = a (2I - a G), a = 2 / (g_lo + g_hi), has the residual
+  // ||I - G X1|| <= r^2, r = (g_hi - g_lo) / (g_hi + g_lo), and every step squares it: the count of
+  // steps to reach 1e-13 is fixed per walk before the launch sequence is recorded.  Every iterate
+  // is a polynomial in G (symmetric, commuting with G), so the products compute upper triangles;
+  // the fixed point attracts (the map's derivative vanishes there), so rounding does not build up.
+  // Scratch arenas: T1 / V hold the iterates, T2 = G X.
+  static double pade_denominator_sq(const std::vector<double>& b, double x) {
+    std::complex<double> acc(0.0, 0.0);
+    const std::complex<double> z(0.0, -x);   // q(ix) = sum_j b_j (-ix)^j
+    for (int j = (int)b.size() - 1; j >= 0; --j) acc = acc * z + b[j];
+    return std::norm(acc);
+  }
+  void newton_solve(Staging& st, Rec& r, const std::vector<int>& all) {
+    const int W = count();
+    tag_ = kTagNewton;
+    std::vector<int> iters(W, 0);
+    std::vector<std::array<double, 5>> cf(W);
+    for (int w = 0; w < W; ++w) {
+      const std::vector<double> b = pade_coeffs(sel_m_[w]);
+      const double rho = std::min(rho_up_[w], 1.25 * rho_lan_[w] > 0.0 ? 1.25 * rho_lan_[w] : rho_up_[w]);
+      const double xmax = std::ldexp(rho, -sel_s_[w]);
+      double glo = 1e300, ghi = 0.0;
+      for (int i = 0; i <= 512; ++i) {
+        const double g = pade_denominator_sq(b, xmax * i / 512.0);
+        glo = std::min(glo, g);
+        ghi = std::max(ghi, g);
+      }
+      ghi *= 1.0 + 1e-6;   // between the grid points
+      const double a = 2.0 / (glo + ghi);
+      double res = (ghi - glo) / (ghi + glo);
+      res *= res;   // after X1
+      int k = 0;
+      while (res > 1e-13 && k < 16) {
+        res *= res;
+        ++k;
+      }
+      iters[w] = k;
+      cf[w] = {-a * a, 0.0, 0.0, 0.0, 2.0 * a};
+    }
+    const int m_g[4] = {kA4, -1, -1, -1};
+    combo(st, r, all, kT1, m_g, cf);   // X1 = -a^2 G + 2a I
+    std::vector<int> xa(W, kT1), xb(W, kV);
+    int kmax = 0;
+    for (int w = 0; w < W; ++w) kmax = std::max(kmax, iters[w]);
+    for (int k = 0; k < kmax; ++k) {
+      std::vector<int> act;
+      for (int w = 0; w < W; ++w)
+        if (iters[w] > k) act.push_back(w);
+      for (int pa : {kT1, kV}) {
+        std::vector<int> l;
+        for (int w : act)
+          if (xa[w] == pa) l.push_back(w);
+        if (l.empty()) continue;
+        const int nx = pa == kT1 ? kV : kT1;
+        product(st, r, l, kA4, pa, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, true);   // G X
+        product(st, r, l, pa, kT2, -1.0, pa, 2.0, 0.0, nx, true, nullptr, nullptr, true);  // 2X - X G X
+      }
+      for (int w : act) std::swap(xa[w], xb[w]);
+    }
+    tag_ = kTagTriangular;
+    for (int pa : {kT1, kV}) {
+      std::vector<int> l;
+      for (int w : all)
+        if (xa[w] == pa) l.push_back(w);
+      if (l.empty()) continue;
+      product(st, r, l, pa, kA6, 1.0, -1, 0.0, 0.0, kA4, true, nullptr, nullptr, true);    // R re = X P2 re
+      product(st, r, l, pa, kY, 1.0, -1, 0.0, 0.0, kA2, true, nullptr, nullptr, true);     // R im = X P2 im
     }
   }
 

@@ -873,6 +873,7 @@ __global__ void __launch_bounds__(kSmemSliceThreads, 1)
   }
 }
 constexpr int64_t kSmemSliceBytes = 200 * 1024;
+constexpr int64_t kSmemSliceMinK = 1024;   // narrower rows go to the warp-per-row kernel
 int smem_slice_grid(int64_t total_rows) {
   const int64_t g = std::min<int64_t>(total_rows, 148 * 2);
   return (int)std::max<int64_t>(1, g);
@@ -950,7 +951,9 @@ void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t to
   if (out.ld % 16 != 0) throw Error{FX_ERR_VALUE, "grouped slice: pitch must be a multiple of 16"};
   if (nslabs <= 0 || total_rows <= 0) return;
   const int64_t sm = (int64_t)sizeof(double) * 2 * kmax;
-  if (std::is_same<TI, double>::value && kmax > 0 && kmax % 4 == 0 && sm <= kSmemSliceBytes) {
+  // narrow rows (the Cholesky panels, K = 128) keep the warp-per-row kernel: a warp covers such
+  // a row in one step, where a CTA per row would leave most of its threads idle
+  if (std::is_same<TI, double>::value && kmax >= kSmemSliceMinK && kmax % 4 == 0 && sm <= kSmemSliceBytes) {
     static bool attr = false;
     if (!attr) {
       FX_CUDA(cudaFuncSetAttribute(k_slice_rows_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,

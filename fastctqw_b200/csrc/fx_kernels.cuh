@@ -231,7 +231,8 @@ enum ProdTag {
   kTagInverse = 4,     // explicit inverse of the Cholesky factor
   kTagTriangular = 5,  // Z = P2 L^-T, R^T = Z L^-1
   kTagSquare = 6,      // squarings
-  kTagDrift = 7        // diagnostic unitarity products
+  kTagDrift = 7,       // diagnostic unitarity products
+  kTagNewton = 8       // Newton-Schulz inverse of the solve (mixed form)
 };
 struct ProdRecord {
   int tag;
@@ -252,7 +253,7 @@ struct PipeOpts {
   bool drift = false;        // diagnostics: unitarity residual after every squaring
 };
 // Default slice schedule of the mixed form (see fx_batch.cu, BatchPipeline::sq_slices).
-constexpr int kMixedN4 = 4, kMixedN3 = 1, kMixedPade = 5;
+constexpr int kMixedN4 = 64, kMixedN3 = 0, kMixedPade = 4;
 void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU,
                         const PipeOpts& o, cudaStream_t s);
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st);

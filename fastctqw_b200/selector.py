@@ -153,7 +153,7 @@ def min_certified_s(m: int, rho: float, tol: float = PHASE_TOL) -> int:
 
 
 def make_dataset_measured(count: int, seed: int, nmin: int = 64, nmax: int = 2048, tmin: float = 0.1,
-                          tmax: float = 1000.0, chunk: int = 96, depth: int = 5) -> dict:
+                          tmax: float = 1000.0, chunk: int = 96, depth: int = 5, form: str = "plain") -> dict:
     """Walks of ``make_walks`` with labels measured on the GPU.
 
     Per chunk of walks: one analyze-only run (features, the Al-Mohy & Higham and the certified
@@ -163,7 +163,8 @@ def make_dataset_measured(count: int, seed: int, nmin: int = 64, nmax: int = 204
     at forced s = s_m - k, k = 0 .. depth - 1, where s_m is the smallest s the rigorous bound
     certifies for that m.  (m, s) passes when the infidelity against the FP64 state is <= 1e-10
     (and no a-posteriori check redid the walk); the label is the cheapest (m, s) (products
-    pi_m + s, ties to the larger m) whose s and every larger tested s pass."""
+    pi_m + s, ties to the larger m) whose s and every larger tested s pass.  The sweeps run in the
+    given precision form (the one the selection will serve)."""
     import torch
     from .batch import OPT_SAMPLE_WALKS, WalkBatch
     dev = torch.device("cuda", 0)
@@ -193,7 +194,7 @@ def make_dataset_measured(count: int, seed: int, nmin: int = 64, nmax: int = 204
             refs.append(ref)
             del lam, V
         outs = [torch.empty_like(p) for p in p0s]
-        sweep = WalkBatch(ns)
+        sweep = WalkBatch(ns, form=form)
         sweep.set_option(OPT_SAMPLE_WALKS, 0)
 
         def infidelities():

@@ -61,7 +61,7 @@ def evaluate(w, ds) -> dict:
     }
 
 
-def end_to_end(w, count: int, seed: int, nmin: int, nmax: int) -> dict:
+def end_to_end(w, count: int, seed: int, nmin: int, nmax: int, form: str = "plain") -> dict:
     """Every selector on fresh walks through the batch engine; infidelity against the FP64 state
     of psi0 = (v_max + v_min) / sqrt 2 (the most phase-sensitive state) and squarings taken."""
     import torch
@@ -80,7 +80,7 @@ def end_to_end(w, count: int, seed: int, nmin: int, nmax: int) -> dict:
     res = {"walks": count, "n_range": [nmin, nmax]}
     for mode in ("plain", "certified", "estimated", "learned"):
         outs = [torch.empty_like(p) for p in p0s]
-        with WalkBatch(ns, selector=mode) as b:
+        with WalkBatch(ns, selector=mode, form=form) as b:
             b.run_device(dX, p0s, outs)
             torch.cuda.synchronize()
             m, s = b.selection()
@@ -106,21 +106,23 @@ def main(argv=None):
     ap.add_argument("--nmax-large", type=int, default=4096)
     ap.add_argument("--epochs", type=int, default=120)
     ap.add_argument("--e2e", type=int, default=192)
+    ap.add_argument("--form", default="mixed", choices=["plain", "mixed"],
+                    help="precision form of the measured sweeps (the form the selection serves)")
     ap.add_argument("--out", default=os.path.join(DATA, "selector_weights.npz"))
     ap.add_argument("--report", default=os.path.join(DATA, "selector_eval.json"))
     a = ap.parse_args(argv)
     t0 = time.time()
-    ds_train = selector.merge(selector.make_dataset_measured(a.train, seed=1, nmax=a.nmax),
+    ds_train = selector.merge(selector.make_dataset_measured(a.train, seed=1, nmax=a.nmax, form=a.form),
                               selector.make_dataset_measured(a.train_large, seed=4, nmin=a.nmax,
-                                                             nmax=a.nmax_large, chunk=16))
-    ds_test = selector.merge(selector.make_dataset_measured(a.test, seed=2, nmax=a.nmax),
+                                                             nmax=a.nmax_large, chunk=16, form=a.form))
+    ds_test = selector.merge(selector.make_dataset_measured(a.test, seed=2, nmax=a.nmax, form=a.form),
                              selector.make_dataset_measured(a.test_large, seed=5, nmin=a.nmax,
-                                                            nmax=a.nmax_large, chunk=16))
+                                                            nmax=a.nmax_large, chunk=16, form=a.form))
     t1 = time.time()
     w, losses = selector.train(ds_train, epochs=a.epochs)
     t2 = time.time()
     selector.save(a.out, w, losses=losses)
-    rep = {"labels": "measured: cheapest (m, s) with infidelity <= 1e-10 against the FP64 state of "
+    rep = {"form": a.form, "labels": "measured: cheapest (m, s) with infidelity <= 1e-10 against the FP64 state of "
                      "(v_max + v_min)/sqrt(2), over forced sweeps s = s_cert(m) - k, k < 5, m in {3,5,7,9,13}",
            "train": a.train + a.train_large, "test": a.test + a.test_large, "n_range": [64, a.nmax_large],
            "t_range": [0.1, 1000.0], "epochs": a.epochs,
@@ -128,7 +130,7 @@ def main(argv=None):
            "seconds_labels": round(t1 - t0, 1), "seconds_train": round(t2 - t1, 1),
            "plain_selection_max_infidelity_train": float(np.max(ds_train["infidelity_plain"])),
            "train_eval": evaluate(w, ds_train), "heldout": evaluate(w, ds_test)}
-    rep["end_to_end"] = end_to_end(w, a.e2e, seed=3, nmin=64, nmax=a.nmax)
+    rep["end_to_end"] = end_to_end(w, a.e2e, seed=3, nmin=64, nmax=a.nmax, form=a.form)
     with open(a.report, "w") as f:
         json.dump(rep, f, indent=1)
     print(json.dumps(rep))

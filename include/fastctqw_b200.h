@@ -59,10 +59,12 @@ enum fx_form {
   FX_FORM_PLAIN = 0,  /* int8 tensor-core products of 5 (FP64 masters) or 4 (FP32)
                          Ozaki slices, exact int32 accumulation; default for complex64 */
   FX_FORM_MIXED = 1,  /* reduced-precision products (complex64 / float32 handles).  Walk
-                         generators X = i*(real symmetric): int8 slices on FP64 masters,
-                         5 slices for the Pade and solve products, each squaring as the
-                         two real products (Re+Im)(Re-Im) and 2 Re Im, with 4 and then 3
-                         slices for the last squarings (FX_OPT_SQ_N4 / FX_OPT_SQ_N3).
+                         generators X = i*(real symmetric): int8 slices on FP64 masters
+                         with the diagonals split off and added in FP64, 4 slices for the
+                         powers, Pade and solve products (FX_OPT_PADE_SLICES), the solve
+                         by a Newton-Schulz inverse, each squaring as three symmetric
+                         products Re^2, Im^2, (Re+Im)^2 at 4 slices (5 for squarings
+                         before the last FX_OPT_SQ_N4, 3 for the last FX_OPT_SQ_N3).
                          Other inputs: BF16 hi+lo split, 3 products (hi*hi, hi*lo,
                          lo*hi), FP32 accumulate, FP32 masters                        */
   FX_FORM_SIMT = 2,   /* CUDA-core FP32 FMA products, FP32 masters (checker)          */
@@ -98,15 +100,16 @@ enum fx_option {
                              loads of one K step, so that its bounded waits run out and
                              the run returns FX_ERR_TIMEOUT; -1 (default) off          */
   FX_OPT_SQ_N4 = 12,      /* mixed form, walk generators: how many squarings before the
-                             3-slice ones run at 4 slices (default 4)                  */
+                             3-slice ones run at 4 slices (default 64: all; the earlier
+                             ones run at 5)                                            */
   FX_OPT_SQ_N3 = 13,      /* mixed form, walk generators: how many of the last squarings run
-                             at 3 slices (default 1)                                   */
+                             at 3 slices (default 0)                                   */
   FX_OPT_DRIFT = 14,      /* diagnostics (walk generators): 1 records the unitarity residual
                              ||U_k^H U_k - I||_F / sqrt(n) after every squaring k = 0..s
                              (fx_unitarity_drift), at the cost of two extra products per
                              squaring                                                  */
-  FX_OPT_PADE_SLICES = 15 /* mixed form, walk generators: int8 slices of the Pade and solve
-                             products (5 default, 4 or 3)                              */
+  FX_OPT_PADE_SLICES = 15 /* mixed form, walk generators: int8 slices of the powers, Pade and
+                             solve products (4 default, 5 or 3)                        */
 };
 
 /* What the last run did. */
@@ -150,7 +153,7 @@ const char* fx_last_error(fx_handle h);
 /* Per product launch of the last run made with FX_OPT_PROFILE = 1 through the walk-generator
  * pipeline: its stage (0 powers, 1 Pade numerator / denominator, 2 the solve's V^2, W^2, VW,
  * 3 Cholesky, 4 triangular inverse, 5 triangular products, 6 squarings, 7 diagnostic unitarity
- * products), its CUDA-event duration in ms and the int8 tensor ops it issued.  Writes
+ * products, 8 Newton-Schulz inverse of the mixed form's solve), its CUDA-event duration in ms and the int8 tensor ops it issued.  Writes
  * min(cap, launches) records and the launch count to *count (0 when no such run was profiled).
  * Diagnostics; no counterpart in the reference. */
 int fx_product_profile(fx_handle h, int32_t* tags, double* ms, double* ops, int32_t cap, int32_t* count);
