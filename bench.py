@@ -33,17 +33,23 @@ sys.path.insert(0, REPO)
 METRIC = "expm(-iHt) ms at N=10k c64; batched walks/s; chosen vs plain @ infid<=1e-10"
 
 
-def product_traffic_per_launch():
-    """DRAM bytes (read + write) per k_gemm_i8 launch of the benchmark walk, from the committed ncu
-    capture of one walk's product launches (dram__bytes_read.sum + dram__bytes_write.sum), or None
-    when no capture for this workload is committed."""
-    path = os.path.join(REPO, "profiles", "k_gemm_i8_walk_n10000_traffic.json")
+def product_traffic_per_launch(form: str):
+    """DRAM bytes (read + write) per k_gemm_i8 launch of the benchmark walk in the given form, from
+    the committed summary of an ncu capture of one walk's product launches
+    (dram__bytes_read.sum + dram__bytes_write.sum, averaged over the walk's launches): the line
+    `dram_bytes_per_launch[<form>]: <bytes>` of profiles/k_gemm_i8_walk_traffic.md.  None when
+    the summary has no line for the form."""
+    import re
+    path = os.path.join(REPO, "profiles", "k_gemm_i8_walk_traffic.md")
     try:
         with open(path) as f:
-            d = json.load(f)
-        return {"bytes": d["dram_bytes_per_launch"], "source": d["summary"]}
-    except (OSError, KeyError, ValueError):
+            text = f.read()
+    except OSError:
         return None
+    m = re.search(r"dram_bytes_per_launch\[" + re.escape(form) + r"\]:\s*([0-9.eE+]+)", text)
+    if not m:
+        return None
+    return {"bytes": float(m.group(1)), "source": "profiles/k_gemm_i8_walk_traffic.md (ncu, one walk's product launches)"}
 
 
 def peaks():
@@ -532,7 +538,8 @@ def main():
     ap.add_argument("--n", type=int, default=10000)
     ap.add_argument("--t", type=float, default=4.5)
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--form", default="plain", choices=["plain", "mixed", "simt"])
+    ap.add_argument("--form", default="mixed", choices=["plain", "mixed", "simt"],
+                    help="precision form of the timed walk; the plain form is timed beside it")
     ap.add_argument("--selector", default="learned", choices=["plain", "certified", "estimated", "learned"],
                     help="(m, s) selection of the timed walk; the plain selection is timed beside it")
     ap.add_argument("--ref-sample-n", type=int, default=1024,
@@ -650,7 +657,7 @@ def main():
     bf = _native.tensor_peak("bf16")
     int8_peak = i8["tops"]
     achieved = pst["prod_ops"] / (pst["prod_ms"] * 1e-3) / 1e12 if pst["prod_ms"] > 0 else None
-    traffic = product_traffic_per_launch()
+    traffic = product_traffic_per_launch(args.form)
     roofline = {
         "bound": "tensor", "kernel": "k_gemm_i8<5,double> (int8 Ozaki-slice product, exact accumulation)",
         "achieved": round(achieved, 1) if achieved else None, "peak": round(int8_peak, 1), "unit": "TOP/s (int8)",
