@@ -38,6 +38,9 @@ namespace {
 constexpr int kS = 5;          // int8 slices (FP64 masters)
 constexpr int kNb = 128;       // Cholesky / inverse block
 constexpr int kEstScratch = 8; // doubles per row of a walk in the estimator scratch
+// The mixed form's Newton-Schulz solve serves walks padded to at least this size; below it the
+// blocked Cholesky has few steps (np / 128), which run grouped over the batch.
+constexpr int kNewtonMinNp = 4096;
 
 struct BWalk {
   int n, np;
@@ -2156,20 +2159,25 @@ class BatchPipeline {
     combo(st, r, all, kA6, m_12, cf);                             // P2 re -> A6
     for (int w = 0; w < W; ++w) cf[w] = {2.0, 0.0, 0.0, 0.0, 0.0};
     combo(st, r, all, kY, m_a2, cf);                              // P2 im -> Y
-    if (form_ == 1) {
-      newton_solve(st, r, all);                                   // R re -> A4, im -> A2
-    } else {
+    // the mixed form solves large walks by Newton-Schulz (their Cholesky would be a long chain
+    // of dependent block steps); small walks, whose few steps run grouped over the batch, and
+    // the plain form keep the Cholesky solve
+    std::vector<int> ns_list, ch_list;
+    for (int w = 0; w < W; ++w)
+      (form_ == 1 && walks_[w].np >= kNewtonMinNp ? ns_list : ch_list).push_back(w);
+    if (!ns_list.empty()) newton_solve(st, r, ns_list);            // R re -> A4, im -> A2
+    if (!ch_list.empty()) {
       tag_ = kTagCholesky;
-      cholesky(st, r, kA4);
-      transpose(st, r, all, kA4, kT1);                            // L^T -> T1
+      cholesky(st, r, kA4, ch_list);
+      transpose(st, r, ch_list, kA4, kT1);                        // L^T -> T1
       tag_ = kTagInverse;
-      inverse(st, r, kT1, kT2, kW, kA2);                          // X = L^-1 -> T2, X^T -> W (scratch A2)
+      inverse(st, r, kT1, kT2, kW, kA2, ch_list);                 // X = L^-1 -> T2, X^T -> W (scratch A2)
       // Z = P2 X^T (re -> V, im -> T1); R^T = Z X (re -> A4, im -> A2)
       tag_ = kTagTriangular;
-      complex_by_real(st, r, all, kA6, kY, kT2, kV, kT1, 1, true);    // P2 symmetric
-      complex_by_real(st, r, all, kV, kT1, kW, kA4, kA2, 2, false);
-      symmetrize(st, r, all, kA4);
-      symmetrize(st, r, all, kA2);
+      complex_by_real(st, r, ch_list, kA6, kY, kT2, kV, kT1, 1, true);    // P2 symmetric
+      complex_by_real(st, r, ch_list, kV, kT1, kW, kA4, kA2, 2, false);
+      symmetrize(st, r, ch_list, kA4);
+      symmetrize(st, r, ch_list, kA2);
     }
 
     gS_ = kS;
@@ -2373,12 +2381,12 @@ class BatchPipeline {
     for (int j = (int)b.size() - 1; j >= 0; --j) acc = acc * z + b[j];
     return std::norm(acc);
   }
-  void newton_solve(Staging& st, Rec& r, const std::vector<int>& all) {
+  void newton_solve(Staging& st, Rec& r, const std::vector<int>& list) {
     const int W = count();
     tag_ = kTagNewton;
     std::vector<int> iters(W, 0);
-    std::vector<std::array<double, 5>> cf(W);
-    for (int w = 0; w < W; ++w) {
+    std::vector<std::array<double, 5>> cf(W, {0.0, 0.0, 0.0, 0.0, 0.0});
+    for (int w : list) {
       const std::vector<double> b = pade_coeffs(sel_m_[w]);
       const double rho = std::min(rho_up_[w], 1.25 * rho_lan_[w] > 0.0 ? 1.25 * rho_lan_[w] : rho_up_[w]);
       const double xmax = std::ldexp(rho, -sel_s_[w]);
@@ -2401,13 +2409,13 @@ class BatchPipeline {
       cf[w] = {-a * a, 0.0, 0.0, 0.0, 2.0 * a};
     }
     const int m_g[4] = {kA4, -1, -1, -1};
-    combo(st, r, all, kT1, m_g, cf);   // X1 = -a^2 G + 2a I
+    combo(st, r, list, kT1, m_g, cf);   // X1 = -a^2 G + 2a I
     std::vector<int> xa(W, kT1), xb(W, kV);
     int kmax = 0;
-    for (int w = 0; w < W; ++w) kmax = std::max(kmax, iters[w]);
+    for (int w : list) kmax = std::max(kmax, iters[w]);
     for (int k = 0; k < kmax; ++k) {
       std::vector<int> act;
-      for (int w = 0; w < W; ++w)
+      for (int w : list)
         if (iters[w] > k) act.push_back(w);
       for (int pa : {kT1, kV}) {
         std::vector<int> l;
@@ -2423,7 +2431,7 @@ class BatchPipeline {
     tag_ = kTagTriangular;
     for (int pa : {kT1, kV}) {
       std::vector<int> l;
-      for (int w : all)
+      for (int w : list)
         if (xa[w] == pa) l.push_back(w);
       if (l.empty()) continue;
       product(st, r, l, pa, kA6, 1.0, -1, 0.0, 0.0, kA4, true, nullptr, nullptr, true);    // R re = X P2 re
@@ -2594,15 +2602,14 @@ class BatchPipeline {
   }
 
   // Blocked right-looking Cholesky of the listed walks' G (in arena g), 128-wide steps.
-  void cholesky(Staging& st, Rec& r, int g) {
-    const int W = count();
+  void cholesky(Staging& st, Rec& r, int g, const std::vector<int>& list) {
     int jmax = 0;
-    for (int w = 0; w < W; ++w) jmax = std::max(jmax, walks_[w].np / kNb);
+    for (int w : list) jmax = std::max(jmax, walks_[w].np / kNb);
     for (int j = 0; j < jmax; ++j) {
       std::vector<GChol> jobs;
       std::vector<GSlab> sa21, sb_l;
       std::vector<GProblem> p21, p22;
-      for (int w = 0; w < W; ++w) {
+      for (int w : list) {
         const BWalk& b = walks_[w];
         if (b.np <= j * kNb) continue;
         double* G = A(g) + b.off;
@@ -2668,17 +2675,12 @@ class BatchPipeline {
     collect(w, a, mid, depth + 1, lv);
     collect(w, mid, b, depth + 1, lv);
   }
-  void inverse(Staging& st, Rec& r, int lt, int x, int xt, int scratch) {
+  void inverse(Staging& st, Rec& r, int lt, int x, int xt, int scratch, const std::vector<int>& list) {
     const int W = count();
     std::vector<int64_t> loff(W);
-    std::vector<int> all(W);
-    for (int w = 0; w < W; ++w) {
-      loff[w] = (int64_t)walks_[w].row0 * kNb;
-      all[w] = w;
-    }
-    const std::vector<RChunk> ch = row_chunks(all, false);
-    const size_t o_lo = st.put(loff), o_all = st.put(all), o_ch = st.put(ch);
-    (void)o_all;
+    for (int w = 0; w < W; ++w) loff[w] = (int64_t)walks_[w].row0 * kNb;
+    const std::vector<RChunk> ch = row_chunks(list, false);
+    const size_t o_lo = st.put(loff), o_ch = st.put(ch);
     double* X = A(x);
     double* XT = A(xt);
     const double* Li = (const double*)linv_.p;
@@ -2692,7 +2694,7 @@ class BatchPipeline {
       FX_LAUNCH_CHECK();
     });
     std::vector<std::vector<Node>> lv;
-    for (int w = 0; w < W; ++w) collect(w, 0, walks_[w].np / kNb, 0, lv);
+    for (int w : list) collect(w, 0, walks_[w].np / kNb, 0, lv);
     for (int d = (int)lv.size() - 1; d >= 0; --d) {
       std::vector<GSlab> sa, sb, sa2, sb2;
       std::vector<GProblem> pa, pb;
