@@ -23,7 +23,8 @@ FORM_PLAIN, FORM_MIXED, FORM_SIMT, FORM_FP64 = 0, 1, 2, 3
 FORMS = {"plain": FORM_PLAIN, "mixed": FORM_MIXED, "simt": FORM_SIMT, "fp64": FORM_FP64}
 (OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE,
  OPT_DEBUG_STAGE, OPT_PROFILE, OPT_SELECTOR, OPT_INJECT_STALL, OPT_SQ_N4, OPT_SQ_N3, OPT_DRIFT,
- OPT_PADE_SLICES) = range(16)
+ OPT_PADE_SLICES, OPT_NEWTON_SLICES, OPT_SOLVE) = range(18)
+SOLVES = {"auto": 0, "cholesky": 1, "newton": 2}
 SELECTORS = {"plain": 0, "certified": 1, "learned": 2, "estimated": 3}
 
 OK, ERR_TYPE, ERR_VALUE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_NONFINITE, ERR_SINGULAR, ERR_NODEV, ERR_FREED = range(10)
@@ -80,6 +81,9 @@ SIGNATURES = {
                        ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int64,
                        ctypes.c_float, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
     "fx_product_error": [],
+    "fx_slice_rows_f64": [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                          ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                          ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "fx_tensor_peak": [ctypes.c_int, ctypes.c_int64, ctypes.POINTER(ctypes.c_double),
                        ctypes.POINTER(ctypes.c_double), ctypes.c_void_p],
     "fx_build_generator": [ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int,
@@ -186,6 +190,26 @@ def product_f32(form: str, A, Bt, alpha=1.0, beta=0.0, C=None, gamma=0.0, D=None
     return D
 
 
+def slice_rows(re, im=None, S: int = 5, kind: int = 1, split_diag: bool = False, neg: bool = False) -> dict:
+    """The product kernels' int8 slicer on torch CUDA float64 rows (diagnostic, fx_slice_rows_f64):
+    digits (S, rows, K) of re (and of im, -im), row exponents, split-off diagonal."""
+    import torch
+    rows, K = re.shape
+    if im is not None and (im.shape != re.shape or im.stride() != re.stride()):
+        raise ValueError("slice_rows: re and im need the same shape and strides")
+    ldo = (K + 15) // 16 * 16
+    out = torch.zeros((3 * S, rows, ldo), dtype=torch.int8, device=re.device)
+    exps = torch.zeros(rows, dtype=torch.int32, device=re.device)
+    dg = torch.zeros(rows, dtype=torch.float64, device=re.device) if split_diag else None
+    rc = lib().fx_slice_rows_f64(kind, S, re.data_ptr(), im.data_ptr() if im is not None else None, re.stride(0),
+                                 rows, K, int(split_diag), int(neg), out.data_ptr(), ldo, exps.data_ptr(),
+                                 dg.data_ptr() if dg is not None else None,
+                                 torch.cuda.current_stream().cuda_stream)
+    if rc != OK:
+        raise RuntimeError(lib().fx_product_error().decode())
+    return {"re": out[:S, :, :K], "im": out[S:2 * S, :, :K], "neg_im": out[2 * S:, :, :K], "exp": exps, "dg": dg}
+
+
 def tensor_peak(kind: str = "int8", iters: int = 50000, reps: int = 5, stream=None) -> dict:
     """Measured dense tensor-core rate (fx_tensor_peak): the median of `reps` launches, in
     tera-ops per second (2 M N K per instruction)."""
@@ -231,7 +255,8 @@ class Engine:
                   timeout_ms: float | None = None, debug_stage: int | None = None,
                   profile: bool | None = None, selector: str | None = None,
                   inject_stall: int | None = None, sq_n4: int | None = None, sq_n3: int | None = None,
-                  drift: bool | None = None, pade_slices: int | None = None) -> None:
+                  drift: bool | None = None, pade_slices: int | None = None,
+                  newton_slices: int | None = None, solve: str | None = None) -> None:
         if form is not None:
             if form not in FORMS:
                 raise ValueError(f"form must be one of {sorted(FORMS)}")
@@ -266,6 +291,12 @@ class Engine:
             self.set_option(OPT_DRIFT, int(bool(drift)))
         if pade_slices is not None:
             self.set_option(OPT_PADE_SLICES, pade_slices)
+        if newton_slices is not None:
+            self.set_option(OPT_NEWTON_SLICES, newton_slices)
+        if solve is not None:
+            if solve not in SOLVES:
+                raise ValueError(f"solve must be one of {sorted(SOLVES)}")
+            self.set_option(OPT_SOLVE, SOLVES[solve])
 
     def spectral_radius(self) -> dict:
         """Lanczos estimate and rigorous upper bound of the shifted generator's spectral radius

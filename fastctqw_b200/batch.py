@@ -22,9 +22,10 @@ from ._native import check, lib
 
 OPT_GRAPH, OPT_TIMEOUT_MS, OPT_FORCE_M, OPT_SELECTOR, OPT_ANALYZE_ONLY, OPT_DIAG_SPLIT = 0, 1, 2, 3, 4, 5
 OPT_AUTOTUNE, OPT_TILE_GROUP, OPT_TILE_ORDER, OPT_SAMPLE_WALKS = 6, 7, 8, 9
-OPT_FORM, OPT_SQ_N4, OPT_SQ_N3, OPT_DRIFT, OPT_PADE_SLICES = 10, 11, 12, 13, 14
-OUTCOMES = {0: "plain", 1: "certified", 2: "learned", -1: "learned rejected by the bound",
-            -2: "failed an a-posteriori check, redone with the plain (m, s)"}
+OPT_FORM, OPT_SQ_N4, OPT_SQ_N3, OPT_DRIFT, OPT_PADE_SLICES, OPT_NEWTON_SLICES, OPT_SOLVE = 10, 11, 12, 13, 14, 15, 16
+OUTCOMES = {0: "plain", 1: "certified", 2: "learned", 3: "estimated",
+            -1: "learned rejected by the bound, plain (m, s) kept",
+            -2: "failed an a-posteriori check, redone with the plain (m, s)", 4: "forced (m, s)"}
 
 
 def _check(rc: int, h) -> None:
@@ -52,7 +53,8 @@ class WalkBatch:
     def __init__(self, ns, dtype=np.complex64, graph: bool = True, selector: str = "plain",
                  analyze_only: bool = False, diag_split: int = 3, autotune: bool = False,
                  form: str = "plain", sq_n4: int | None = None, sq_n3: int | None = None,
-                 drift: bool = False, pade_slices: int | None = None) -> None:
+                 drift: bool = False, pade_slices: int | None = None,
+                 newton_slices: int | None = None, solve: str = "auto") -> None:
         self.ns = [int(n) for n in ns]
         self.dtype = np.dtype(dtype)
         if self.dtype not in (np.dtype(np.complex64), np.dtype(np.complex128)):
@@ -77,6 +79,10 @@ class WalkBatch:
             self.set_option(OPT_SQ_N3, sq_n3)
         if pade_slices is not None:
             self.set_option(OPT_PADE_SLICES, pade_slices)
+        if newton_slices is not None:
+            self.set_option(OPT_NEWTON_SLICES, newton_slices)
+        if solve != "auto":
+            self.set_option(OPT_SOLVE, _native.SOLVES[solve])
         if form != "plain":
             if form != "mixed":
                 raise ValueError("batched walks take form 'plain' or 'mixed'")

@@ -970,10 +970,29 @@ class BatchPipeline {
   void set_graph(bool g) { use_graph_ = g; }
   void set_timeout(unsigned ms) { timeout_ms_ = ms; }
   void set_profile(bool p) { profile_ = p; }
-  // 0 plain (Al-Mohy & Higham), 1 certified bound, 2 learned (gated by the bound).
-  void set_selector(int k) { selector_ = k; }
+  // 0 plain (Al-Mohy & Higham), 1 certified bound, 2 learned (gated by the bound), 3 estimated.
+  // Phase 1 runs the Lanczos estimate only where a selection or the form needs it.
+  void set_selector(int k) {
+    const bool before = needs_lanczos();
+    selector_ = k;
+    if (needs_lanczos() != before) rerecord_phase1();
+  }
+  bool needs_lanczos() const { return selector_ >= 2 || form_ == 1 || analyze_only_; }
+  void rerecord_phase1() {
+    if (graph1_) cudaGraphExecDestroy(graph1_);
+    graph1_ = nullptr;
+    st1_ = Staging();
+    r1_ = Rec();
+    desc1_.release();
+    record_phase1();
+    key2_.clear();
+  }
   // Stop after the selection (statistics, norms, estimates, features; no exponential).
-  void set_analyze_only(bool a) { analyze_only_ = a; }
+  void set_analyze_only(bool a) {
+    const bool before = needs_lanczos();
+    analyze_only_ = a;
+    if (needs_lanczos() != before) rerecord_phase1();
+  }
   // Phase-2 schedule: tune it at the next run, or set it.
   void set_autotune(bool a) { autotune_ = a; }
   void set_schedule(int group, int order) {
@@ -991,13 +1010,7 @@ class BatchPipeline {
   void set_diag_split(int v) {
     if (v == split_) return;
     split_ = v;
-    if (graph1_) cudaGraphExecDestroy(graph1_);
-    graph1_ = nullptr;
-    st1_ = Staging();
-    r1_ = Rec();
-    desc1_.release();
-    record_phase1();
-    key2_.clear();
+    rerecord_phase1();
   }
   int selector() const { return selector_; }
   // Spectral-radius estimates of walk w in the last run: Lanczos (a lower estimate) and the
@@ -1012,7 +1025,11 @@ class BatchPipeline {
   // Precision form of the squarings: 0 plain (every squaring the exact complex square, 4 real
   // products at 5 slices); 1 mixed (each squaring as the two real products (Er + Ei)(Er - Ei)
   // and 2 Er Ei, 5 slices except the last n4 + n3 squarings: n4 at 4 slices, then n3 at 3).
-  void set_form(int form, int n4, int n3, int pade_slices = kS) {
+  void set_form(int form, int n4, int n3, int pade_slices = kS, int newton_slices = kS) {
+    if (newton_slices != newton_S_) {   // read when phase 2 is recorded
+      newton_S_ = newton_slices;
+      key2_.clear();
+    }
     if (form == form_ && n4 == sq_n4_ && n3 == sq_n3_ && pade_slices == pade_S_) return;
     const bool rerecord = form != form_ || (form == 1 && pade_slices != pade_S_);
     form_ = form;
@@ -1020,16 +1037,17 @@ class BatchPipeline {
     sq_n3_ = n3;
     pade_S_ = pade_slices;
     key2_.clear();
-    if (rerecord) {   // phase 1's powers take the form's slice count and diagonal split
-      if (graph1_) cudaGraphExecDestroy(graph1_);
-      graph1_ = nullptr;
-      st1_ = Staging();
-      r1_ = Rec();
-      desc1_.release();
-      record_phase1();
-    }
+    // phase 1's powers take the form's slice count and diagonal split
+    if (rerecord) rerecord_phase1();
   }
   int pade_slices() const { return pade_S_; }
+  // Solve of the walk-generator Pade step: 0 Newton-Schulz for mixed-form walks padded to 4096
+  // or more and Cholesky otherwise, 1 Cholesky, 2 Newton-Schulz.
+  void set_solve(int mode) {
+    if (mode == solve_mode_) return;
+    solve_mode_ = mode;
+    key2_.clear();
+  }
   int form() const { return form_; }
   // Diagnostics: the unitarity residual ||U_k^H U_k - I||_F / sqrt(n) of the iterate after every
   // squaring k = 0..s (k = 0: the Pade result), from two extra 5-slice products per squaring.
@@ -1107,12 +1125,14 @@ class BatchPipeline {
     FX_CUDA(cudaMemcpyAsync(h_flags.data(), flags(), sizeof(int) * W, cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaMemcpyAsync(norms_.data(), norms(), sizeof(double) * 8 * W, cudaMemcpyDeviceToHost, s));
     lan_host_.assign((size_t)W * 4 * kLanSteps, 0.0);
-    FX_CUDA(cudaMemcpyAsync(lan_host_.data(), lanc_.p, sizeof(double) * lan_host_.size(), cudaMemcpyDeviceToHost, s));
+    const bool lan = lan_recorded_;
+    if (lan)
+      FX_CUDA(cudaMemcpyAsync(lan_host_.data(), lanc_.p, sizeof(double) * lan_host_.size(), cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaStreamSynchronize(s));
     check_err();
     rho_lan_.assign(W, 0.0);
     rho_up_.assign(W, 0.0);
-    for (int w = 0; w < W; ++w) {
+    for (int w = 0; w < W && lan; ++w) {
       const double* base = lan_host_.data() + (size_t)w * 4 * kLanSteps;
       rho_lan_[w] = std::max(tridiag_radius(base, kLanSteps), tridiag_radius(base + 2 * kLanSteps, kLanSteps));
     }
@@ -1188,33 +1208,35 @@ class BatchPipeline {
         m = cert_m_[w];
         sq = cert_s_[w];
         outcome_[w] = 1;
-      } else if (selector_ == 3) {
+      } else if (selector_ == 3 || selector_ == 2) {
         // the phase bound at the Lanczos estimate of the spectral radius, with a margin (never
         // above the rigorous bound rho_up)
+        const double rho_est = std::min(rho_up, rho_lan_[w] * (1.0 + kLanMargin));
         int em = 13, es = 0;
-        certified_choice(std::min(rho_up, rho_lan_[w] * (1.0 + kLanMargin)), kPhaseTol, &em, &es);
+        certified_choice(rho_est, kPhaseTol, &em, &es);
         if (pade_products(em) + es < pade_products(m) + sq) {
           m = em;
           sq = es;
           outcome_[w] = 3;
         }
-      } else if (selector_ == 2) {
-        const float* o = prop.data() + 6 * w;
-        int c = 0;
-        for (int k = 1; k < 5; ++k)
-          if (o[k] > o[c]) c = k;
-        const int pm = kDegrees[c];
-        const int ps = std::max(0, (int)std::lround(o[5]));
-        if (pade_products(pm) + ps < pade_products(m) + sq) {
-          // gate: the phase bound at the spectral radius as far as it is known -- the rigorous
-          // bound, or the Lanczos estimate with its margin -- at the phase error that keeps the
+        if (selector_ == 2) {
+          // the learned proposal replaces the estimated choice when it is cheaper still and
+          // passes the gate: the same phase bound at the phase error that keeps the
           // infidelity of every state below 1e-10
-          if (certified(pm, ps, std::min(rho_up, rho_lan_[w] * (1.0 + kLanMargin)), kGateTol)) {
-            m = pm;
-            sq = ps;
-            outcome_[w] = 2;
-          } else {
-            outcome_[w] = -1;   // rejected by the bound: plain (m, s)
+          const float* o = prop.data() + 6 * w;
+          int c = 0;
+          for (int k = 1; k < 5; ++k)
+            if (o[k] > o[c]) c = k;
+          const int pm = kDegrees[c];
+          const int ps = std::max(0, (int)std::lround(o[5]));
+          if (pade_products(pm) + ps < pade_products(m) + sq) {
+            if (certified(pm, ps, rho_est, kGateTol)) {
+              m = pm;
+              sq = ps;
+              outcome_[w] = 2;
+            } else if (outcome_[w] != 3) {
+              outcome_[w] = -1;   // rejected by the bound, and no estimated choice: plain (m, s)
+            }
           }
         }
       }
@@ -1481,6 +1503,7 @@ class BatchPipeline {
   std::vector<int> plain_m_, plain_s_, cert_m_, cert_s_, outcome_;
   std::vector<double> features_;
   int selector_ = 0;
+  bool lan_recorded_ = false;   // phase 1 as recorded runs the Lanczos estimate
   bool analyze_only_ = false;
   int split_ = 3;
   int tile_group_ = 8, tile_order_ = 0;   // phase-2 schedule of the grouped products
@@ -1500,6 +1523,8 @@ class BatchPipeline {
   int inject_ = -1, prod_index_ = 0;   // stall injection (diagnostics), product launches so far
   int form_ = 0, sq_n4_ = 0, sq_n3_ = 0;   // squaring form and slice schedule
   int pade_S_ = kS;                        // mixed form: slices of the Pade and solve products
+  int newton_S_ = kS;                      // mixed form: slices of the early Newton-Schulz steps
+  int solve_mode_ = 0;                     // 0 by form and size, 1 Cholesky, 2 Newton-Schulz
   int gS_ = kS;                            // slices of the grouped products being recorded
   DevArena lanc_;                          // Lanczos coefficients (W x 2 runs x kLanSteps x 2)
   std::vector<double> lan_host_, rho_lan_, rho_up_;
@@ -1738,7 +1763,8 @@ class BatchPipeline {
     r.launches += 6;
     estimate(st, r, all, kA4, kA4, 3);
     estimate(st, r, all, kA4, kA6, 4);
-    lanczos(st, r, all);
+    lan_recorded_ = needs_lanczos();
+    if (lan_recorded_) lanczos(st, r, all);
   }
 
   // Lanczos runs on B = Im Y (arena Y) of the listed walks into lanc_ (kLanSteps steps).
@@ -2163,8 +2189,10 @@ class BatchPipeline {
     // of dependent block steps); small walks, whose few steps run grouped over the batch, and
     // the plain form keep the Cholesky solve
     std::vector<int> ns_list, ch_list;
-    for (int w = 0; w < W; ++w)
-      (form_ == 1 && walks_[w].np >= kNewtonMinNp ? ns_list : ch_list).push_back(w);
+    for (int w = 0; w < W; ++w) {
+      const bool ns = solve_mode_ == 2 || (solve_mode_ == 0 && form_ == 1 && walks_[w].np >= kNewtonMinNp);
+      (ns ? ns_list : ch_list).push_back(w);
+    }
     if (!ns_list.empty()) newton_solve(st, r, ns_list);            // R re -> A4, im -> A2
     if (!ch_list.empty()) {
       tag_ = kTagCholesky;
@@ -2384,7 +2412,7 @@ class BatchPipeline {
   void newton_solve(Staging& st, Rec& r, const std::vector<int>& list) {
     const int W = count();
     tag_ = kTagNewton;
-    std::vector<int> iters(W, 0);
+    std::vector<int> iters(W, 0), lo_steps(W, 0);
     std::vector<std::array<double, 5>> cf(W, {0.0, 0.0, 0.0, 0.0, 0.0});
     for (int w : list) {
       const std::vector<double> b = pade_coeffs(sel_m_[w]);
@@ -2406,6 +2434,15 @@ class BatchPipeline {
         ++k;
       }
       iters[w] = k;
+      // steps whose model residual stays above kNewtonLoRes take newton_S_ slices: the
+      // iteration corrects their rounding (its fixed point attracts), and the later steps at
+      // the full slice count square the residual as in exact arithmetic
+      double rk = (ghi - glo) / (ghi + glo);
+      rk *= rk;
+      for (int j = 0; j < k; ++j) {
+        rk *= rk;
+        if (rk > kNewtonLoRes) lo_steps[w] = j + 1;
+      }
       cf[w] = {-a * a, 0.0, 0.0, 0.0, 2.0 * a};
     }
     const int m_g[4] = {kA4, -1, -1, -1};
@@ -2417,15 +2454,21 @@ class BatchPipeline {
       std::vector<int> act;
       for (int w : list)
         if (iters[w] > k) act.push_back(w);
+      const int full = gS_;
       for (int pa : {kT1, kV}) {
-        std::vector<int> l;
-        for (int w : act)
-          if (xa[w] == pa) l.push_back(w);
-        if (l.empty()) continue;
-        const int nx = pa == kT1 ? kV : kT1;
-        product(st, r, l, kA4, pa, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, true);   // G X
-        product(st, r, l, pa, kT2, -1.0, pa, 2.0, 0.0, nx, true, nullptr, nullptr, true);  // 2X - X G X
+        for (int S : {newton_S_, full}) {
+          std::vector<int> l;
+          for (int w : act)
+            if (xa[w] == pa && (k < lo_steps[w] ? newton_S_ : full) == S) l.push_back(w);
+          if (l.empty()) continue;
+          const int nx = pa == kT1 ? kV : kT1;
+          gS_ = S;
+          product(st, r, l, kA4, pa, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, true);   // G X
+          product(st, r, l, pa, kT2, -1.0, pa, 2.0, 0.0, nx, true, nullptr, nullptr, true);  // 2X - X G X
+          if (S == full) break;   // newton_S_ == full: one group
+        }
       }
+      gS_ = full;
       for (int w : act) std::swap(xa[w], xb[w]);
     }
     tag_ = kTagTriangular;
@@ -2439,6 +2482,8 @@ class BatchPipeline {
     }
   }
 
+  // Model residual below which the Newton-Schulz steps run at the full slice count.
+  static constexpr double kNewtonLoRes = 1e-3;
   // Slice count of squaring k (0-based) of walk w in the mixed form.
   int sq_slices(int w, int k) const {
     const int rem = sel_s_[w] - k;   // 1 for the last squaring
@@ -2753,7 +2798,8 @@ void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, voi
   p->set_profile(o.profile);
   p->set_timeout(o.timeout_ms);
   p->set_inject_stall(o.inject_stall);
-  p->set_form(o.form == FX_FORM_MIXED ? 1 : 0, o.sq_n4, o.sq_n3, o.pade_slices);
+  p->set_form(o.form == FX_FORM_MIXED ? 1 : 0, o.sq_n4, o.sq_n3, o.pade_slices, o.newton_slices);
+  p->set_solve(o.solve);
   p->set_drift(o.drift);
   p->run(x, p0, p1, u, s);
 }
@@ -2790,6 +2836,7 @@ struct fx_batch {
   fx::HostStage stage;       // page-locked chunks for the copies of the host matrices
   int sq_n4 = fx::kMixedN4, sq_n3 = fx::kMixedN3;   // mixed-form slice schedule
   int pade_slices = fx::kMixedPade;
+  int newton_slices = fx::kMixedNewton;
   std::string last_error;
 };
 
@@ -2925,20 +2972,31 @@ int fx_batch_set_option(fx_batch_handle b, int key, double value) {
     case FX_BATCH_OPT_FORM:
       if (value != FX_FORM_PLAIN && value != FX_FORM_MIXED)
         return bfail(b, fx::Error{FX_ERR_VALUE, "batch form must be FX_FORM_PLAIN or FX_FORM_MIXED"});
-      b->p->set_form(value == FX_FORM_MIXED ? 1 : 0, b->sq_n4, b->sq_n3, b->pade_slices);
+      b->p->set_form(value == FX_FORM_MIXED ? 1 : 0, b->sq_n4, b->sq_n3, b->pade_slices, b->newton_slices);
       return FX_OK;
     case FX_BATCH_OPT_SQ_N4:
     case FX_BATCH_OPT_SQ_N3: {
       if (value < 0 || value > 64) return bfail(b, fx::Error{FX_ERR_VALUE, "squaring counts must be 0..64"});
       (key == FX_BATCH_OPT_SQ_N4 ? b->sq_n4 : b->sq_n3) = (int)value;
-      b->p->set_form(b->p->form(), b->sq_n4, b->sq_n3, b->pade_slices);
+      b->p->set_form(b->p->form(), b->sq_n4, b->sq_n3, b->pade_slices, b->newton_slices);
       return FX_OK;
     }
     case FX_BATCH_OPT_PADE_SLICES:
       if (value != 3 && value != 4 && value != 5)
         return bfail(b, fx::Error{FX_ERR_VALUE, "Pade slice count must be 3, 4 or 5"});
       b->pade_slices = (int)value;
-      b->p->set_form(b->p->form(), b->sq_n4, b->sq_n3, b->pade_slices);
+      b->p->set_form(b->p->form(), b->sq_n4, b->sq_n3, b->pade_slices, b->newton_slices);
+      return FX_OK;
+    case FX_BATCH_OPT_SOLVE:
+      if (value != 0 && value != 1 && value != 2)
+        return bfail(b, fx::Error{FX_ERR_VALUE, "solve must be 0 (by form and size), 1 or 2"});
+      b->p->set_solve((int)value);
+      return FX_OK;
+    case FX_BATCH_OPT_NEWTON_SLICES:
+      if (value != 3 && value != 4 && value != 5)
+        return bfail(b, fx::Error{FX_ERR_VALUE, "Newton slice count must be 3, 4 or 5"});
+      b->newton_slices = (int)value;
+      b->p->set_form(b->p->form(), b->sq_n4, b->sq_n3, b->pade_slices, b->newton_slices);
       return FX_OK;
     case FX_BATCH_OPT_DRIFT: b->p->set_drift(value != 0.0); return FX_OK;
   }

@@ -93,6 +93,43 @@ int fx_product_f32(int form, int64_t M, int64_t N, int64_t K, const float* A, in
   return FX_OK;
 }
 
+// Diagnostic: the grouped int8 slicer on one block of rows of FP64 planes (device buffers).
+// kind 0 / 1 picks the warp-per-row or the two-pass streaming kernel; S slices; split_diag
+// leaves row r's element at column r out of the slices (single plane only) and writes it to dg;
+// neg also writes the slices of -im.  out holds 3 S planes of rows x ldo bytes (re, im, -im).
+int fx_slice_rows_f64(int kind, int S, const double* re, const double* im, int64_t ld, int64_t rows, int64_t K,
+                      int split_diag, int neg, int8_t* out, int64_t ldo, int32_t* exps, double* dg, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  fx::GSlab* d_slab = nullptr;
+  try {
+    if ((kind != 0 && kind != 1) || S < 3 || S > 5 || !re || !out || !exps || rows <= 0 || K <= 0 || K > ld ||
+        ldo < K || ldo % 16 != 0 || rows > (1 << 30) || K > (1 << 30) || (split_diag && (im || !dg)) ||
+        (neg && !im))
+      throw fx::Error{FX_ERR_VALUE, "fx_slice_rows_f64: invalid arguments"};
+    fx::GSlab h{re, im, ld, (int)rows, (int)K, 0, split_diag ? 0 : fx::kNoDiag};
+    FX_CUDA(cudaMalloc(&d_slab, sizeof(fx::GSlab)));
+    FX_CUDA(cudaMemcpyAsync(d_slab, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    fx::I8Slices o{};
+    const size_t plane = (size_t)rows * ldo;
+    for (int q = 0; q < S; ++q) {
+      o.re[q] = out + (size_t)q * plane;
+      if (im) o.im[q] = out + (size_t)(S + q) * plane;
+      if (neg) o.neg_im[q] = out + (size_t)(2 * S + q) * plane;
+    }
+    o.exp = exps;
+    o.ld = ldo;
+    o.dg = split_diag ? dg : nullptr;
+    fx::launch_slice_rows_grouped<double>(S, d_slab, 1, rows, o, neg != 0, s, K, kind);
+    FX_CUDA(cudaStreamSynchronize(s));
+  } catch (const fx::Error& e) {
+    g_dbg_err = e.msg;
+    if (d_slab) cudaFree(d_slab);
+    return e.code;
+  }
+  cudaFree(d_slab);
+  return FX_OK;
+}
+
 const char* fx_product_error(void) { return g_dbg_err.c_str(); }
 
 }  // extern "C"

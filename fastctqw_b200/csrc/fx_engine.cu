@@ -91,6 +91,8 @@ struct RunOpts {
   int inject_stall;  // diagnostics of the grouped path: product launch that skips a K step (-1 off)
   int sq_n4, sq_n3;  // mixed form of the grouped path: squarings at 4 and at 3 slices
   int pade_slices;   // mixed form of the grouped path: slices of the Pade and solve products
+  int newton_slices; // mixed form of the grouped path: slices of the early Newton-Schulz steps
+  int solve;         // grouped path: Pade solve, 0 by form and size, 1 Cholesky, 2 Newton-Schulz
   int drift;         // diagnostics of the grouped path: unitarity residual after every squaring
 };
 
@@ -1045,7 +1047,8 @@ struct fx_engine {
   fx::BatchPipeline* grouped = nullptr;   // grouped pipeline for walk generators (lazy)
   void* check_buf = nullptr;              // input statistics of the routing check
   fx::HostStage stage;                    // page-locked chunks for copies of host buffers
-  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0, 0, -1, fx::kMixedN4, fx::kMixedN3, fx::kMixedPade, 0};
+  fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0, 0, -1, fx::kMixedN4, fx::kMixedN3, fx::kMixedPade,
+                      fx::kMixedNewton, 0, 0};
   fx_stats stats{};
   std::string last_error;
 };
@@ -1138,6 +1141,8 @@ void run_device(fx_handle h, const void* dA, void* dU, const void* dpsi0, void* 
     po.sq_n4 = h->opts.sq_n4;
     po.sq_n3 = h->opts.sq_n3;
     po.pade_slices = h->opts.pade_slices;
+    po.newton_slices = h->opts.newton_slices;
+    po.solve = h->opts.solve;
     po.drift = h->opts.drift != 0;
     fx::batch_pipeline_run(h->grouped, dA, dpsi0, dpsi, dU, po, s);
     FX_CUDA(cudaEventRecord(h->ev1, s));
@@ -1304,6 +1309,14 @@ int fx_set_option(fx_handle h, int key, double value) {
     case FX_OPT_PADE_SLICES:
       if (v != 3 && v != 4 && v != 5) return fail(h, fx::Error{FX_ERR_VALUE, "Pade slice count must be 3, 4 or 5"});
       h->opts.pade_slices = v;
+      return FX_OK;
+    case FX_OPT_SOLVE:
+      if (v != 0 && v != 1 && v != 2) return fail(h, fx::Error{FX_ERR_VALUE, "solve must be 0, 1 or 2"});
+      h->opts.solve = v;
+      return FX_OK;
+    case FX_OPT_NEWTON_SLICES:
+      if (v != 3 && v != 4 && v != 5) return fail(h, fx::Error{FX_ERR_VALUE, "Newton slice count must be 3, 4 or 5"});
+      h->opts.newton_slices = v;
       return FX_OK;
   }
   return fail(h, fx::Error{FX_ERR_VALUE, "unknown option"});

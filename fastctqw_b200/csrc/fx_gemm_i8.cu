@@ -758,126 +758,122 @@ __device__ __forceinline__ double scale_for(int S, int e, bool& one) {
   return one ? ldexp(1.0, sh) : 0.0;
 }
 
-// ---- grouped slicing with the row in shared memory: one CTA per row (grid-stride over the
-// stacked rows).  The row's planes are read from HBM once, with 16-byte loads, into shared
-// memory while the row maximum is taken on the way; the digits are then cut from shared memory
-// and written as packed 4-byte words (consecutive threads, consecutive words).  The warp-per-row
-// kernels above read every row twice (the maximum first), and with many rows in flight the
-// second read misses L2.  Used when the launch's widest row fits the shared memory.
-// re (and im) share one row exponent (with -im too when NEG); the diagonal of a single-plane
-// slab is optionally left out (the diagonal split).
-constexpr int kSmemSliceThreads = 512;
-__device__ __forceinline__ double block_max(double v, double* red) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  __syncthreads();   // red may still be read by the previous reduction
-  if ((threadIdx.x & 31) == 0) red[w] = v;
-  __syncthreads();
-  double m = 0.0;
-  for (int i = 0; i < nw; ++i) m = fmax(m, red[i]);
-  return m;
+// ---- grouped slicing of wide rows in two streaming passes.  The warp-per-row kernel above
+// reads a row twice (the maximum first); with thousands of 80 KB rows in flight the second read
+// misses L2, and a warp per row keeps few loads in flight.  Here (1) a warp per row takes the
+// row maximum with four 16-byte loads in flight per lane and writes the row exponent (and the
+// split-off diagonal), and (2) a block per (row, 2048-column chunk) cuts the digits with that
+// exponent: both passes stream at full occupancy.  Digits and exponents are the same as
+// slice_row's.  re (and im) share one row exponent (with -im too when NEG); the diagonal of a
+// single-plane slab is optionally left out (the diagonal split).
+__device__ __forceinline__ int find_slab(const GSlab* slabs, int nslabs, int64_t row) {
+  int lo = 0, hi = nslabs - 1;
+  while (lo < hi) {   // last slab with row0 <= row
+    const int mid = (lo + hi + 1) >> 1;
+    if (slabs[mid].row0 <= row) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
-template <bool NEG>
-__global__ void __launch_bounds__(kSmemSliceThreads, 1)
-    k_slice_rows_smem(const GSlab* slabs, int nslabs, int64_t total_rows, int64_t kmax, int S, I8Slices out) {
-  extern __shared__ __align__(16) double srow[];   // [2][kmax]
-  __shared__ double red[kSmemSliceThreads / 32];
-  for (int64_t row = blockIdx.x; row < total_rows; row += gridDim.x) {
-    int lo = 0, hi = nslabs - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (slabs[mid].row0 <= row) lo = mid;
-      else hi = mid - 1;
+template <typename TI>
+__global__ void __launch_bounds__(256) k_row_exp_grouped(const GSlab* slabs, int nslabs, int64_t total_rows,
+                                                         I8Slices out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (row >= total_rows) return;
+  const GSlab sb = slabs[find_slab(slabs, nslabs, row)];
+  const int64_t local = row - sb.row0;
+  if (local < 0 || local >= sb.rows) return;
+  const int64_t K = sb.K;
+  const TI* re = (const TI*)sb.re + local * sb.ld;
+  const TI* im = sb.im ? (const TI*)sb.im + local * sb.ld : nullptr;
+  int64_t dcol = (sb.diag0 != kNoDiag && out.dg && !im) ? local + sb.diag0 : -1;
+  if (dcol >= K) dcol = -1;
+  const bool vec = ((reinterpret_cast<uintptr_t>(re) | reinterpret_cast<uintptr_t>(im)) & 15) == 0;
+  double mx = 0.0;
+#pragma unroll 4
+  for (int64_t k0 = (int64_t)lane * 4; k0 < K; k0 += 128) {
+    double v[4];
+    load4<TI>(re, k0, K, vec, v);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) mx = fmax(mx, k0 + j == dcol ? 0.0 : fabs(v[j]));
+    if (im) {
+      load4<TI>(im, k0, K, vec, v);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mx = fmax(mx, fabs(v[j]));
     }
-    const GSlab sb = slabs[lo];
-    const int64_t local = row - sb.row0;
-    if (local < 0 || local >= sb.rows) continue;   // the same for the whole CTA
-    const int64_t K = sb.K;
-    const double* re = (const double*)sb.re + local * sb.ld;
-    const double* im = sb.im ? (const double*)sb.im + local * sb.ld : nullptr;
-    const int64_t dcol = (sb.diag0 != kNoDiag && out.dg && !im) ? local + sb.diag0 : -1;
-    const bool has_d = dcol >= 0 && dcol < K;
-    double* s0 = srow;
-    double* s1 = srow + kmax;
-    const bool vec = ((reinterpret_cast<uintptr_t>(re) | reinterpret_cast<uintptr_t>(im)) & 15) == 0 && (K & 1) == 0;
-    double m1 = 0.0;
-    if (vec) {
-      for (int64_t k = 2 * (int64_t)threadIdx.x; k < K; k += 2 * blockDim.x) {
-        double2 a = __ldcs(reinterpret_cast<const double2*>(re + k));
-        if (has_d && k == dcol) a.x = 0.0;
-        if (has_d && k + 1 == dcol) a.y = 0.0;
-        *reinterpret_cast<double2*>(s0 + k) = a;
-        m1 = fmax(m1, fmax(fabs(a.x), fabs(a.y)));
-        if (im) {
-          const double2 b = __ldcs(reinterpret_cast<const double2*>(im + k));
-          *reinterpret_cast<double2*>(s1 + k) = b;
-          m1 = fmax(m1, fmax(fabs(b.x), fabs(b.y)));
-        }
-      }
-    } else {
-      for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
-        const double a = (has_d && k == dcol) ? 0.0 : re[k];
-        s0[k] = a;
-        m1 = fmax(m1, fabs(a));
-        if (im) {
-          const double b = im[k];
-          s1[k] = b;
-          m1 = fmax(m1, fabs(b));
-        }
-      }
-    }
-    m1 = block_max(m1, red);   // also orders the shared row before the digit pass
-    const int e1 = row_exponent(m1);
-    if (threadIdx.x == 0) {
-      out.exp[row] = e1;
-      if (has_d) out.dg[row] = re[dcol];
-    }
-    bool one1;
-    const double sc1 = scale_for(S, e1, one1);
-    const int64_t ld = out.ld;
-    for (int64_t k0 = 4 * (int64_t)threadIdx.x; k0 < K; k0 += 4 * blockDim.x) {
-      double a[4], b[4];
+  }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        a[j] = k0 + j < K ? s0[k0 + j] : 0.0;
-        b[j] = (im && k0 + j < K) ? s1[k0 + j] : 0.0;
-      }
-#pragma unroll
-      for (int plane = 0; plane < 2; ++plane) {
-        if (plane == 1 && !im) continue;
-        const double* x = plane == 0 ? a : b;
-        uint32_t pk[kMaxSlices] = {}, pn[kMaxSlices] = {};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const double xs = one1 ? x[j] * sc1 : ldexp(ldexp(x[j], -e1), 7 * S);
-          int d[kMaxSlices];
-          cut_digits(xs, S, d);
-#pragma unroll
-          for (int q = 0; q < kMaxSlices; ++q)
-            if (q < S) {
-              pk[q] |= ((uint32_t)(uint8_t)(int8_t)d[q]) << (8 * j);
-              if (NEG && plane == 1) pn[q] |= ((uint32_t)(uint8_t)(int8_t)(-d[q])) << (8 * j);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kMaxSlices; ++q) {
-          if (q >= S) continue;
-          int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
-          if (dst) *reinterpret_cast<uint32_t*>(dst + row * ld + k0) = pk[q];
-          if (NEG && plane == 1 && out.neg_im[q]) *reinterpret_cast<uint32_t*>(out.neg_im[q] + row * ld + k0) = pn[q];
-        }
-      }
-    }
-    __syncthreads();   // the next row overwrites the shared row
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) {
+    out.exp[row] = row_exponent(mx);
+    if (dcol >= 0) out.dg[row] = (double)re[dcol];
   }
 }
-constexpr int64_t kSmemSliceBytes = 200 * 1024;
-constexpr int64_t kSmemSliceMinK = 1024;   // narrower rows go to the warp-per-row kernel
-int smem_slice_grid(int64_t total_rows) {
-  const int64_t g = std::min<int64_t>(total_rows, 148 * 2);
-  return (int)std::max<int64_t>(1, g);
+constexpr int kStreamChunk = 2048;   // columns per block of the digit pass (256 threads x 2 x 4)
+template <typename TI, bool NEG>
+__global__ void __launch_bounds__(256) k_slice_stream_grouped(const GSlab* slabs, int nslabs, int S, I8Slices out) {
+  const int64_t row = blockIdx.x;
+  const GSlab sb = slabs[find_slab(slabs, nslabs, row)];
+  const int64_t local = row - sb.row0;
+  if (local < 0 || local >= sb.rows) return;
+  const int64_t K = sb.K;
+  const int64_t base = (int64_t)blockIdx.y * kStreamChunk + 4 * (int64_t)threadIdx.x;
+  if (base >= K) return;
+  const TI* re = (const TI*)sb.re + local * sb.ld;
+  const TI* im = sb.im ? (const TI*)sb.im + local * sb.ld : nullptr;
+  int64_t dcol = (sb.diag0 != kNoDiag && out.dg && !im) ? local + sb.diag0 : -1;
+  if (dcol >= K) dcol = -1;
+  const bool vec = ((reinterpret_cast<uintptr_t>(re) | reinterpret_cast<uintptr_t>(im)) & 15) == 0;
+  // both groups' loads before any digit is cut: four 16-byte loads in flight per thread
+  double x[2][2][4] = {};
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    const int64_t k0 = base + g * (kStreamChunk / 2);
+    if (k0 < K) {
+      load4<TI>(re, k0, K, vec, x[g][0]);
+      if (im) load4<TI>(im, k0, K, vec, x[g][1]);
+    }
+  }
+  const int e = out.exp[row];
+  bool one;
+  const double sc = scale_for(S, e, one);
+  const int64_t ld = out.ld;
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    const int64_t k0 = base + g * (kStreamChunk / 2);
+    if (k0 >= K) continue;
+#pragma unroll
+    for (int plane = 0; plane < 2; ++plane) {
+      if (plane == 1 && !im) continue;
+      uint32_t pk[kMaxSlices] = {}, pn[kMaxSlices] = {};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        double v = x[g][plane][j];
+        if (plane == 0 && k0 + j == dcol) v = 0.0;
+        const double xs = one ? v * sc : ldexp(ldexp(v, -e), 7 * S);
+        int d[kMaxSlices];
+        cut_digits(xs, S, d);
+#pragma unroll
+        for (int q = 0; q < kMaxSlices; ++q)
+          if (q < S) {
+            pk[q] |= ((uint32_t)(uint8_t)(int8_t)d[q]) << (8 * j);
+            if (NEG && plane == 1) pn[q] |= ((uint32_t)(uint8_t)(int8_t)(-d[q])) << (8 * j);
+          }
+      }
+#pragma unroll
+      for (int q = 0; q < kMaxSlices; ++q) {
+        if (q >= S) continue;
+        int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
+        if (dst) *reinterpret_cast<uint32_t*>(dst + row * ld + k0) = pk[q];
+        if (NEG && plane == 1 && out.neg_im[q]) *reinterpret_cast<uint32_t*>(out.neg_im[q] + row * ld + k0) = pn[q];
+      }
+    }
+  }
 }
+// Narrower rows go to the warp-per-row kernel: up to this width the rows in flight fit L2, so
+// its second read of a row is an L2 hit.
+constexpr int64_t kStreamSliceMinK = 1024;
 
 void make_map_u8(CUtensorMap* m, const int8_t* base, int64_t rows, int64_t cols, int64_t ld, int box_rows);
 
@@ -946,29 +942,21 @@ template void launch_slice_rows<double>(int, const double*, const double*, int64
 
 template <typename TI>
 void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, I8Slices out,
-                               bool want_neg_im, cudaStream_t s, int64_t kmax, bool two_planes) {
+                               bool want_neg_im, cudaStream_t s, int64_t kmax, int kind) {
   if (S < 3 || S > kMaxSlices) throw Error{FX_ERR_VALUE, "slice count must be 3, 4 or 5"};
   if (out.ld % 16 != 0) throw Error{FX_ERR_VALUE, "grouped slice: pitch must be a multiple of 16"};
   if (nslabs <= 0 || total_rows <= 0) return;
-  const int64_t sm = (int64_t)sizeof(double) * 2 * kmax;
-  // narrow rows (the Cholesky panels, K = 128) keep the warp-per-row kernel: a warp covers such
-  // a row in one step, where a CTA per row would leave most of its threads idle
-  if (std::is_same<TI, double>::value && kmax >= kSmemSliceMinK && kmax % 4 == 0 && sm <= kSmemSliceBytes) {
-    static bool attr = false;
-    if (!attr) {
-      FX_CUDA(cudaFuncSetAttribute(k_slice_rows_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)kSmemSliceBytes));
-      FX_CUDA(cudaFuncSetAttribute(k_slice_rows_smem<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)kSmemSliceBytes));
-      attr = true;
-    }
-    (void)two_planes;
+  if (kind < 0) kind = kmax >= kStreamSliceMinK ? 1 : 0;
+  if (kind == 1) {
+    if (kmax <= 0) throw Error{FX_ERR_VALUE, "grouped slice: the streaming kernel needs the widest row"};
+    const unsigned g1 = (unsigned)cdiv(total_rows, 8);
+    const dim3 g2((unsigned)total_rows, (unsigned)cdiv(kmax, kStreamChunk));
+    k_row_exp_grouped<TI><<<g1, 256, 0, s>>>(slabs, nslabs, total_rows, out);
+    FX_LAUNCH_CHECK();
     if (want_neg_im)
-      k_slice_rows_smem<true><<<smem_slice_grid(total_rows), kSmemSliceThreads, sm, s>>>(slabs, nslabs, total_rows,
-                                                                                           kmax, S, out);
+      k_slice_stream_grouped<TI, true><<<g2, 256, 0, s>>>(slabs, nslabs, S, out);
     else
-      k_slice_rows_smem<false><<<smem_slice_grid(total_rows), kSmemSliceThreads, sm, s>>>(slabs, nslabs, total_rows,
-                                                                                            kmax, S, out);
+      k_slice_stream_grouped<TI, false><<<g2, 256, 0, s>>>(slabs, nslabs, S, out);
     FX_LAUNCH_CHECK();
     return;
   }
@@ -979,9 +967,9 @@ void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t to
   FX_LAUNCH_CHECK();
 }
 template void launch_slice_rows_grouped<float>(int, const GSlab*, int, int64_t, I8Slices, bool, cudaStream_t,
-                                               int64_t, bool);
+                                               int64_t, int);
 template void launch_slice_rows_grouped<double>(int, const GSlab*, int, int64_t, I8Slices, bool, cudaStream_t,
-                                                int64_t, bool);
+                                                int64_t, int);
 
 
 namespace {

@@ -250,10 +250,14 @@ struct PipeOpts {
   int form = FX_FORM_PLAIN;  // FX_FORM_MIXED: two-product squarings with the slice schedule below
   int sq_n4 = 0, sq_n3 = 0;  // mixed form: the last sq_n3 squarings at 3 slices, the sq_n4 before at 4
   int pade_slices = 5;       // mixed form: slices of the Pade and solve products
+  int newton_slices = 5;     // mixed form: slices of the Newton-Schulz steps that leave a residual
+                             // above 1e-3 (the later ones take pade_slices)
+  int solve = 0;             // Pade solve: 0 by form and size, 1 Cholesky, 2 Newton-Schulz
   bool drift = false;        // diagnostics: unitarity residual after every squaring
 };
-// Default slice schedule of the mixed form (see fx_batch.cu, BatchPipeline::sq_slices).
-constexpr int kMixedN4 = 64, kMixedN3 = 0, kMixedPade = 4;
+// Default slice schedule of the mixed form (see fx_batch.cu, BatchPipeline::sq_slices and
+// BatchPipeline::newton_solve).
+constexpr int kMixedN4 = 8, kMixedN3 = 0, kMixedPade = 4, kMixedNewton = 3;
 void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, void* dpsi, void* dU,
                         const PipeOpts& o, cudaStream_t s);
 void batch_pipeline_stats(const BatchPipeline* p, fx_stats* st);
@@ -302,11 +306,13 @@ struct GSlab {
                         // which is left out of the slices and written to I8Slices::dg
 };
 constexpr int kNoDiag = -(1 << 30);
-// kmax: the widest slab (K) of the launch, when known (> 0): rows whose planes fit the shared
-// memory are then sliced by the shared-memory kernel (one HBM read per row).
+// kmax: the widest slab (K) of the launch, when known (> 0): launches with rows of 1024 columns
+// or more are sliced in two streaming passes (row exponents, then digits over row chunks).
+// kind: -1 by kmax as above, 0 the warp-per-row kernel, 1 the two streaming passes (both give
+// the same digits; the choice is for the kernel tests).
 template <typename TI>
 void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, I8Slices out,
-                               bool want_neg_im, cudaStream_t s, int64_t kmax = 0, bool two_planes = true);
+                               bool want_neg_im, cudaStream_t s, int64_t kmax = 0, int kind = -1);
 // In place A <- (A + A^T) / 2 of an n x n plane (exact symmetry of a result known to be
 // symmetric in exact arithmetic).
 template <typename T>

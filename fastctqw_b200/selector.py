@@ -24,9 +24,10 @@ It is trained on the GPU on labels *measured* by the engine (``make_dataset_meas
 training walk runs at a grid of forced (m, s) and its result is compared with the FP64
 eigendecomposition on the state that exposes the truncation error most, the equal superposition
 of the eigenvectors at the two ends of the spectrum; the label is the cheapest (m, s) whose
-infidelity stays <= 1e-10.  At run time a proposal is used only when it is cheaper than the plain
-choice, the phase bound at min(rho_up, 1.1 rho_L) stays below 1e-5 (``gate``) and the result
-passes the a-posteriori checks; otherwise the plain (m, s) is used.
+infidelity stays <= 1e-10.  At run time a proposal is used only when it is cheaper than the
+estimated choice (the phase bound at min(rho_up, 1.1 rho_L), at 1e-6), that bound at the proposal
+stays below 1e-5 (``gate``) and the result passes the a-posteriori checks; otherwise the
+estimated choice (or the plain one, when that is cheaper) is used.
 
 Features (per walk): log2 n, log2 ||Y||_1, log2 (||X||_F / sqrt n), log2 (1 + max off-diagonal
 nonzeros of a row), log2 rho_L, rank-one shift flag, log2 d4, log2 d6.
@@ -263,14 +264,23 @@ def rho_gate(features: np.ndarray) -> np.ndarray:
 
 
 def gate(features, plain_m, plain_s, prop_m, prop_s) -> np.ndarray:
-    """Selection outcome per walk, as the engine decides it: 2 accepted, -1 rejected by the
-    bound, 0 not cheaper than the plain choice."""
+    """Selection outcome per walk, as the engine decides it: 2 proposal accepted, 3 estimated
+    choice (the proposal rejected by the bound or not cheaper), -1 rejected with the plain
+    choice kept, 0 plain choice (nothing cheaper)."""
     r = rho_gate(features)
+    em, es = estimated_choice(features)
     out = np.zeros(len(r), dtype=np.int32)
     for i in range(len(r)):
+        cost = PRODUCTS[int(plain_m[i])] + int(plain_s[i])
+        if PRODUCTS[int(em[i])] + int(es[i]) < cost:
+            out[i] = 3
+            cost = PRODUCTS[int(em[i])] + int(es[i])
         pm, ps = int(prop_m[i]), int(prop_s[i])
-        if PRODUCTS[pm] + ps < PRODUCTS[int(plain_m[i])] + int(plain_s[i]):
-            out[i] = 2 if certified(pm, ps, float(r[i]), GATE_TOL) else -1
+        if PRODUCTS[pm] + ps < cost:
+            if certified(pm, ps, float(r[i]), GATE_TOL):
+                out[i] = 2
+            elif out[i] != 3:
+                out[i] = -1
     return out
 
 

@@ -44,16 +44,15 @@ def evaluate(w, ds) -> dict:
     em, es = selector.estimated_choice(ds["features"])
     est = np.minimum(plain, products(em, es))
     label = products(ds["label_m"], ds["label_s"])
-    learned = np.where(outcome == 2, products(pm, ps), plain)
-    cheaper = outcome != 0
+    learned = np.where(outcome == 2, products(pm, ps), np.where(outcome == 3, est, plain))
     return {
         "instances": int(len(plain)),
         "label_m_accuracy": float(np.mean(pm == ds["label_m"])),
         "label_s_accuracy": float(np.mean(ps == ds["label_s"])),
         "label_s_mae": float(np.mean(np.abs(out[:, 5] - ys))),
-        "proposals_cheaper_than_plain": int(cheaper.sum()),
         "accepted": int((outcome == 2).sum()),
-        "rejected_by_gate": int((outcome == -1).sum()),
+        "estimated_fallback": int((outcome == 3).sum()),
+        "rejected_plain_kept": int((outcome == -1).sum()),
         "below_measured_label": int(np.sum((outcome == 2) & (products(pm, ps) < label))),
         "products_per_walk": {"plain": float(plain.mean()), "certified": float(cert.mean()),
                               "estimated": float(est.mean()), "learned": float(learned.mean()),

@@ -62,9 +62,10 @@ enum fx_form {
                          generators X = i*(real symmetric): int8 slices on FP64 masters
                          with the diagonals split off and added in FP64, 4 slices for the
                          powers, Pade and solve products (FX_OPT_PADE_SLICES), the solve
-                         by a Newton-Schulz inverse, each squaring as three symmetric
-                         products Re^2, Im^2, (Re+Im)^2 at 4 slices (5 for squarings
-                         before the last FX_OPT_SQ_N4, 3 for the last FX_OPT_SQ_N3).
+                         by a Newton-Schulz inverse for n >= 4096, each squaring as
+                         three symmetric products Re^2, Im^2, (Re+Im)^2 at 4 slices (5
+                         for squarings before the last FX_OPT_SQ_N4, 3 for the last
+                         FX_OPT_SQ_N3).
                          Other inputs: BF16 hi+lo split, 3 products (hi*hi, hi*lo,
                          lo*hi), FP32 accumulate, FP32 masters                        */
   FX_FORM_SIMT = 2,   /* CUDA-core FP32 FMA products, FP32 masters (checker)          */
@@ -89,27 +90,35 @@ enum fx_option {
                              0 Al-Mohy & Higham (default), 1 the cheapest (m, s) the
                              truncation bound certifies at phase error 1e-6 from the
                              rigorous spectral bound min(||Y||_1, d4, d6), 2 the learned
-                             MLP proposal, accepted only when the phase bound at
-                             min(rigorous bound, 1.1 x the Lanczos estimate) stays below
-                             1e-5 (infidelity <= 1e-10 for every state) and the result
-                             passes the a-posteriori checks (else option 0), 3 the
-                             same phase bound at a Lanczos estimate of the spectral radius
-                             (30 steps, two starts) raised by 10% (estimated selection) */
+                             MLP proposal, used when it is cheaper than option 3's choice,
+                             the phase bound at min(rigorous bound, 1.1 x the Lanczos
+                             estimate) stays below 1e-5 (infidelity <= 1e-10 for every
+                             state) and the result passes the a-posteriori checks (else
+                             option 3), 3 the same phase bound at a Lanczos estimate of the
+                             spectral radius (30 steps, two starts) raised by 10%, at 1e-6
+                             (estimated selection)                                     */
   FX_OPT_INJECT_STALL = 11, /* diagnostics of the failure path (walk generators): k >= 0 makes
                              the k-th product launch of every run leave out the operand
                              loads of one K step, so that its bounded waits run out and
                              the run returns FX_ERR_TIMEOUT; -1 (default) off          */
   FX_OPT_SQ_N4 = 12,      /* mixed form, walk generators: how many squarings before the
-                             3-slice ones run at 4 slices (default 64: all; the earlier
-                             ones run at 5)                                            */
+                             3-slice ones run at 4 slices (default 8; the earlier ones,
+                             whose errors later squarings amplify most, run at 5)      */
   FX_OPT_SQ_N3 = 13,      /* mixed form, walk generators: how many of the last squarings run
                              at 3 slices (default 0)                                   */
   FX_OPT_DRIFT = 14,      /* diagnostics (walk generators): 1 records the unitarity residual
                              ||U_k^H U_k - I||_F / sqrt(n) after every squaring k = 0..s
                              (fx_unitarity_drift), at the cost of two extra products per
                              squaring                                                  */
-  FX_OPT_PADE_SLICES = 15 /* mixed form, walk generators: int8 slices of the powers, Pade and
+  FX_OPT_PADE_SLICES = 15, /* mixed form, walk generators: int8 slices of the powers, Pade and
                              solve products (4 default, 5 or 3)                        */
+  FX_OPT_NEWTON_SLICES = 16, /* mixed form, walk generators: int8 slices of the Newton-Schulz
+                             steps of the solve whose model residual stays above 1e-3 (3
+                             default, 4 or 5; the later steps take FX_OPT_PADE_SLICES) */
+  FX_OPT_SOLVE = 17       /* walk generators: solve of the Pade step R = G^-1 P^2 (G SPD):
+                             0 (default) Newton-Schulz for mixed-form walks padded to 4096
+                             or more, blocked Cholesky otherwise; 1 Cholesky; 2
+                             Newton-Schulz                                             */
 };
 
 /* What the last run did. */
@@ -134,8 +143,9 @@ typedef struct fx_stats {
   int32_t prod_launches;
   int32_t reserved2;
   int32_t selector;     /* FX_OPT_SELECTOR of the run                                  */
-  int32_t sel_outcome;  /* 0 plain, 1 certified, 2 learned accepted, 3 estimated, -1 learned
-                           rejected by the bound, -2 failed an a-posteriori check
+  int32_t sel_outcome;  /* 0 plain, 1 certified, 2 learned accepted, 3 estimated (also a
+                           learned proposal that was rejected or not cheaper), -1 learned
+                           rejected by the bound with no estimated choice cheaper than plain, -2 failed an a-posteriori check
                            (Cholesky of Q^H Q or unitarity) and was redone with the plain
                            (m, s)                                                   */
   int32_t plain_m;      /* (m, s) of the Al-Mohy & Higham selection                    */
@@ -167,8 +177,10 @@ int fx_product_profile(fx_handle h, int32_t* tags, double* ms, double* ops, int3
 int fx_unitarity_drift(fx_handle h, double* out, int32_t cap, int32_t* count);
 /* Spectral-radius estimates of the shifted generator of the last walk-generator run: a Lanczos
  * estimate (30 steps from two pseudo-random starts; Ritz values lie inside the spectrum, so it
- * does not exceed the radius) and the rigorous upper bound min(||Y||_1, d4, d6).  Diagnostics
- * of the (m, s) selection; no counterpart in the reference. */
+ * does not exceed the radius) and the rigorous upper bound min(||Y||_1, d4, d6).  The Lanczos
+ * estimate runs only where it is used (the learned and estimated selections, the mixed form);
+ * elsewhere *rho_lanczos is 0.  Diagnostics of the (m, s) selection; no counterpart in the
+ * reference. */
 int fx_spectral_radius(fx_handle h, double* rho_lanczos, double* rho_up);
 
 /* U = expm(A), both host buffers of n*n elements of the handle's dtype. */
@@ -193,6 +205,19 @@ int fx_product_f32(int form, int64_t M, int64_t N, int64_t K, const float* A, in
                    const float* Bt, int64_t ldb, float alpha, float beta, const float* C,
                    int64_t ldc, float gamma, float* D, int64_t ldd, void* stream);
 const char* fx_product_error(void);
+
+/* Diagnostics (no counterpart in the reference): the grouped int8 slicer of the product kernels
+ * on one block of `rows` rows of FP64 planes (device buffers, row pitch ld elements).  Each row
+ * is scaled by 2^(7S - e), e its exponent (as the products use it), and cut into S signed
+ * digits from the top with round-half-even.  kind 0: warp-per-row kernel, 1: the two streaming
+ * passes (row exponents, then digits over row chunks) that rows of 1024 columns or more take;
+ * both give the same digits.  im may be null; split_diag (single plane, dg non-null) leaves row
+ * r's element at column r out of the slices and writes it to dg[r]; neg (im non-null) also
+ * writes the digits of -im.  out: 3 S planes of rows x ldo bytes (re digits 0..S-1, im, -im;
+ * ldo >= K, a multiple of 16), exps: rows int32.  Messages through fx_product_error. */
+int fx_slice_rows_f64(int kind, int S, const double* re, const double* im, int64_t ld, int64_t rows,
+                      int64_t K, int split_diag, int neg, int8_t* out, int64_t ldo, int32_t* exps,
+                      double* dg, void* stream);
 
 /* Measured dense tensor-core rate of the current GPU (diagnostics; no counterpart in the
  * reference): one CTA per SM issues `iters` (1..2^20) x 2 tcgen05.mma of M = 128, N = 256, K = 32 bytes
@@ -245,8 +270,11 @@ enum fx_batch_option {
   FX_BATCH_OPT_SQ_N4 = 11,       /* mixed form: squarings at 4 slices (as FX_OPT_SQ_N4)          */
   FX_BATCH_OPT_SQ_N3 = 12,       /* mixed form: last squarings at 3 slices (as FX_OPT_SQ_N3)     */
   FX_BATCH_OPT_DRIFT = 13,       /* diagnostics: per-squaring unitarity residual (as FX_OPT_DRIFT) */
-  FX_BATCH_OPT_PADE_SLICES = 14  /* mixed form: slices of the Pade and solve products (as        */
+  FX_BATCH_OPT_PADE_SLICES = 14, /* mixed form: slices of the Pade and solve products (as        */
                                  /* FX_OPT_PADE_SLICES)                                         */
+  FX_BATCH_OPT_NEWTON_SLICES = 15, /* mixed form: slices of the early Newton-Schulz steps (as    */
+                                  /* FX_OPT_NEWTON_SLICES)                                      */
+  FX_BATCH_OPT_SOLVE = 16         /* solve of the Pade step (as FX_OPT_SOLVE)                   */
 };
 /* count walks of sizes n[0..count); dtype FX_C64 or FX_C128 (of X, psi0 and psi). */
 int fx_batch_create(size_t count, const int64_t* n, int dtype, fx_batch_handle* out);

@@ -134,6 +134,7 @@ def test_estimated_selection_uses_the_lanczos_radius():
         assert eo.infidelity(U.astype(np.complex128) @ p, Uref @ p) <= INFID
     dev = torch.device("cuda", 0)
     e = Engine(n, np.complex64)
+    e.configure(selector="estimated")
     dX = torch.from_numpy(X).to(dev)
     p0 = torch.zeros(n, dtype=torch.complex64, device=dev)
     p0[0] = 1.0

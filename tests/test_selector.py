@@ -103,13 +103,20 @@ def test_learned_gate_and_estimated_rule_use_the_lanczos_radius():
     from fastctqw_b200 import selector
     f = np.zeros((1, 8), dtype=np.float64)
     f[0, 1] = f[0, 6] = f[0, 7] = np.log2(3000.0)   # rho_up = 3000
-    f[0, 4] = np.log2(1000.0)                        # rho_L = 1000 -> 1100 with the margin
+    f[0, 4] = np.log2(800.0)                         # rho_L = 800 -> 880 with the margin
     m, s = selector.estimated_choice(f)
-    assert (m[0], s[0]) == selector.certified_choice(1100.0)
+    assert (m[0], s[0]) == selector.certified_choice(880.0)
     mr, sr = selector.certified_choice(3000.0)
     assert selector.PRODUCTS[int(m[0])] + s[0] < selector.PRODUCTS[mr] + sr
-    pm, ps = selector.certified_choice(1100.0, selector.GATE_TOL)
+    # a proposal at the gate's own tolerance is cheaper than the estimated choice: accepted
+    pm, ps = selector.certified_choice(880.0, selector.GATE_TOL)
+    assert selector.PRODUCTS[pm] + ps < selector.PRODUCTS[int(m[0])] + s[0]
     out = selector.gate(f, np.array([13]), np.array([12]), np.array([pm]), np.array([ps]))
     assert out[0] == 2
-    out = selector.gate(f, np.array([13]), np.array([12]), np.array([13]), np.array([ps - 1]))
-    assert out[0] == -1
+    # one squaring fewer fails the gate: the estimated choice is used
+    out = selector.gate(f, np.array([13]), np.array([12]), np.array([pm]), np.array([ps - 1]))
+    assert out[0] == 3
+    # with a plain choice cheaper than the estimated one, a rejected proposal keeps the plain one
+    cp = selector.PRODUCTS[int(m[0])] + s[0] - 1
+    out = selector.gate(f, np.array([13]), np.array([cp - 6]), np.array([pm]), np.array([ps - 1]))
+    assert out[0] == (-1 if selector.PRODUCTS[pm] + ps - 1 < cp else 0)
