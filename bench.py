@@ -659,7 +659,10 @@ def main():
     achieved = pst["prod_ops"] / (pst["prod_ms"] * 1e-3) / 1e12 if pst["prod_ms"] > 0 else None
     traffic = product_traffic_per_launch(args.form)
     roofline = {
-        "bound": "tensor", "kernel": "k_gemm_i8<5,double> (int8 Ozaki-slice product, exact accumulation)",
+        "bound": "tensor",
+        "kernel": ("k_gemm_i8<4,double> and <3,double> (int8 Ozaki-slice products, exact accumulation; "
+                   "4 slices, the early Newton-Schulz steps 3)" if args.form == "mixed" else
+                   "k_gemm_i8<5,double> (int8 Ozaki-slice product, exact accumulation)"),
         "achieved": round(achieved, 1) if achieved else None, "peak": round(int8_peak, 1), "unit": "TOP/s (int8)",
         "frac": round(achieved / int8_peak, 3) if achieved else None,
         "peak_source": "measured on this GPU by fx_tensor_peak (tcgen05.mma kind::i8 M128 N256, operands in "

@@ -1005,8 +1005,10 @@ class BatchPipeline {
     *order = tile_order_;
   }
   const std::vector<std::array<double, 3>>& tuned() const { return tuned_; }
-  // Diagonal split of the solve's products, a mask: 1 V^2, W^2, VW; 2 the complex products
-  // P2 L^-T and Z L^-1 (default 3); changing it re-records both phases.
+  // Diagonal split, a mask: 1 the real products (V^2, W^2, VW, and every product of the mixed
+  // form); 2 the complex products P2 L^-T and Z L^-1; 4 the plain form's powers and Pade
+  // products; 8 the plain form's squarings as three split products (as the mixed form's).
+  // Default 3; changing it re-records both phases.
   void set_diag_split(int v) {
     if (v == split_) return;
     split_ = v;
@@ -1745,7 +1747,7 @@ class BatchPipeline {
     // the mixed form's slice count, with the diagonals split off (the shifted generator's rows
     // are dominated by their diagonal, and its powers' even more)
     gS_ = form_ == 1 ? pade_S_ : kS;
-    const bool psplit = form_ == 1;
+    const bool psplit = form_ == 1 || (split_ & 4);
     product(st, r, all, kY, kY, -1.0, -1, 0.0, 0.0, kA2, true, nullptr, nullptr, psplit);
     product(st, r, all, kA2, kA2, 1.0, -1, 0.0, 0.0, kA4, true, nullptr, nullptr, psplit);
     product(st, r, all, kA4, kA2, 1.0, -1, 0.0, 0.0, kA6, true, nullptr, nullptr, psplit);
@@ -2119,7 +2121,7 @@ class BatchPipeline {
     // the Pade and solve products: 5 slices, or the mixed form's count; the mixed form also takes
     // the (dominant) diagonals of the Pade products' operands out of their slices
     gS_ = form_ == 1 ? pade_S_ : kS;
-    const bool psplit = form_ == 1;
+    const bool psplit = form_ == 1 || (split_ & 4);
     // m = 9: A8 = A4 A4 -> T2
     tag_ = kTagPade;
     product(st, r, m9, kA4, kA4, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, psplit);
@@ -2228,7 +2230,7 @@ class BatchPipeline {
       for (int w = 0; w < W; ++w)
         if (sel_s_[w] > k) act.push_back(w);
       if (drift_) drift(st, r, act, er, ei, std::vector<int>(W, std::min(k, kDriftMax - 1)));
-      if (form_ == 1)
+      if (form_ == 1 || (split_ & 8))
         square3(st, r, act, er, ei, tr, ti, k);
       else
         square(st, r, act, er, ei, tr, ti);
@@ -2486,6 +2488,7 @@ class BatchPipeline {
   static constexpr double kNewtonLoRes = 1e-3;
   // Slice count of squaring k (0-based) of walk w in the mixed form.
   int sq_slices(int w, int k) const {
+    if (form_ != 1) return kS;
     const int rem = sel_s_[w] - k;   // 1 for the last squaring
     return rem <= sq_n3_ ? 3 : rem <= sq_n3_ + sq_n4_ ? 4 : kS;
   }
@@ -2965,8 +2968,8 @@ int fx_batch_set_option(fx_batch_handle b, int key, double value) {
       return FX_OK;
     }
     case FX_BATCH_OPT_DIAG_SPLIT:
-      if (value != 0 && value != 1 && value != 2 && value != 3)
-        return bfail(b, fx::Error{FX_ERR_VALUE, "diagonal split must be a mask of 1 and 2"});
+      if (value < 0 || value > 15 || value != (double)(int)value)
+        return bfail(b, fx::Error{FX_ERR_VALUE, "diagonal split must be a mask of 1, 2, 4 and 8"});
       b->p->set_diag_split((int)value);
       return FX_OK;
     case FX_BATCH_OPT_FORM:

@@ -257,9 +257,12 @@ enum fx_batch_option {
   FX_BATCH_OPT_FORCE_M = 2,     /* diagnostics: force the Pade degree (-1 automatic)            */
   FX_BATCH_OPT_SELECTOR = 3,    /* as FX_OPT_SELECTOR                                           */
   FX_BATCH_OPT_ANALYZE_ONLY = 4, /* 1: stop after the selection (features and (m, s) only)      */
-  FX_BATCH_OPT_DIAG_SPLIT = 5,   /* mask, default 3: products of the solve that take their       */
-                                 /* operands' diagonals out of the int8 slices and add those    */
-                                 /* terms in FP64; 1 V^2, W^2, VW; 2 P2 L^-T and Z L^-1          */
+  FX_BATCH_OPT_DIAG_SPLIT = 5,   /* mask, default 3: products that take their operands'          */
+                                 /* diagonals out of the int8 slices and add those terms in     */
+                                 /* FP64; 1 the real products (V^2, W^2, VW; all of the mixed   */
+                                 /* form's), 2 P2 L^-T and Z L^-1, 4 the plain form's powers     */
+                                 /* and Pade products, 8 the plain form's squarings as three   */
+                                 /* split products Re^2, Im^2, (Re+Im)^2 (as the mixed form's)  */
   FX_BATCH_OPT_AUTOTUNE = 6,     /* 1: at the next run, time the candidate schedules of the     */
                                  /* post-selection products on this batch and keep the fastest */
   FX_BATCH_OPT_TILE_GROUP = 7,   /* schedule: tiles in G x G blocks, G = 4, 8 (default) or 16    */
