@@ -51,7 +51,7 @@ class WalkBatch:
     """Owner of one ``fx_batch`` handle: device workspace for walks of sizes ``ns``."""
 
     def __init__(self, ns, dtype=np.complex64, graph: bool = True, selector: str = "plain",
-                 analyze_only: bool = False, diag_split: int = 3, autotune: bool = False,
+                 analyze_only: bool = False, diag_split: int = 7, autotune: bool = False,
                  form: str = "plain", sq_n4: int | None = None, sq_n3: int | None = None,
                  drift: bool = False, pade_slices: int | None = None,
                  newton_slices: int | None = None, solve: str = "auto") -> None:
@@ -69,7 +69,7 @@ class WalkBatch:
             self.set_option(OPT_SELECTOR, _native.SELECTORS[selector])
         if analyze_only:
             self.set_option(OPT_ANALYZE_ONLY, 1)
-        if int(diag_split) != 3:
+        if int(diag_split) != 7:
             self.set_option(OPT_DIAG_SPLIT, int(diag_split))
         if autotune:
             self.set_option(OPT_AUTOTUNE, 1)

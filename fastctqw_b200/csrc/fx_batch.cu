@@ -38,9 +38,25 @@ namespace {
 constexpr int kS = 5;          // int8 slices (FP64 masters)
 constexpr int kNb = 128;       // Cholesky / inverse block
 constexpr int kEstScratch = 8; // doubles per row of a walk in the estimator scratch
-// The mixed form's Newton-Schulz solve serves walks padded to at least this size; below it the
-// blocked Cholesky has few steps (np / 128), which run grouped over the batch.
+// The mixed form's reduced slice counts (and its Newton-Schulz solve) serve walks padded to at
+// least this size.  Below it the products are short and their epilogues weigh as much as their
+// MMAs, so fewer slices save little, and the blocked Cholesky has few steps (np / 128), which
+// run grouped over the batch: smaller walks keep the plain schedule in either form.
+constexpr int kMixedMinNp = 4096;
+// The mixed form's Pade and solve products run at its reduced slice count only when the
+// selection takes at most this many squarings (their errors are amplified 2^s); above it, 5.
+constexpr int kMixedMaxPadeS = 10;
+// Walks padded to at least this size solve the Pade step by Newton-Schulz (either form).
 constexpr int kNewtonMinNp = 4096;
+// Walks padded to at least this size, or whose selection takes at least kSquare3MinS squarings,
+// square in the three-product form (Re^2, Im^2, (Re+Im)^2, each with the diagonal split) in
+// either form.  Large walks: three products instead of four, and at these sizes the products'
+// MMAs outweigh their epilogues.  Long chains: the split keeps the iterate's dominant diagonal
+// out of the slices, and the 2^(s-k) amplification of squaring k's error needs those bits (on
+// walks with 15 to 17 squarings the exact complex square left infidelities near 1e-10, the
+// split form 2e-11 and below).
+constexpr int kSquare3MinNp = 4096;
+constexpr int kSquare3MinS = 12;
 
 struct BWalk {
   int n, np;
@@ -51,6 +67,9 @@ struct BWalk {
 // ------------------------------------------------------------------ grouped elementwise
 struct Planes4 {
   const double* m[4];
+};
+struct Planes5 {
+  const double* m[5];
 };
 
 // Elementwise work over walks of uneven sizes is cut into row chunks of about kChunkElems
@@ -92,6 +111,52 @@ __global__ void kb_combo(double* D, Planes4 M, const RChunk* ch, const BWalk* wk
     if (2 * (int64_t)c2 == r) vx += g;
     else if (2 * (int64_t)c2 + 1 == r) vy += g;
     dst[e2] = make_double2(vx, vy);
+  }
+}
+
+// Two linear combinations of the same planes in one pass: D1 = sum_k c_k M_k (+ g1 on the
+// diagonal), D2 = sum_k d_k M_k (+ g2); coef[12 w ..] = (c_0..c_4, g1, d_0..d_4, g2).  A plane
+// whose coefficients are both zero is not read.
+__global__ void kb_combo2(double* D1, double* D2, Planes5 M, const RChunk* ch, const BWalk* wk, const double* coef) {
+  const RChunk q = ch[blockIdx.x];
+  const BWalk b = wk[q.w];
+  const double* c = coef + 12 * q.w;
+  const uint32_t half = (uint32_t)b.np / 2, total = (uint32_t)(q.r1 - q.r0) * half;
+  const double2* src[5];
+  double c1[5], c2[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const bool on = M.m[k] && (c[k] != 0.0 || c[6 + k] != 0.0);
+    c1[k] = on ? c[k] : 0.0;
+    c2[k] = on ? c[6 + k] : 0.0;
+    src[k] = on ? reinterpret_cast<const double2*>(M.m[k] + b.off) : nullptr;
+  }
+  const double g1 = c[5], g2 = c[11];
+  double2* d1 = reinterpret_cast<double2*>(D1 + b.off);
+  double2* d2 = reinterpret_cast<double2*>(D2 + b.off);
+  for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
+    const uint32_t rr = t / half, c2i = t - rr * half;
+    const int64_t r = q.r0 + (int64_t)rr;
+    const int64_t e2 = r * half + c2i;   // double2 index of (r, 2 c2i)
+    double ax = 0.0, ay = 0.0, bx = 0.0, by = 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+      if (src[k]) {
+        const double2 m = src[k][e2];
+        ax += c1[k] * m.x;
+        ay += c1[k] * m.y;
+        bx += c2[k] * m.x;
+        by += c2[k] * m.y;
+      }
+    if (2 * (int64_t)c2i == r) {
+      ax += g1;
+      bx += g2;
+    } else if (2 * (int64_t)c2i + 1 == r) {
+      ay += g1;
+      by += g2;
+    }
+    d1[e2] = make_double2(ax, ay);
+    d2[e2] = make_double2(bx, by);
   }
 }
 
@@ -972,12 +1037,19 @@ class BatchPipeline {
   void set_profile(bool p) { profile_ = p; }
   // 0 plain (Al-Mohy & Higham), 1 certified bound, 2 learned (gated by the bound), 3 estimated.
   // Phase 1 runs the Lanczos estimate only where a selection or the form needs it.
+  // Phase 1 runs the 1-norm estimates of A^8 and A^10 only where the Al-Mohy & Higham
+  // selection itself is made (plain and certified selections, analyze-only runs); the
+  // estimated and learned selections take the plain choice, their fallback, from the bounds
+  // ||A^8|| <= ||A^4||^2 and ||A^10|| <= ||A^4|| ||A^6|| (a choice with as many squarings or
+  // more).
   void set_selector(int k) {
-    const bool before = needs_lanczos();
+    const int before = phase1_needs();
     selector_ = k;
-    if (needs_lanczos() != before) rerecord_phase1();
+    if (phase1_needs() != before) rerecord_phase1();
   }
   bool needs_lanczos() const { return selector_ >= 2 || form_ == 1 || analyze_only_; }
+  bool needs_estimates() const { return selector_ <= 1 || analyze_only_; }
+  int phase1_needs() const { return (needs_lanczos() ? 1 : 0) | (needs_estimates() ? 2 : 0); }
   void rerecord_phase1() {
     if (graph1_) cudaGraphExecDestroy(graph1_);
     graph1_ = nullptr;
@@ -989,9 +1061,9 @@ class BatchPipeline {
   }
   // Stop after the selection (statistics, norms, estimates, features; no exponential).
   void set_analyze_only(bool a) {
-    const bool before = needs_lanczos();
+    const int before = phase1_needs();
     analyze_only_ = a;
-    if (needs_lanczos() != before) rerecord_phase1();
+    if (phase1_needs() != before) rerecord_phase1();
   }
   // Phase-2 schedule: tune it at the next run, or set it.
   void set_autotune(bool a) { autotune_ = a; }
@@ -1008,7 +1080,7 @@ class BatchPipeline {
   // Diagonal split, a mask: 1 the real products (V^2, W^2, VW, and every product of the mixed
   // form); 2 the complex products P2 L^-T and Z L^-1; 4 the plain form's powers and Pade
   // products; 8 the plain form's squarings as three split products (as the mixed form's).
-  // Default 3; changing it re-records both phases.
+  // Default 7; changing it re-records both phases.
   void set_diag_split(int v) {
     if (v == split_) return;
     split_ = v;
@@ -1043,8 +1115,8 @@ class BatchPipeline {
     if (rerecord) rerecord_phase1();
   }
   int pade_slices() const { return pade_S_; }
-  // Solve of the walk-generator Pade step: 0 Newton-Schulz for mixed-form walks padded to 4096
-  // or more and Cholesky otherwise, 1 Cholesky, 2 Newton-Schulz.
+  // Solve of the walk-generator Pade step: 0 Newton-Schulz for walks padded to 4096 or more and
+  // Cholesky otherwise, 1 Cholesky, 2 Newton-Schulz.
   void set_solve(int mode) {
     if (mode == solve_mode_) return;
     solve_mode_ = mode;
@@ -1137,6 +1209,11 @@ class BatchPipeline {
     for (int w = 0; w < W && lan; ++w) {
       const double* base = lan_host_.data() + (size_t)w * 4 * kLanSteps;
       rho_lan_[w] = std::max(tridiag_radius(base, kLanSteps), tridiag_radius(base + 2 * kLanSteps, kLanSteps));
+    }
+    for (int w = 0; w < W && !est_recorded_; ++w) {   // bounds in place of the estimates
+      double* nw = norms_.data() + 8 * w;
+      nw[3] = nw[1] * nw[1];
+      nw[4] = nw[1] * nw[2];
     }
     for (int w = 0; w < W; ++w) {
       if (h_flags[w] & 4) throw Error{FX_ERR_NONFINITE, "input " + std::to_string(w) + " contains NaN or Inf"};
@@ -1506,8 +1583,9 @@ class BatchPipeline {
   std::vector<double> features_;
   int selector_ = 0;
   bool lan_recorded_ = false;   // phase 1 as recorded runs the Lanczos estimate
+  bool est_recorded_ = true;    // phase 1 as recorded runs the 1-norm estimates of A^8, A^10
   bool analyze_only_ = false;
-  int split_ = 3;
+  int split_ = 7;
   int tile_group_ = 8, tile_order_ = 0;   // phase-2 schedule of the grouped products
   int sample_walks_ = 2, sample_count_ = 0;   // sampled comparison with the plain method
   double sample_max_infid_ = 0.0;
@@ -1746,12 +1824,12 @@ class BatchPipeline {
     tag_ = kTagPowers;
     // the mixed form's slice count, with the diagonals split off (the shifted generator's rows
     // are dominated by their diagonal, and its powers' even more)
-    gS_ = form_ == 1 ? pade_S_ : kS;
     const bool psplit = form_ == 1 || (split_ & 4);
-    product(st, r, all, kY, kY, -1.0, -1, 0.0, 0.0, kA2, true, nullptr, nullptr, psplit);
-    product(st, r, all, kA2, kA2, 1.0, -1, 0.0, 0.0, kA4, true, nullptr, nullptr, psplit);
-    product(st, r, all, kA4, kA2, 1.0, -1, 0.0, 0.0, kA6, true, nullptr, nullptr, psplit);
-    gS_ = kS;
+    by_slices(all, [&](int w) { return reduced(w) ? pade_S_ : kS; }, [&](const std::vector<int>& l) {
+      product(st, r, l, kY, kY, -1.0, -1, 0.0, 0.0, kA2, true, nullptr, nullptr, psplit);
+      product(st, r, l, kA2, kA2, 1.0, -1, 0.0, 0.0, kA4, true, nullptr, nullptr, psplit);
+      product(st, r, l, kA4, kA2, 1.0, -1, 0.0, 0.0, kA6, true, nullptr, nullptr, psplit);
+    });
     const int arenas[3] = {kY, kA4, kA6};
     r.ops.push_back([=]() {
       const BWalk* wk = (const BWalk*)d_walks_.p;
@@ -1763,8 +1841,11 @@ class BatchPipeline {
       }
     });
     r.launches += 6;
-    estimate(st, r, all, kA4, kA4, 3);
-    estimate(st, r, all, kA4, kA6, 4);
+    est_recorded_ = needs_estimates();
+    if (est_recorded_) {
+      estimate(st, r, all, kA4, kA4, 3);
+      estimate(st, r, all, kA4, kA6, 4);
+    }
     lan_recorded_ = needs_lanczos();
     if (lan_recorded_) lanczos(st, r, all);
   }
@@ -2052,6 +2133,27 @@ class BatchPipeline {
     });
   }
 
+  // Two combinations of up to five arenas in one pass (kb_combo2); coef per walk as there.
+  void combo2(Staging& st, Rec& r, const std::vector<int>& list, int d1, int d2, const int m_arena[5],
+              const std::vector<std::array<double, 12>>& coef) {
+    if (list.empty()) return;
+    std::vector<double> c(12 * count(), 0.0);
+    for (int w : list)
+      for (int k = 0; k < 12; ++k) c[12 * w + k] = coef[w][k];
+    const std::vector<RChunk> ch = row_chunks(list, false);
+    const size_t o_ch = st.put(ch), o_c = st.put(c);
+    Planes5 M{};
+    for (int k = 0; k < 5; ++k) M.m[k] = m_arena[k] >= 0 ? A(m_arena[k]) : nullptr;
+    double* D1 = A(d1);
+    double* D2 = A(d2);
+    const unsigned nch = (unsigned)ch.size();
+    r.launches += 1;
+    r.ops.push_back([=]() {
+      kb_combo2<<<nch, 256, 0, stream_>>>(D1, D2, M, dev<RChunk>(o_ch), (const BWalk*)d_walks_.p, dev<double>(o_c));
+      FX_LAUNCH_CHECK();
+    });
+  }
+
   void transpose(Staging& st, Rec& r, const std::vector<int>& list, int in, int out) {
     if (list.empty()) return;
     const size_t o_l = st.put(list);
@@ -2118,13 +2220,15 @@ class BatchPipeline {
     std::vector<std::array<double, 5>> cf(W), cg(W);
     std::vector<double> al(W, 1.0), ga(W, 0.0);
     auto cs = [&](int w, int p) { return std::ldexp(1.0, -p * sel_s_[w]); };
-    // the Pade and solve products: 5 slices, or the mixed form's count; the mixed form also takes
-    // the (dominant) diagonals of the Pade products' operands out of their slices
-    gS_ = form_ == 1 ? pade_S_ : kS;
+    // the Pade and solve products: 5 slices, or the mixed form's count (pade_slices_of); the
+    // (dominant) diagonals of the Pade products' operands are taken out of their slices
     const bool psplit = form_ == 1 || (split_ & 4);
+    const auto ps = [&](int w) { return pade_slices_of(w); };
     // m = 9: A8 = A4 A4 -> T2
     tag_ = kTagPade;
-    product(st, r, m9, kA4, kA4, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, psplit);
+    by_slices(m9, ps, [&](const std::vector<int>& l) {
+      product(st, r, l, kA4, kA4, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, psplit);
+    });
     // m = 13: T1 = b13 A6 + b11 A4 + b9 A2 (scaled), T2 = A6 T1 (scaled)
     for (int w : m13) {
       const auto b = pade_coeffs(13);
@@ -2133,7 +2237,9 @@ class BatchPipeline {
     }
     const int m_642[4] = {kA6, kA4, kA2, -1};
     combo(st, r, m13, kT1, m_642, cf);
-    product(st, r, m13, kA6, kT1, 1.0, -1, 0.0, 0.0, kT2, true, &al, nullptr, psplit);
+    by_slices(m13, ps, [&](const std::vector<int>& l) {
+      product(st, r, l, kA6, kT1, 1.0, -1, 0.0, 0.0, kT2, true, &al, nullptr, psplit);
+    });
     // odd part: T1 = [T2] + b7 A6 + b5 A4 + b3 A2 + b1 I  (T2 = W1 for m = 13, A8 for m = 9)
     const int m_t2642[4] = {kT2, kA6, kA4, kA2};
     for (int w = 0; w < W; ++w) {
@@ -2150,7 +2256,9 @@ class BatchPipeline {
     }
     combo(st, r, all, kT1, m_t2642, cf);
     // U = i W with W = c Yim T1
-    product(st, r, all, kY, kT1, 1.0, -1, 0.0, 0.0, kW, true, &al, nullptr, psplit);
+    by_slices(all, ps, [&](const std::vector<int>& l) {
+      product(st, r, l, kY, kT1, 1.0, -1, 0.0, 0.0, kW, true, &al, nullptr, psplit);
+    });
     // even part.  m = 13: T1 = b12 A6 + b10 A4 + b8 A2, T2 = b6 A6 + b4 A4 + b2 A2,
     // V = A6 T1 + T2 + b0 I.  m < 13: V = [b8 A8] + b6 A6 + b4 A4 + b2 A2 + b0 I.
     for (int w : m13) {
@@ -2171,14 +2279,18 @@ class BatchPipeline {
       else cf[w] = {0.0, 0.0, 0.0, b[2] * cs(w, 2), b[0]};
     }
     combo(st, r, mlt13, kV, m_t2642, cf);
-    product(st, r, m13, kA6, kT1, 1.0, kT2, 1.0, 0.0, kV, true, &al, &ga, psplit);
+    by_slices(m13, ps, [&](const std::vector<int>& l) {
+      product(st, r, l, kA6, kT1, 1.0, kT2, 1.0, 0.0, kV, true, &al, &ga, psplit);
+    });
 
     // ---- solve: G = V^2 + W^2 = L L^T, P2 = (V + iW)^2, R = G^-1 P2
     // V ~ b_0 I once scaled: these products and the complex ones below split the diagonals off
     tag_ = kTagSolve;
-    product(st, r, all, kV, kV, 1.0, -1, 0.0, 0.0, kT1, true, nullptr, nullptr, true);    // VV
-    product(st, r, all, kW, kW, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, true);    // WW
-    product(st, r, all, kV, kW, 1.0, -1, 0.0, 0.0, kA2, true, nullptr, nullptr, true);    // VW
+    by_slices(all, ps, [&](const std::vector<int>& l) {
+      product(st, r, l, kV, kV, 1.0, -1, 0.0, 0.0, kT1, true, nullptr, nullptr, true);    // VV
+      product(st, r, l, kW, kW, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, true);    // WW
+      product(st, r, l, kV, kW, 1.0, -1, 0.0, 0.0, kA2, true, nullptr, nullptr, true);    // VW
+    });
     const int m_12[4] = {kT1, kT2, -1, -1};
     const int m_a2[4] = {kA2, -1, -1, -1};
     for (int w = 0; w < W; ++w) cf[w] = {1.0, 1.0, 0.0, 0.0, 0.0};
@@ -2187,30 +2299,30 @@ class BatchPipeline {
     combo(st, r, all, kA6, m_12, cf);                             // P2 re -> A6
     for (int w = 0; w < W; ++w) cf[w] = {2.0, 0.0, 0.0, 0.0, 0.0};
     combo(st, r, all, kY, m_a2, cf);                              // P2 im -> Y
-    // the mixed form solves large walks by Newton-Schulz (their Cholesky would be a long chain
-    // of dependent block steps); small walks, whose few steps run grouped over the batch, and
-    // the plain form keep the Cholesky solve
+    // large walks solve by Newton-Schulz (their Cholesky would be a long chain of dependent
+    // block steps); smaller walks, whose few steps run grouped over the batch, keep the
+    // Cholesky solve
     std::vector<int> ns_list, ch_list;
     for (int w = 0; w < W; ++w) {
-      const bool ns = solve_mode_ == 2 || (solve_mode_ == 0 && form_ == 1 && walks_[w].np >= kNewtonMinNp);
+      const bool ns = solve_mode_ == 2 || (solve_mode_ == 0 && walks_[w].np >= kNewtonMinNp);
       (ns ? ns_list : ch_list).push_back(w);
     }
-    if (!ns_list.empty()) newton_solve(st, r, ns_list);            // R re -> A4, im -> A2
-    if (!ch_list.empty()) {
+    by_slices(ns_list, ps, [&](const std::vector<int>& l) { newton_solve(st, r, l); });   // R re -> A4, im -> A2
+    by_slices(ch_list, ps, [&](const std::vector<int>& l) {
       tag_ = kTagCholesky;
-      cholesky(st, r, kA4, ch_list);
-      transpose(st, r, ch_list, kA4, kT1);                        // L^T -> T1
+      cholesky(st, r, kA4, l);
+      transpose(st, r, l, kA4, kT1);                              // L^T -> T1
       tag_ = kTagInverse;
-      inverse(st, r, kT1, kT2, kW, kA2, ch_list);                 // X = L^-1 -> T2, X^T -> W (scratch A2)
+      inverse(st, r, kT1, kT2, kW, kA2, l);                       // X = L^-1 -> T2, X^T -> W (scratch A2)
       // Z = P2 X^T (re -> V, im -> T1); R^T = Z X (re -> A4, im -> A2)
       tag_ = kTagTriangular;
-      complex_by_real(st, r, ch_list, kA6, kY, kT2, kV, kT1, 1, true);    // P2 symmetric
-      complex_by_real(st, r, ch_list, kV, kT1, kW, kA4, kA2, 2, false);
-      symmetrize(st, r, ch_list, kA4);
-      symmetrize(st, r, ch_list, kA2);
-    }
+      complex_by_real(st, r, l, kA6, kY, kT2, kV, kT1, 1, true);    // P2 symmetric
+      complex_by_real(st, r, l, kV, kT1, kW, kA4, kA2, 2, false);
+      symmetrize(st, r, l, kA4);
+      symmetrize(st, r, l, kA2);
+    });
 
-    gS_ = kS;
+
     // ---- squarings in I + E form: E = R - I, E <- 2E + E^2
     for (int w = 0; w < W; ++w) cf[w] = {1.0, 0.0, 0.0, 0.0, -1.0};
     const int m_a4[4] = {kA4, -1, -1, -1};
@@ -2230,10 +2342,10 @@ class BatchPipeline {
       for (int w = 0; w < W; ++w)
         if (sel_s_[w] > k) act.push_back(w);
       if (drift_) drift(st, r, act, er, ei, std::vector<int>(W, std::min(k, kDriftMax - 1)));
-      if (form_ == 1 || (split_ & 8))
-        square3(st, r, act, er, ei, tr, ti, k);
-      else
-        square(st, r, act, er, ei, tr, ti);
+      std::vector<int> act3, act4;
+      for (int w : act) (use_square3(w) ? act3 : act4).push_back(w);
+      if (!act3.empty()) square3(st, r, act3, er, ei, tr, ti, k);
+      if (!act4.empty()) square(st, r, act4, er, ei, tr, ti);
       for (int w : act) {
         std::swap(er[w], tr[w]);
         std::swap(ei[w], ti[w]);
@@ -2484,11 +2596,34 @@ class BatchPipeline {
     }
   }
 
+  // Walk w takes the mixed form's reduced slice counts (powers, squarings, early Newton-Schulz
+  // steps; the Pade and solve products by pade_slices_of).
+  bool reduced(int w) const { return form_ == 1 && walks_[w].np >= kMixedMinNp; }
+  // Slice count of walk w's Pade and solve products.
+  int pade_slices_of(int w) const { return reduced(w) && sel_s_[w] <= kMixedMaxPadeS ? pade_S_ : kS; }
+  // Walk w squares as three split products (square3), else as the exact complex square.
+  bool use_square3(int w) const {
+    return walks_[w].np >= kSquare3MinNp || sel_s_[w] >= kSquare3MinS || (split_ & 8);
+  }
+  // Calls f(group) for the walks of list grouped by slices(w), with gS_ set to the group's count
+  // while f records; gS_ is 5 again afterwards.
+  template <typename Sl, typename F>
+  void by_slices(const std::vector<int>& list, Sl&& slices, F&& f) {
+    for (int S : {kS, 4, 3}) {
+      std::vector<int> g;
+      for (int w : list)
+        if (slices(w) == S) g.push_back(w);
+      if (g.empty()) continue;
+      gS_ = S;
+      f(g);
+    }
+    gS_ = kS;
+  }
   // Model residual below which the Newton-Schulz steps run at the full slice count.
-  static constexpr double kNewtonLoRes = 1e-3;
+  static constexpr double kNewtonLoRes = 1e-4;
   // Slice count of squaring k (0-based) of walk w in the mixed form.
   int sq_slices(int w, int k) const {
-    if (form_ != 1) return kS;
+    if (!reduced(w)) return kS;
     const int rem = sel_s_[w] - k;   // 1 for the last squaring
     return rem <= sq_n3_ ? 3 : rem <= sq_n3_ + sq_n4_ ? 4 : kS;
   }
@@ -2532,12 +2667,11 @@ class BatchPipeline {
         product(st, r, l, im, im, 1.0, -1, 0.0, 0.0, kA6, true, nullptr, nullptr, true);   // t2
         product(st, r, l, kV, kV, 1.0, -1, 0.0, 0.0, kW, true, nullptr, nullptr, true);    // t3
         gS_ = kS;
-        const int m_re[4] = {re, kY, kA6, -1};
-        std::fill(cf.begin(), cf.end(), std::array<double, 5>{2.0, 1.0, -1.0, 0.0, 0.0});
-        combo(st, r, l, ore, m_re, cf);
-        const int m_im[4] = {im, kW, kY, kA6};
-        std::fill(cf.begin(), cf.end(), std::array<double, 5>{2.0, 1.0, -1.0, -1.0, 0.0});
-        combo(st, r, l, oim, m_im, cf);
+        // Re = 2 Er + t1 - t2, Im = 2 Ei + t3 - t1 - t2, in one pass over the five planes
+        const int m_out[5] = {re, im, kY, kA6, kW};
+        const std::vector<std::array<double, 12>> c2(
+            W, std::array<double, 12>{2.0, 0.0, 1.0, -1.0, 0.0, 0.0, 0.0, 2.0, -1.0, -1.0, 1.0, 0.0});
+        combo2(st, r, l, ore, oim, m_out, c2);
       }
     }
   }

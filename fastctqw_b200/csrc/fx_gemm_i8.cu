@@ -26,12 +26,12 @@
 //          later squarings.
 //
 // Kernel layout: persistent CTAs, K step 64 bytes (64B swizzle), one stage = S A-slice tiles +
-// S Bt-slice tiles, 3 stages; warp 0 TMA producer, warp 1 MMA issuer, warps 2-9 epilogue
-// (two warps per TMEM lane quarter, each draining half of the tile columns).
+// S Bt-slice tiles, 3 stages; warp 0 TMA producer, warp 1 MMA issuer (B slices in pairs, one
+// N = 2 x tile-width MMA for two adjacent levels), warps 2-17 epilogue (four warps per TMEM
+// lane quarter, each draining a quarter of the tile columns).
 // Symmetric-output mode computes only tiles touching the upper triangle and mirrors them.
 // All waits are bounded (see fx_tc_common.cuh).
 #include <algorithm>
-#include <cstdlib>
 #include <type_traits>
 
 #include "fx_kernels.cuh"
@@ -80,18 +80,7 @@ struct I8Params {
   const double* adg;   // diagonal split: removed diagonals by stacked row
   const double* bdg;
   int skip_tile;       // diagnostics: the producer skips the first K step's loads of this tile
-  int pairs;           // issue B slices in pairs (N = 2 kBN MMAs) where their levels are adjacent
 };
-// Pairing of the MMA issue (I8Params::pairs); FX_I8_PAIRS=0 in the environment selects the one-
-// slice-per-instruction issue, for comparisons of the two.
-int i8_pairs_default() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = std::getenv("FX_I8_PAIRS");
-    v = (e && e[0] == '0') ? 0 : 1;
-  }
-  return v;
-}
 
 __host__ __device__ constexpr uint32_t idesc_i8(int m, int n) {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
@@ -350,48 +339,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
             }
             tc_fence_after();
             const uint32_t st = smem_u32(smem + (size_t)s * kStage);
-            if (p.pairs) {
-              // Two B slices per instruction: slices pb and pb + 1 lie back to back in shared
-              // memory and their levels pa + pb and pa + pb + 1 in adjacent TMEM column blocks,
-              // so one MMA of N = 2 kBN covers both (one A read for twice the columns).  Row
-              // pa = 0 writes every level first, in pairs of equal first-write state.
+            // Two B slices per instruction: slices pb and pb + 1 lie back to back in shared
+            // memory and their levels pa + pb and pa + pb + 1 in adjacent TMEM column blocks, so
+            // one MMA of N = 2 kBN covers both (one A read for twice the columns; 6 instructions
+            // per 32 bytes of K instead of 10 at S = 4, 9 instead of 15 at S = 5).  Row pa = 0
+            // writes every level first, in pairs of equal first-write state.
 #pragma unroll
-              for (int pa = 0; pa < S; ++pa) {
+            for (int pa = 0; pa < S; ++pa) {
 #pragma unroll
-                for (int pb = 0; pb < S; pb += 2) {
-                  const int lvl = pa + pb;
-                  if (lvl > S - 1) continue;
-                  const bool two = lvl + 1 <= S - 1;
-                  const uint32_t a_addr = st + pa * Cf::kATile;
-                  const uint32_t b_addr = st + S * Cf::kATile + pb * Cf::kBTile;
-                  const uint32_t tmem_d = tmem_base + (uint32_t)(lvl * kBN);
+              for (int pb = 0; pb < S; pb += 2) {
+                const int lvl = pa + pb;  // 0..S-1 <=> level l = 2..S+1
+                if (lvl > S - 1) continue;
+                const bool two = lvl + 1 <= S - 1;
+                const uint32_t a_addr = st + pa * Cf::kATile;
+                const uint32_t b_addr = st + S * Cf::kATile + pb * Cf::kBTile;
+                const uint32_t tmem_d = tmem_base + (uint32_t)(lvl * kBN);
 #pragma unroll
-                  for (int k32 = 0; k32 < kBK / 32; ++k32) {
-                    umma_i8(tmem_d, desc_sw64(a_addr + k32 * 32), desc_sw64(b_addr + k32 * 32),
-                            two ? idesc2 : idesc, first[lvl] ? 0u : 1u);
-                    first[lvl] = false;
-                    if (two) first[lvl + 1] = false;
-                    issued_any = true;
-                  }
-                }
-              }
-            } else {
-#pragma unroll
-              for (int pa = 0; pa < S; ++pa) {
-#pragma unroll
-                for (int pb = 0; pb < S; ++pb) {
-                  const int lvl = pa + pb;  // 0..S-1 <=> level l = 2..S+1
-                  if (lvl > S - 1) continue;
-                  const uint32_t a_addr = st + pa * Cf::kATile;
-                  const uint32_t b_addr = st + S * Cf::kATile + pb * Cf::kBTile;
-                  const uint32_t tmem_d = tmem_base + (uint32_t)(lvl * kBN);
-#pragma unroll
-                  for (int k32 = 0; k32 < kBK / 32; ++k32) {
-                    umma_i8(tmem_d, desc_sw64(a_addr + k32 * 32), desc_sw64(b_addr + k32 * 32), idesc,
-                            first[lvl] ? 0u : 1u);
-                    first[lvl] = false;
-                    issued_any = true;
-                  }
+                for (int k32 = 0; k32 < kBK / 32; ++k32) {
+                  umma_i8(tmem_d, desc_sw64(a_addr + k32 * 32), desc_sw64(b_addr + k32 * 32), two ? idesc2 : idesc,
+                          first[lvl] ? 0u : 1u);
+                  first[lvl] = false;
+                  if (two) first[lvl + 1] = false;
+                  issued_any = true;
                 }
               }
             }
@@ -1071,7 +1040,6 @@ void launch_gemm_i8(int S, int64_t M, int64_t N, int64_t K, const I8Term* terms,
   p.err = err;
   p.timeout_ns = (unsigned long long)timeout_ms * 1000000ull;
   p.skip_tile = -1;
-  p.pairs = i8_pairs_default();
   if (S == 4)
     launch_i8_cfg<4, TO>(p, terms, nterms, M, N, K, lda, ldb, s);
   else if (S == 5)
@@ -1148,7 +1116,6 @@ void launch_gemm_i8_grouped(int S, const I8Term* terms, int nterms, int64_t pitc
   p.adg = adg;
   p.bdg = bdg;
   p.skip_tile = skip_tile;
-  p.pairs = i8_pairs_default();
   if (S == 3)
     launch_i8_grouped_cfg<3, TO>(p, terms, nterms, pitch, a_rows, b_rows, ntiles, s);
   else if (S == 4)

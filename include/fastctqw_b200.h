@@ -57,15 +57,21 @@ enum fx_status {
 /* Arithmetic forms for the matrix products (fx_set_option(FX_OPT_FORM, ...)). */
 enum fx_form {
   FX_FORM_PLAIN = 0,  /* int8 tensor-core products of 5 (FP64 masters) or 4 (FP32)
-                         Ozaki slices, exact int32 accumulation; default for complex64 */
+                         Ozaki slices, exact int32 accumulation; default for complex64.
+                         Walk generators: the powers, Pade and solve products split
+                         their operands' diagonals off (added in FP64); walks padded to
+                         4096 or more, or needing 12 or more squarings, square as three
+                         split products Re^2, Im^2, (Re+Im)^2, the others as the exact
+                         complex square                                               */
   FX_FORM_MIXED = 1,  /* reduced-precision products (complex64 / float32 handles).  Walk
-                         generators X = i*(real symmetric): int8 slices on FP64 masters
-                         with the diagonals split off and added in FP64, 4 slices for the
-                         powers, Pade and solve products (FX_OPT_PADE_SLICES), the solve
-                         by a Newton-Schulz inverse for n >= 4096, each squaring as
-                         three symmetric products Re^2, Im^2, (Re+Im)^2 at 4 slices (5
-                         for squarings before the last FX_OPT_SQ_N4, 3 for the last
-                         FX_OPT_SQ_N3).
+                         generators X = i*(real symmetric) padded to 4096 or more: int8
+                         slices on FP64 masters with the diagonals split off and added in
+                         FP64, 4 slices for the powers and (when s <= 10) the Pade and
+                         solve products (FX_OPT_PADE_SLICES), the solve by a
+                         Newton-Schulz inverse, each squaring as three symmetric products
+                         Re^2, Im^2, (Re+Im)^2 at 4 slices (5 for squarings before the
+                         last FX_OPT_SQ_N4, 3 for the last FX_OPT_SQ_N3).  Smaller walk
+                         generators take the plain form's schedule.
                          Other inputs: BF16 hi+lo split, 3 products (hi*hi, hi*lo,
                          lo*hi), FP32 accumulate, FP32 masters                        */
   FX_FORM_SIMT = 2,   /* CUDA-core FP32 FMA products, FP32 masters (checker)          */
@@ -111,14 +117,16 @@ enum fx_option {
                              (fx_unitarity_drift), at the cost of two extra products per
                              squaring                                                  */
   FX_OPT_PADE_SLICES = 15, /* mixed form, walk generators: int8 slices of the powers, Pade and
-                             solve products (4 default, 5 or 3)                        */
-  FX_OPT_NEWTON_SLICES = 16, /* mixed form, walk generators: int8 slices of the Newton-Schulz
-                             steps of the solve whose model residual stays above 1e-3 (3
-                             default, 4 or 5; the later steps take FX_OPT_PADE_SLICES) */
+                             solve products (4 default, 5 or 3; the Pade and solve
+                             products take 5 when the selection needs more than 10
+                             squarings)                                                */
+  FX_OPT_NEWTON_SLICES = 16, /* walk generators: int8 slices of the Newton-Schulz steps of
+                             the solve whose model residual stays above 1e-4 (3 default,
+                             4 or 5; the later steps take the Pade products' count: the
+                             iteration corrects the early steps' rounding)             */
   FX_OPT_SOLVE = 17       /* walk generators: solve of the Pade step R = G^-1 P^2 (G SPD):
-                             0 (default) Newton-Schulz for mixed-form walks padded to 4096
-                             or more, blocked Cholesky otherwise; 1 Cholesky; 2
-                             Newton-Schulz                                             */
+                             0 (default) Newton-Schulz for walks padded to 4096 or more,
+                             blocked Cholesky otherwise; 1 Cholesky; 2 Newton-Schulz  */
 };
 
 /* What the last run did. */
@@ -257,7 +265,7 @@ enum fx_batch_option {
   FX_BATCH_OPT_FORCE_M = 2,     /* diagnostics: force the Pade degree (-1 automatic)            */
   FX_BATCH_OPT_SELECTOR = 3,    /* as FX_OPT_SELECTOR                                           */
   FX_BATCH_OPT_ANALYZE_ONLY = 4, /* 1: stop after the selection (features and (m, s) only)      */
-  FX_BATCH_OPT_DIAG_SPLIT = 5,   /* mask, default 3: products that take their operands'          */
+  FX_BATCH_OPT_DIAG_SPLIT = 5,   /* mask, default 7: products that take their operands'          */
                                  /* diagonals out of the int8 slices and add those terms in     */
                                  /* FP64; 1 the real products (V^2, W^2, VW; all of the mixed   */
                                  /* form's), 2 P2 L^-T and Z L^-1, 4 the plain form's powers     */

@@ -1,13 +1,15 @@
 """The mixed (reduced-precision) form of the walk-generator pipeline (needs a GPU).
 
-The mixed form runs every squaring as two real products, Re = 2 Er + (Er + Ei)(Er - Ei) and
-Im = 2 Ei + 2 Er Ei (the planes of the iterate commute), and cuts the operands of the last
-squarings into fewer int8 slices (4, then 3): their errors are not amplified by later squarings.
-The Pade and solve products keep 5 slices.  Checked here against the FP64 eigendecomposition
-propagator, with the tolerances of the parity tests (complex64 U within 1e-5 relative, states at
-infidelity <= 1e-10); the per-squaring unitarity residual (FX_OPT_DRIFT) against one computed
-directly from the returned U; and the reduced-slice products themselves, by running every
-squaring at 4 or at 3 slices and comparing the error with the slices' resolution.
+For walks padded to 4096 or more the mixed form slices the powers, the Pade and solve products
+(when s <= 10) and the squarings into 4 int8 slices (5 for the squarings before the last 8),
+with every operand's diagonal split off and added in FP64; it squares E <- 2E + E^2 as three
+symmetric products Er^2, Ei^2, (Er + Ei)^2 and solves the Pade step by Newton-Schulz (early
+steps at 3 slices).  Smaller walks take the plain form's schedule.  Checked here against the
+FP64 eigendecomposition propagator, with the tolerances of the parity tests (complex64 U within
+1e-5 relative, states at infidelity <= 1e-10); the per-squaring unitarity residual
+(FX_OPT_DRIFT) against one computed directly from the returned U; and the reduced-slice
+squarings themselves, by running every squaring at 4 or at 3 slices and comparing the error
+with the slices' resolution.
 """
 import numpy as np
 import pytest
@@ -21,12 +23,16 @@ INFID = 1e-10
 
 
 def _dense(n, t=4.5, seed=11):
+    """Dense G(n, 0.5) Laplacian walk generator and its FP64 propagator (torch eigh on the
+    device: numpy's takes too long at n = 4096)."""
+    import torch
     from fastctqw_b200 import graphs
     A = graphs.erdos_renyi(n, 0.5, seed=seed, dtype=np.float32)
     L = np.diag(A.sum(axis=1)) - A
     X = np.asarray(-1j * (-1.0 * L) * t, dtype=np.complex64)
-    lam, V = np.linalg.eigh(X.imag.astype(np.float64))
-    return X, (V * np.exp(1j * lam)) @ V.T
+    lam, V = torch.linalg.eigh(torch.from_numpy(X.imag.astype(np.float64)).to("cuda"))
+    Vc = V.to(torch.complex128)
+    return X, ((Vc * torch.exp(1j * lam)) @ Vc.T).cpu().numpy()
 
 
 def _walk(X, form, **kw):
@@ -48,8 +54,9 @@ def _walk(X, form, **kw):
     return out
 
 
-@pytest.mark.parametrize("n", [1024, 2048])
+@pytest.mark.parametrize("n", [1024, 2048, 4096])
 def test_mixed_form_meets_the_accuracy_bar(n):
+    """Below 4096 the mixed form runs the plain schedule, from 4096 its reduced slices."""
     from fastctqw_b200 import graphs
     X, Uref = _dense(n)
     U, psi, st, _ = _walk(X, "mixed")
@@ -64,7 +71,7 @@ def test_mixed_form_meets_the_accuracy_bar(n):
 def test_drift_curve_matches_the_returned_propagator():
     """The residual after the last squaring equals ||U^H U - I||_F / sqrt(n) of the returned U up
     to its complex64 rounding; one value per squaring plus the Pade result."""
-    n = 1024
+    n = 4096
     X, _ = _dense(n)
     for form in ("plain", "mixed"):
         U, _, st, drift = _walk(X, form, drift=True)
@@ -80,7 +87,7 @@ def test_drift_curve_matches_the_returned_propagator():
 def test_reduced_slice_squarings_have_the_slices_resolution(slices):
     """Every squaring at 4 (or 3) slices: the products are right (not garbage) and their error is
     of the size the slices resolve, far above the 5-slice error."""
-    n = 1024
+    n = 4096
     X, Uref = _dense(n, t=2.0)
     U5, _, st, _ = _walk(X, "mixed", sq_n4=0, sq_n3=0)
     kw = {"sq_n4": 64, "sq_n3": 0} if slices == 4 else {"sq_n4": 0, "sq_n3": 64}
@@ -89,6 +96,8 @@ def test_reduced_slice_squarings_have_the_slices_resolution(slices):
     assert e5 <= C64_REL
     bound = {4: 1e-5, 3: 1e-2}[slices]
     assert er <= bound, (slices, er, st["s"])
+    # the reduced slices did run: their error is not the 5-slice error
+    assert er > e5, (slices, er, e5)
 
 
 def test_mixed_batch_matches_plain_batch():

@@ -112,7 +112,7 @@ def test_trained_selector_gains_over_plain():
     ns = [X.shape[0] for X in Xs]
     bp = WalkBatch(ns)
     plain = bp.run(Xs, psi0)
-    _, s_plain = bp.selection()
+    m_plain, s_plain = bp.selection()
     be = WalkBatch(ns, selector="estimated")
     be.run(Xs, psi0)
     m_est, s_est = be.selection()
@@ -125,7 +125,10 @@ def test_trained_selector_gains_over_plain():
     assert s_l.sum() < s_plain.sum(), (s_l.sum(), s_plain.sum())
     for k in range(len(Xs)):
         assert _inf(learned[k], refs[k]) <= 1e-10, (k, _inf(learned[k], refs[k]))
-        if d["outcome"][k] <= 0:
+        # a walk left on its fallback choice with the plain run's (m, s) computes the same
+        # (the fallback of these selections comes from norm bounds, not the 1-norm estimates,
+        # so it can take a squaring more than the plain selection)
+        if d["outcome"][k] <= 0 and (m_l[k], s_l[k]) == (m_plain[k], s_plain[k]):
             assert np.array_equal(learned[k], plain[k])
 
 
