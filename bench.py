@@ -650,6 +650,7 @@ def main():
     torch.cuda.synchronize()
     pst = eng.stats()
     stages = {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in eng.product_profile().items()}
+    timeline = {k: round(v, 3) for k, v in eng.timeline().items()}
     eng.configure(profile=False)
     pk, pk_kind = peaks()
     from fastctqw_b200 import _native
@@ -676,6 +677,7 @@ def main():
         "bf16_peak_measured_here": round(bf["tops"], 1),
         "bf16_peak_measured_peaks_json": pk.get("bf16_tflops"), "peaks_json": pk_kind,
         "stages": stages,
+        "walk_timeline_ms": timeline,
     }
 
     # ---- the plain form (5-slice products, exact complex squarings) with the plain (Al-Mohy &

@@ -320,6 +320,7 @@ class Engine:
 
     PRODUCT_STAGES = ("powers", "pade", "solve", "cholesky", "inverse", "triangular", "squarings",
                       "diagnostics", "newton")
+    TIMELINE = ("phase1", "host_gap", "phase2", "checks")
 
     def product_profile(self) -> dict:
         """Per-stage product time of the last profiled walk-generator run (configure(profile=True)):
@@ -333,11 +334,21 @@ class Engine:
         check(lib().fx_product_profile(self._h, tags, ms, ops, n, ctypes.byref(cnt)), self._h)
         out: dict = {}
         for i in range(n):
+            if tags[i] >= len(self.PRODUCT_STAGES):
+                continue   # timeline records: timeline()
             d = out.setdefault(self.PRODUCT_STAGES[tags[i]], {"launches": 0, "ms": 0.0, "ops": 0.0})
             d["launches"] += 1
             d["ms"] += ms[i]
             d["ops"] += ops[i]
+        self._timeline = {self.TIMELINE[tags[i] - len(self.PRODUCT_STAGES)]: ms[i]
+                          for i in range(n) if tags[i] >= len(self.PRODUCT_STAGES)}
         return out
+
+    def timeline(self) -> dict:
+        """Device time of the last profiled walk-generator run by part (ms): phase 1, the gap
+        between the phases, phase 2, the checks (read with product_profile)."""
+        self.product_profile()
+        return dict(self._timeline)
 
     # -- host buffers
     def _host_in(self, A) -> np.ndarray:

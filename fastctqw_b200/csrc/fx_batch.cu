@@ -1022,6 +1022,8 @@ class BatchPipeline {
   ~BatchPipeline() {
     if (graph1_) cudaGraphExecDestroy(graph1_);
     if (graph2_) cudaGraphExecDestroy(graph2_);
+    for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
+    for (cudaEvent_t e : phase_ev_) cudaEventDestroy(e);
   }
 
   int count() const { return (int)walks_.size(); }
@@ -1179,6 +1181,7 @@ class BatchPipeline {
     gemm_launches_ = 0;
     prod_index_ = 0;
     prof_reset();
+    phase_mark(0);
     std::vector<const void*> tab(4 * W, nullptr);
     for (int w = 0; w < W; ++w) {
       tab[w] = dX[w];
@@ -1192,6 +1195,7 @@ class BatchPipeline {
 
     // ---- phase 1: statistics and shifts, powers, exact norms, estimates (one host round trip)
     run_recorded(desc1_, st1_, r1_, graph1_, use_graph_ && !profile_ && inject_ < 0);
+    phase_mark(1);
     std::vector<double>& h_wo = walkrec_;
     h_wo.assign(kWO * W, 0.0);
     std::vector<int> h_flags(W);
@@ -1343,7 +1347,9 @@ class BatchPipeline {
       autotune_ = false;
     }
     FX_CUDA(cudaMemsetAsync(walk_err(), 0, sizeof(int) * W, s));
+    phase_mark(2);
     run_phase2(tab);
+    phase_mark(3);
     std::vector<int> werr(W), own(W, 0);
     int herr = 0;
     FX_CUDA(cudaMemcpyAsync(werr.data(), walk_err(), sizeof(int) * W, cudaMemcpyDeviceToHost, s));
@@ -1386,9 +1392,17 @@ class BatchPipeline {
         sub.selection((int)i, &sel_m_[w], &sel_s_[w]);
       }
     }
+    phase_mark(4);
     FX_CUDA(cudaStreamSynchronize(s));
     check_err();
     prof_collect();
+    if (profile_) {   // the run's timeline (not part of the product totals)
+      for (int k = 0; k < 4; ++k) {
+        float t = 0;
+        FX_CUDA(cudaEventElapsedTime(&t, phase_ev_[k], phase_ev_[k + 1]));
+        prod_list_.push_back(ProdRecord{kTagPhase1 + k, (double)t, 0.0, 0.0});
+      }
+    }
     if (drift_ && drift_buf_.p) {
       drift_host_.assign((size_t)W * kDriftMax, 0.0);
       FX_CUDA(cudaMemcpy(drift_host_.data(), drift_buf_.p, sizeof(double) * drift_host_.size(), cudaMemcpyDeviceToHost));
@@ -1405,8 +1419,8 @@ class BatchPipeline {
       key.insert(key.end(), {(double)sel_m_[w], (double)sel_s_[w], (double)rank1_[w], mu_[w].real(),
                              mu_[w].imag(), nu_[w].real(), nu_[w].imag(), tab[W + w] ? 1.0 : 0.0,
                              tab[2 * W + w] ? 1.0 : 0.0, tab[3 * W + w] ? 1.0 : 0.0});
-      // the mixed form's Newton-Schulz solve takes its step count and scaling from these
-      if (form_ == 1) key.insert(key.end(), {rho_up_[w], rho_lan_[w]});
+      // the Newton-Schulz solve takes its step count and scaling from these
+      key.insert(key.end(), {rho_up_[w], rho_lan_[w]});
     }
     if (key != key2_ || profile_) {
       st2_ = Staging();
@@ -1582,6 +1596,7 @@ class BatchPipeline {
   std::vector<int> plain_m_, plain_s_, cert_m_, cert_s_, outcome_;
   std::vector<double> features_;
   int selector_ = 0;
+  std::vector<cudaEvent_t> phase_ev_;   // profile mode: the run's timeline events
   bool lan_recorded_ = false;   // phase 1 as recorded runs the Lanczos estimate
   bool est_recorded_ = true;    // phase 1 as recorded runs the 1-norm estimates of A^8, A^10
   bool analyze_only_ = false;
@@ -1716,6 +1731,17 @@ class BatchPipeline {
     return out;
   }
 
+  // Profile mode: event k of the run's timeline (0 start, 1 after phase 1, 2 before phase 2,
+  // 3 after phase 2, 4 end).
+  void phase_mark(int k) {
+    if (!profile_) return;
+    while ((int)phase_ev_.size() < 5) {
+      cudaEvent_t e;
+      FX_CUDA(cudaEventCreate(&e));
+      phase_ev_.push_back(e);
+    }
+    FX_CUDA(cudaEventRecord(phase_ev_[k], stream_));
+  }
   void prof_reset() {
     ev_work_.clear();
     prod_list_.clear();

@@ -232,7 +232,13 @@ enum ProdTag {
   kTagTriangular = 5,  // Z = P2 L^-T, R^T = Z L^-1
   kTagSquare = 6,      // squarings
   kTagDrift = 7,       // diagnostic unitarity products
-  kTagNewton = 8       // Newton-Schulz inverse of the solve (mixed form)
+  kTagNewton = 8,      // Newton-Schulz inverse of the solve
+  // whole-run timeline records (profile mode, no ops): phase 1, the host gap between the two
+  // phases (read-back, selection, recording or graph launch), phase 2, the checks after it
+  kTagPhase1 = 9,
+  kTagHostGap = 10,
+  kTagPhase2 = 11,
+  kTagChecks = 12
 };
 struct ProdRecord {
   int tag;

@@ -171,9 +171,11 @@ const char* fx_last_error(fx_handle h);
 /* Per product launch of the last run made with FX_OPT_PROFILE = 1 through the walk-generator
  * pipeline: its stage (0 powers, 1 Pade numerator / denominator, 2 the solve's V^2, W^2, VW,
  * 3 Cholesky, 4 triangular inverse, 5 triangular products, 6 squarings, 7 diagnostic unitarity
- * products, 8 Newton-Schulz inverse of the mixed form's solve), its CUDA-event duration in ms and the int8 tensor ops it issued.  Writes
- * min(cap, launches) records and the launch count to *count (0 when no such run was profiled).
- * Diagnostics; no counterpart in the reference. */
+ * products, 8 Newton-Schulz inverse of the solve), its CUDA-event duration in ms and the int8
+ * tensor ops it issued; then four timeline records of the whole run (ops 0): 9 phase 1, 10 the
+ * gap between the phases (read-back, selection, graph launch), 11 phase 2, 12 the checks after
+ * it.  Writes min(cap, records) records and the record count to *count (0 when no such run was
+ * profiled).  Diagnostics; no counterpart in the reference. */
 int fx_product_profile(fx_handle h, int32_t* tags, double* ms, double* ops, int32_t cap, int32_t* count);
 
 /* The unitarity residuals of the last run made with FX_OPT_DRIFT = 1: out[k] =
