@@ -818,95 +818,64 @@ __global__ void __launch_bounds__(256) k_row_exp_grouped(const GSlab* slabs, int
     if (dcol >= 0) out.dg[row] = (double)re[dcol];
   }
 }
-// Digit pass: persistent CTAs over units of (row, 1024-column chunk), 4 columns per thread;
-// the next unit's loads are issued before the current unit's digits are cut, so that every
-// thread keeps a unit's loads in flight while it computes.
-constexpr int kStreamChunk = 1024;   // columns per unit (256 threads x 4)
-constexpr int kStreamCtasPerSm = 3;   // resident at 80 registers a thread
-template <typename TI>
-struct StreamUnit {
-  const TI* re;
-  const TI* im;
-  int64_t row, k0, K, dcol;
-  bool ok;
-};
-template <typename TI>
-__device__ __forceinline__ StreamUnit<TI> stream_unit(const GSlab* slabs, int nslabs, int64_t u, int64_t cpr,
-                                                      const I8Slices& out) {
-  StreamUnit<TI> x{};
-  x.row = u / cpr;
-  const GSlab sb = slabs[find_slab(slabs, nslabs, x.row)];
-  const int64_t local = x.row - sb.row0;
-  x.K = sb.K;
-  x.k0 = (u - x.row * cpr) * kStreamChunk + 4 * (int64_t)threadIdx.x;
-  x.ok = local >= 0 && local < sb.rows && x.k0 < x.K;
-  if (!x.ok) return x;
-  x.re = (const TI*)sb.re + local * sb.ld;
-  x.im = sb.im ? (const TI*)sb.im + local * sb.ld : nullptr;
-  x.dcol = (sb.diag0 != kNoDiag && out.dg && !x.im) ? local + sb.diag0 : -1;
-  if (x.dcol >= x.K) x.dcol = -1;
-  return x;
-}
-template <typename TI>
-__device__ __forceinline__ void stream_load(const StreamUnit<TI>& x, double v[2][4]) {
-  if (!x.ok) return;
-  const bool vec = ((reinterpret_cast<uintptr_t>(x.re) | reinterpret_cast<uintptr_t>(x.im)) & 15) == 0;
-  load4<TI>(x.re, x.k0, x.K, vec, v[0]);
-  if (x.im) load4<TI>(x.im, x.k0, x.K, vec, v[1]);
-}
+constexpr int kStreamChunk = 2048;   // columns per block of the digit pass (256 threads x 2 x 4)
 template <typename TI, bool NEG>
-__global__ void __launch_bounds__(256, kStreamCtasPerSm) k_slice_stream_grouped(const GSlab* slabs, int nslabs, int64_t units,
-                                                              int64_t cpr, int S, I8Slices out) {
-  int64_t u = blockIdx.x;
-  if (u >= units) return;
-  StreamUnit<TI> cu = stream_unit<TI>(slabs, nslabs, u, cpr, out);
-  double cur[2][4] = {}, nxt[2][4] = {};
-  stream_load<TI>(cu, cur);
+__global__ void __launch_bounds__(256) k_slice_stream_grouped(const GSlab* slabs, int nslabs, int S, I8Slices out) {
+  const int64_t row = blockIdx.x;
+  const GSlab sb = slabs[find_slab(slabs, nslabs, row)];
+  const int64_t local = row - sb.row0;
+  if (local < 0 || local >= sb.rows) return;
+  const int64_t K = sb.K;
+  const int64_t base = (int64_t)blockIdx.y * kStreamChunk + 4 * (int64_t)threadIdx.x;
+  if (base >= K) return;
+  const TI* re = (const TI*)sb.re + local * sb.ld;
+  const TI* im = sb.im ? (const TI*)sb.im + local * sb.ld : nullptr;
+  int64_t dcol = (sb.diag0 != kNoDiag && out.dg && !im) ? local + sb.diag0 : -1;
+  if (dcol >= K) dcol = -1;
+  const bool vec = ((reinterpret_cast<uintptr_t>(re) | reinterpret_cast<uintptr_t>(im)) & 15) == 0;
+  // both groups' loads before any digit is cut: four 16-byte loads in flight per thread
+  double x[2][2][4] = {};
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    const int64_t k0 = base + g * (kStreamChunk / 2);
+    if (k0 < K) {
+      load4<TI>(re, k0, K, vec, x[g][0]);
+      if (im) load4<TI>(im, k0, K, vec, x[g][1]);
+    }
+  }
+  const int e = out.exp[row];
+  bool one;
+  const double sc = scale_for(S, e, one);
   const int64_t ld = out.ld;
-  for (; u < units; u += gridDim.x) {
-    const int64_t un = u + gridDim.x;
-    StreamUnit<TI> nu{};
-    if (un < units) {
-      nu = stream_unit<TI>(slabs, nslabs, un, cpr, out);
-      stream_load<TI>(nu, nxt);
-    }
-    if (cu.ok) {
-      const int e = out.exp[cu.row];
-      bool one;
-      const double sc = scale_for(S, e, one);
 #pragma unroll
-      for (int plane = 0; plane < 2; ++plane) {
-        if (plane == 1 && !cu.im) continue;
-        uint32_t pk[kMaxSlices] = {}, pn[kMaxSlices] = {};
+  for (int g = 0; g < 2; ++g) {
+    const int64_t k0 = base + g * (kStreamChunk / 2);
+    if (k0 >= K) continue;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          double v = cur[plane][j];
-          if (plane == 0 && cu.k0 + j == cu.dcol) v = 0.0;
-          const double xs = one ? v * sc : ldexp(ldexp(v, -e), 7 * S);
-          int d[kMaxSlices];
-          cut_digits(xs, S, d);
+    for (int plane = 0; plane < 2; ++plane) {
+      if (plane == 1 && !im) continue;
+      uint32_t pk[kMaxSlices] = {}, pn[kMaxSlices] = {};
 #pragma unroll
-          for (int q = 0; q < kMaxSlices; ++q)
-            if (q < S) {
-              pk[q] |= ((uint32_t)(uint8_t)(int8_t)d[q]) << (8 * j);
-              if (NEG && plane == 1) pn[q] |= ((uint32_t)(uint8_t)(int8_t)(-d[q])) << (8 * j);
-            }
-        }
+      for (int j = 0; j < 4; ++j) {
+        double v = x[g][plane][j];
+        if (plane == 0 && k0 + j == dcol) v = 0.0;
+        const double xs = one ? v * sc : ldexp(ldexp(v, -e), 7 * S);
+        int d[kMaxSlices];
+        cut_digits(xs, S, d);
 #pragma unroll
-        for (int q = 0; q < kMaxSlices; ++q) {
-          if (q >= S) continue;
-          int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
-          if (dst) *reinterpret_cast<uint32_t*>(dst + cu.row * ld + cu.k0) = pk[q];
-          if (NEG && plane == 1 && out.neg_im[q])
-            *reinterpret_cast<uint32_t*>(out.neg_im[q] + cu.row * ld + cu.k0) = pn[q];
-        }
+        for (int q = 0; q < kMaxSlices; ++q)
+          if (q < S) {
+            pk[q] |= ((uint32_t)(uint8_t)(int8_t)d[q]) << (8 * j);
+            if (NEG && plane == 1) pn[q] |= ((uint32_t)(uint8_t)(int8_t)(-d[q])) << (8 * j);
+          }
       }
-    }
-    cu = nu;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      cur[0][j] = nxt[0][j];
-      cur[1][j] = nxt[1][j];
+      for (int q = 0; q < kMaxSlices; ++q) {
+        if (q >= S) continue;
+        int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
+        if (dst) *reinterpret_cast<uint32_t*>(dst + row * ld + k0) = pk[q];
+        if (NEG && plane == 1 && out.neg_im[q]) *reinterpret_cast<uint32_t*>(out.neg_im[q] + row * ld + k0) = pn[q];
+      }
     }
   }
 }
@@ -989,14 +958,13 @@ void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t to
   if (kind == 1) {
     if (kmax <= 0) throw Error{FX_ERR_VALUE, "grouped slice: the streaming kernel needs the widest row"};
     const unsigned g1 = (unsigned)cdiv(total_rows, 8);
-    const int64_t cpr = cdiv(kmax, kStreamChunk), units = total_rows * cpr;
-    const unsigned g2 = (unsigned)std::min<int64_t>(units, (int64_t)sm_count() * kStreamCtasPerSm);
+    const dim3 g2((unsigned)total_rows, (unsigned)cdiv(kmax, kStreamChunk));
     k_row_exp_grouped<TI><<<g1, 256, 0, s>>>(slabs, nslabs, total_rows, out);
     FX_LAUNCH_CHECK();
     if (want_neg_im)
-      k_slice_stream_grouped<TI, true><<<g2, 256, 0, s>>>(slabs, nslabs, units, cpr, S, out);
+      k_slice_stream_grouped<TI, true><<<g2, 256, 0, s>>>(slabs, nslabs, S, out);
     else
-      k_slice_stream_grouped<TI, false><<<g2, 256, 0, s>>>(slabs, nslabs, units, cpr, S, out);
+      k_slice_stream_grouped<TI, false><<<g2, 256, 0, s>>>(slabs, nslabs, S, out);
     FX_LAUNCH_CHECK();
     return;
   }
