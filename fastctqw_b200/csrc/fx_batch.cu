@@ -2089,7 +2089,9 @@ class BatchPipeline {
     const int nsa = (int)a_sorted.size(), nsb = (int)b_sorted.size(), nt = (int)tiles.size();
     const double ops = tile_ops(tiles, 1, S);
     int64_t a_span = 0, b_span = 0;
-    const int64_t ka = widest(a_sorted), kb = widest(b_sorted);
+    const std::vector<int> pla = slice_plan(a_sorted), plb = slice_plan(b_sorted);
+    const size_t o_pla = st.put(pla), o_plb = st.put(plb);
+    const int bla = pla.back(), blb = plb.back();
     for (const GSlab& g : a_sorted) a_span = std::max<int64_t>(a_span, (int64_t)g.row0 + g.rows);
     for (const GSlab& g : b_sorted) b_span = std::max<int64_t>(b_span, (int64_t)g.row0 + g.rows);
     r.launches += same ? 2 : 3;
@@ -2106,11 +2108,13 @@ class BatchPipeline {
       outa.dg = split ? adiag() : nullptr;
       outb.dg = split ? bdiag() : nullptr;
       outa.ld = outb.ld = pitch_;
-      launch_slice_rows_grouped<double>(S, dev<GSlab>(o_sa), nsa, a_span, outa, false, stream_, ka);
+      launch_slice_rows_grouped<double>(S, dev<GSlab>(o_sa), nsa, a_span, outa, false, stream_,
+                                        SlicePlan{dev<int>(o_pla), bla});
       I8Term t{};
       for (int q = 0; q < S; ++q) t.a[q] = outa.re[q];
       if (!same) {
-        launch_slice_rows_grouped<double>(S, dev<GSlab>(o_sb), nsb, b_span, outb, false, stream_, kb);
+        launch_slice_rows_grouped<double>(S, dev<GSlab>(o_sb), nsb, b_span, outb, false, stream_,
+                                          SlicePlan{dev<int>(o_plb), blb});
         for (int q = 0; q < S; ++q) t.b[q] = outb.re[q];
       } else {
         for (int q = 0; q < S; ++q) t.b[q] = outa.re[q];
@@ -2124,11 +2128,6 @@ class BatchPipeline {
     });
   }
 
-  static int64_t widest(const std::vector<GSlab>& v) {
-    int64_t k = 0;
-    for (const GSlab& g : v) k = std::max<int64_t>(k, g.K);
-    return k;
-  }
   // Row chunks of the listed walks' n x n (use_n) or np x np blocks, about kChunkElems each.
   std::vector<RChunk> row_chunks(const std::vector<int>& list, bool use_n) const {
     std::vector<RChunk> ch;
@@ -2488,7 +2487,9 @@ class BatchPipeline {
       std::sort(sa.begin(), sa.end(), [](const GSlab& x, const GSlab& y) { return x.row0 < y.row0; });
       const size_t o_sa = st.put(sa), o_r = st.put(prr), o_i = st.put(pri), o_t = st.put(tiles);
       const int nsa = (int)sa.size(), nt = (int)tiles.size();
-      const int64_t kw = widest(sa);
+      const std::vector<int> pl = slice_plan(sa);
+      const size_t o_pl = st.put(pl);
+      const int bl = pl.back();
       const double ops = tile_ops(tiles, 2);
       r.launches += 3;
       r.gemms += 2;
@@ -2501,7 +2502,8 @@ class BatchPipeline {
         }
         out.exp = aexp();
         out.ld = pitch_;
-        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, rows_, out, true, stream_, kw);
+        launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, rows_, out, true, stream_,
+                                          SlicePlan{dev<int>(o_pl), bl});
         I8Term t[2];
         // real: Re Re + Im (-Im)
         for (int q = 0; q < kS; ++q) {
@@ -2738,7 +2740,9 @@ class BatchPipeline {
     const size_t o_sa = st.put(sa), o_p1 = st.put(p1), o_p2 = st.put(p2), o_t1 = st.put(t1), o_t2 = st.put(t2);
     const size_t o_ch = st.put(ch), o_er = st.put(erp), o_sl = st.put(slot);
     const int nsa = (int)sa.size(), n1 = (int)t1.size(), n2 = (int)t2.size();
-    const int64_t kw = widest(sa);
+    const std::vector<int> pl = slice_plan(sa);
+    const size_t o_pl = st.put(pl);
+    const int bl = pl.back();
     const unsigned nch = (unsigned)ch.size();
     const double ops1 = tile_ops(t1, 2), ops2 = tile_ops(t2, 1);
     r.launches += 4;
@@ -2751,7 +2755,8 @@ class BatchPipeline {
       }
       out.exp = aexp();
       out.ld = pitch_;
-      launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, rows_, out, false, stream_, kw);
+      launch_slice_rows_grouped<double>(kS, dev<GSlab>(o_sa), nsa, rows_, out, false, stream_,
+                                        SlicePlan{dev<int>(o_pl), bl});
       I8Term t[2];
       for (int q = 0; q < kS; ++q) {
         t[0].a[q] = t[0].b[q] = out.re[q];

@@ -107,8 +107,12 @@ int fx_slice_rows_f64(int kind, int S, const double* re, const double* im, int64
         (neg && !im))
       throw fx::Error{FX_ERR_VALUE, "fx_slice_rows_f64: invalid arguments"};
     fx::GSlab h{re, im, ld, (int)rows, (int)K, 0, split_diag ? 0 : fx::kNoDiag};
-    FX_CUDA(cudaMalloc(&d_slab, sizeof(fx::GSlab)));
+    const std::vector<int> plan = fx::slice_plan(std::vector<fx::GSlab>{h});
+    // one allocation: the slab, then its block plan
+    FX_CUDA(cudaMalloc(&d_slab, sizeof(fx::GSlab) + sizeof(int) * plan.size()));
+    int* d_plan = reinterpret_cast<int*>(d_slab + 1);
     FX_CUDA(cudaMemcpyAsync(d_slab, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    FX_CUDA(cudaMemcpyAsync(d_plan, plan.data(), sizeof(int) * plan.size(), cudaMemcpyHostToDevice, s));
     fx::I8Slices o{};
     const size_t plane = (size_t)rows * ldo;
     for (int q = 0; q < S; ++q) {
@@ -119,7 +123,8 @@ int fx_slice_rows_f64(int kind, int S, const double* re, const double* im, int64
     o.exp = exps;
     o.ld = ldo;
     o.dg = split_diag ? dg : nullptr;
-    fx::launch_slice_rows_grouped<double>(S, d_slab, 1, rows, o, neg != 0, s, K, kind);
+    fx::launch_slice_rows_grouped<double>(S, d_slab, 1, rows, o, neg != 0, s, fx::SlicePlan{d_plan, plan.back()},
+                                          kind);
     FX_CUDA(cudaStreamSynchronize(s));
   } catch (const fx::Error& e) {
     g_dbg_err = e.msg;

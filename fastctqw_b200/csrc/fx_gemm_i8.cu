@@ -142,10 +142,6 @@ __device__ __forceinline__ void tile_of(const I8Params& p, int tile, int& mb, in
   nb = rr / gsize;
 }
 
-// 2^k as a double for |k| < 1000 (exact), else 0 (the caller then falls back to ldexp).
-__device__ __forceinline__ double pow2_or_zero(int k) {
-  return (k > -1000 && k < 1000) ? __longlong_as_double((long long)(k + 1023) << 52) : 0.0;
-}
 // 2^k as a normal double for -1022 <= k <= 1023, +inf above, 0 below.
 __device__ __forceinline__ double pow2_normal(int k) {
   return k > 1023 ? __longlong_as_double(0x7ff0000000000000ll)
@@ -613,6 +609,41 @@ __device__ __forceinline__ void load4(const TI* src, int64_t k0, int64_t K, bool
   }
 }
 
+// Digits of four values xs[0..3] (|xs| < 2^(7S), FP64), packed one byte each (two's complement)
+// into w[q] for digit q: v = rint(xs) (round half to even), then from the top
+// d_q = round-half-even(r / 2^k), k = 7 (S - 1 - q), r -= d_q 2^k, the last digit the remainder.
+// Rounding to an integer by adding M = 1.5 * 2^52 (the sum lies in [2^52, 2^53), where the
+// spacing of doubles is 1, so the addition rounds to the nearest integer, ties to even, and the
+// low 32 bits of the sum hold that integer; the classic technique of, e.g., Muller et al.,
+// Handbook of Floating-Point Arithmetic): every step is exact FP64 arithmetic on the FMA pipe,
+// r / 2^k and t 2^k being powers-of-two scalings of integers below 2^36.  Integer shift forms
+// of the same rule kept the integer ALU busy for three quarters of the slicer's time.
+__device__ __forceinline__ void cut_digits4(const double xs[4], int S, uint32_t w[kMaxSlices]) {
+  constexpr double M = 0x1.8p52;
+  double r[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) r[j] = (xs[j] + M) - M;
+#pragma unroll
+  for (int q = 0; q < kMaxSlices; ++q) {
+    if (q >= S) continue;
+    uint32_t d[4];
+    if (q < S - 1) {
+      const int k = 7 * (S - 1 - q);
+      const double down = pow2_normal(-k), up = pow2_normal(k);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double tm = fma(r[j], down, M);
+        d[j] = (uint32_t)__double2loint(tm);
+        r[j] = fma(-(tm - M), up, r[j]);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) d[j] = (uint32_t)__double2loint(r[j] + M);
+    }
+    w[q] = __byte_perm(__byte_perm(d[0], d[1], 0x0040), __byte_perm(d[2], d[3], 0x0040), 0x5410);
+  }
+}
+
 // rre / rim: the source row (rim may be null); orow: offset of the row in the slice planes;
 // NEG: also write the slices of -im (out.neg_im).
 template <typename TI, bool NEG>
@@ -665,37 +696,21 @@ __device__ __forceinline__ void slice_row(const TI* rre, const TI* rim, int64_t 
       const TI* src = plane == 0 ? rre : rim;
       if (!src) continue;
       double* x = cur[plane];
-      uint32_t packed[kMaxSlices] = {0, 0, 0, 0, 0}, packed_neg[kMaxSlices] = {0, 0, 0, 0, 0};
+      uint32_t packed[kMaxSlices];
       const bool neg = NEG && plane == 1;
+      double xs[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         if (plane == 0 && k0 + j == dcol) x[j] = 0.0;
-        const double xs = one_factor ? x[j] * scale : ldexp(ldexp(x[j], -e), 7 * S);
-        // v and every remainder are integers below 2^35 in magnitude, so this runs exactly in
-        // FP64: t = rint(r 2^-k) (round half to even), r -= t 2^k
-        double r = rint(xs);
-#pragma unroll
-        for (int q = 0; q < kMaxSlices; ++q) {
-          if (q >= S) continue;
-          int d;
-          if (q < S - 1) {
-            const int k = 7 * (S - 1 - q);
-            const double t = rint(r * pow2_or_zero(-k));
-            r = fma(-t, pow2_or_zero(k), r);
-            d = (int)t;
-          } else {
-            d = (int)r;
-          }
-          packed[q] |= ((uint32_t)(uint8_t)(int8_t)d) << (8 * j);
-          if (neg) packed_neg[q] |= ((uint32_t)(uint8_t)(int8_t)(-d)) << (8 * j);
-        }
+        xs[j] = one_factor ? x[j] * scale : ldexp(ldexp(x[j], -e), 7 * S);
       }
+      cut_digits4(xs, S, packed);
 #pragma unroll
       for (int q = 0; q < kMaxSlices; ++q) {
         if (q >= S) continue;
         int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
         if (dst) *reinterpret_cast<uint32_t*>(dst + orow * out.ld + k0) = packed[q];
-        if (neg && out.neg_im[q]) *reinterpret_cast<uint32_t*>(out.neg_im[q] + orow * out.ld + k0) = packed_neg[q];
+        if (neg && out.neg_im[q]) *reinterpret_cast<uint32_t*>(out.neg_im[q] + orow * out.ld + k0) = __vneg4(packed[q]);
       }
     }
 #pragma unroll
@@ -736,22 +751,7 @@ __global__ void __launch_bounds__(256, 2) k_slice_rows_grouped(const GSlab* slab
   slice_row<TI, NEG>(re, im, sb.K, S, out, row, lane, (dcol >= 0 && dcol < sb.K) ? dcol : -1);
 }
 
-// ---- digit helpers of the shared-memory slicing kernel below (the digits of slice_row).
-__device__ __forceinline__ void cut_digits(double xs, int S, int d[kMaxSlices]) {
-  double r = rint(xs);
-#pragma unroll
-  for (int q = 0; q < kMaxSlices; ++q) {
-    if (q >= S) continue;
-    if (q < S - 1) {
-      const int k = 7 * (S - 1 - q);
-      const double t = rint(r * pow2_or_zero(-k));
-      r = fma(-t, pow2_or_zero(k), r);
-      d[q] = (int)t;
-    } else {
-      d[q] = (int)r;
-    }
-  }
-}
+// ---- helpers of the streaming slicing kernels below.
 __device__ __forceinline__ int row_exponent(double mx) {
   int e = 0;
   if (mx > 0.0) {
@@ -818,71 +818,76 @@ __global__ void __launch_bounds__(256) k_row_exp_grouped(const GSlab* slabs, int
     if (dcol >= 0) out.dg[row] = (double)re[dcol];
   }
 }
-constexpr int kStreamChunk = 2048;   // columns per block of the digit pass (256 threads x 2 x 4)
+// Digit pass over a block plan: block b serves slab i with plan[i] <= b < plan[i + 1] and covers
+// kPlanGroups 4-column groups of that slab's rows x K elements in row-major order, so that
+// narrow rows leave no thread idle and no block searches rows; two groups' loads are in flight
+// per thread before their digits are cut.
 template <typename TI, bool NEG>
-__global__ void __launch_bounds__(256) k_slice_stream_grouped(const GSlab* slabs, int nslabs, int S, I8Slices out) {
-  const int64_t row = blockIdx.x;
-  const GSlab sb = slabs[find_slab(slabs, nslabs, row)];
-  const int64_t local = row - sb.row0;
-  if (local < 0 || local >= sb.rows) return;
-  const int64_t K = sb.K;
-  const int64_t base = (int64_t)blockIdx.y * kStreamChunk + 4 * (int64_t)threadIdx.x;
-  if (base >= K) return;
-  const TI* re = (const TI*)sb.re + local * sb.ld;
-  const TI* im = sb.im ? (const TI*)sb.im + local * sb.ld : nullptr;
-  int64_t dcol = (sb.diag0 != kNoDiag && out.dg && !im) ? local + sb.diag0 : -1;
-  if (dcol >= K) dcol = -1;
-  const bool vec = ((reinterpret_cast<uintptr_t>(re) | reinterpret_cast<uintptr_t>(im)) & 15) == 0;
-  // both groups' loads before any digit is cut: four 16-byte loads in flight per thread
-  double x[2][2][4] = {};
-#pragma unroll
-  for (int g = 0; g < 2; ++g) {
-    const int64_t k0 = base + g * (kStreamChunk / 2);
-    if (k0 < K) {
-      load4<TI>(re, k0, K, vec, x[g][0]);
-      if (im) load4<TI>(im, k0, K, vec, x[g][1]);
-    }
+__global__ void __launch_bounds__(256, 3) k_slice_digits_planned(const GSlab* slabs, const int* plan, int nslabs, int S,
+                                                              I8Slices out) {
+  int lo = 0, hi = nslabs - 1;
+  while (lo < hi) {   // last slab whose first block is <= this block
+    const int mid = (lo + hi + 1) >> 1;
+    if (plan[mid] <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
   }
-  const int e = out.exp[row];
-  bool one;
-  const double sc = scale_for(S, e, one);
+  const GSlab sb = slabs[lo];
+  const uint32_t gpr = (uint32_t)(sb.K + 3) / 4, total = (uint32_t)sb.rows * gpr;
+  const uint32_t first = ((uint32_t)blockIdx.x - (uint32_t)plan[lo]) * (uint32_t)kPlanGroups + threadIdx.x;
+  const TI* re0 = (const TI*)sb.re;
+  const TI* im0 = (const TI*)sb.im;
+  const bool split = sb.diag0 != kNoDiag && out.dg && !im0;
+  const bool vec = ((reinterpret_cast<uintptr_t>(re0) | reinterpret_cast<uintptr_t>(im0) |
+                     (uintptr_t)(sb.ld * (int64_t)sizeof(TI))) & 15) == 0;
   const int64_t ld = out.ld;
+#pragma unroll 1
+  for (uint32_t g0 = first; g0 < first + kPlanGroups && g0 < total; g0 += 512) {
+    double x[2][2][4] = {};
+    uint32_t rr[2], kk[2];
+    bool ok[2];
 #pragma unroll
-  for (int g = 0; g < 2; ++g) {
-    const int64_t k0 = base + g * (kStreamChunk / 2);
-    if (k0 >= K) continue;
-#pragma unroll
-    for (int plane = 0; plane < 2; ++plane) {
-      if (plane == 1 && !im) continue;
-      uint32_t pk[kMaxSlices] = {}, pn[kMaxSlices] = {};
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        double v = x[g][plane][j];
-        if (plane == 0 && k0 + j == dcol) v = 0.0;
-        const double xs = one ? v * sc : ldexp(ldexp(v, -e), 7 * S);
-        int d[kMaxSlices];
-        cut_digits(xs, S, d);
-#pragma unroll
-        for (int q = 0; q < kMaxSlices; ++q)
-          if (q < S) {
-            pk[q] |= ((uint32_t)(uint8_t)(int8_t)d[q]) << (8 * j);
-            if (NEG && plane == 1) pn[q] |= ((uint32_t)(uint8_t)(int8_t)(-d[q])) << (8 * j);
-          }
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t g = g0 + 256u * h;
+      ok[h] = g < total && g < first + kPlanGroups;
+      rr[h] = ok[h] ? g / gpr : 0;
+      kk[h] = ok[h] ? 4 * (g - rr[h] * gpr) : 0;
+      if (ok[h]) {
+        load4<TI>(re0 + (int64_t)rr[h] * sb.ld, kk[h], sb.K, vec, x[h][0]);
+        if (im0) load4<TI>(im0 + (int64_t)rr[h] * sb.ld, kk[h], sb.K, vec, x[h][1]);
       }
+    }
 #pragma unroll
-      for (int q = 0; q < kMaxSlices; ++q) {
-        if (q >= S) continue;
-        int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
-        if (dst) *reinterpret_cast<uint32_t*>(dst + row * ld + k0) = pk[q];
-        if (NEG && plane == 1 && out.neg_im[q]) *reinterpret_cast<uint32_t*>(out.neg_im[q] + row * ld + k0) = pn[q];
+    for (int h = 0; h < 2; ++h) {
+      if (!ok[h]) continue;
+      const int64_t row = (int64_t)sb.row0 + rr[h], k0 = kk[h];
+      const int64_t dcol = split ? (int64_t)rr[h] + sb.diag0 : -1;
+      const int e = out.exp[row];
+      bool one;
+      const double sc = scale_for(S, e, one);
+#pragma unroll
+      for (int plane = 0; plane < 2; ++plane) {
+        if (plane == 1 && !im0) continue;
+        uint32_t pk[kMaxSlices];
+        double xs[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          double v = x[h][plane][j];
+          if (plane == 0 && k0 + j == dcol) v = 0.0;
+          xs[j] = one ? v * sc : ldexp(ldexp(v, -e), 7 * S);
+        }
+        cut_digits4(xs, S, pk);
+#pragma unroll
+        for (int q = 0; q < kMaxSlices; ++q) {
+          if (q >= S) continue;
+          int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
+          if (dst) *reinterpret_cast<uint32_t*>(dst + row * ld + k0) = pk[q];
+          if (NEG && plane == 1 && out.neg_im[q])
+            *reinterpret_cast<uint32_t*>(out.neg_im[q] + row * ld + k0) = __vneg4(pk[q]);
+        }
       }
     }
   }
 }
-// Narrower rows go to the warp-per-row kernel: up to this width the rows in flight fit L2, so
-// its second read of a row is an L2 hit.
-constexpr int64_t kStreamSliceMinK = 1024;
-
 void make_map_u8(CUtensorMap* m, const int8_t* base, int64_t rows, int64_t cols, int64_t ld, int box_rows);
 
 }  // namespace
@@ -948,23 +953,31 @@ template void launch_slice_rows<float>(int, const float*, const float*, int64_t,
 template void launch_slice_rows<double>(int, const double*, const double*, int64_t, int64_t, int64_t, I8Slices,
                                         bool, cudaStream_t);
 
+std::vector<int> slice_plan(const std::vector<GSlab>& sorted) {
+  std::vector<int> plan(sorted.size() + 1, 0);
+  for (size_t i = 0; i < sorted.size(); ++i) {
+    const int64_t groups = (int64_t)sorted[i].rows * ((sorted[i].K + 3) / 4);
+    plan[i + 1] = plan[i] + (int)cdiv(groups, kPlanGroups);
+  }
+  return plan;
+}
+
 template <typename TI>
 void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, I8Slices out,
-                               bool want_neg_im, cudaStream_t s, int64_t kmax, int kind) {
+                               bool want_neg_im, cudaStream_t s, SlicePlan plan, int kind) {
   if (S < 3 || S > kMaxSlices) throw Error{FX_ERR_VALUE, "slice count must be 3, 4 or 5"};
   if (out.ld % 16 != 0) throw Error{FX_ERR_VALUE, "grouped slice: pitch must be a multiple of 16"};
   if (nslabs <= 0 || total_rows <= 0) return;
-  if (kind < 0) kind = kmax >= kStreamSliceMinK ? 1 : 0;
+  if (kind < 0) kind = plan.plan ? 1 : 0;
   if (kind == 1) {
-    if (kmax <= 0) throw Error{FX_ERR_VALUE, "grouped slice: the streaming kernel needs the widest row"};
-    const unsigned g1 = (unsigned)cdiv(total_rows, 8);
-    const dim3 g2((unsigned)total_rows, (unsigned)cdiv(kmax, kStreamChunk));
-    k_row_exp_grouped<TI><<<g1, 256, 0, s>>>(slabs, nslabs, total_rows, out);
+    if (!plan.plan) throw Error{FX_ERR_VALUE, "grouped slice: the two-pass slicer needs a block plan"};
+    k_row_exp_grouped<TI><<<(unsigned)cdiv(total_rows, 8), 256, 0, s>>>(slabs, nslabs, total_rows, out);
     FX_LAUNCH_CHECK();
+    if (plan.blocks <= 0) return;
     if (want_neg_im)
-      k_slice_stream_grouped<TI, true><<<g2, 256, 0, s>>>(slabs, nslabs, S, out);
+      k_slice_digits_planned<TI, true><<<plan.blocks, 256, 0, s>>>(slabs, plan.plan, nslabs, S, out);
     else
-      k_slice_stream_grouped<TI, false><<<g2, 256, 0, s>>>(slabs, nslabs, S, out);
+      k_slice_digits_planned<TI, false><<<plan.blocks, 256, 0, s>>>(slabs, plan.plan, nslabs, S, out);
     FX_LAUNCH_CHECK();
     return;
   }
@@ -975,9 +988,9 @@ void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t to
   FX_LAUNCH_CHECK();
 }
 template void launch_slice_rows_grouped<float>(int, const GSlab*, int, int64_t, I8Slices, bool, cudaStream_t,
-                                               int64_t, int);
+                                               SlicePlan, int);
 template void launch_slice_rows_grouped<double>(int, const GSlab*, int, int64_t, I8Slices, bool, cudaStream_t,
-                                                int64_t, int);
+                                                SlicePlan, int);
 
 
 namespace {

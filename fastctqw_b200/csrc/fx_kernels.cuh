@@ -312,13 +312,21 @@ struct GSlab {
                         // which is left out of the slices and written to I8Slices::dg
 };
 constexpr int kNoDiag = -(1 << 30);
-// kmax: the widest slab (K) of the launch, when known (> 0): launches with rows of 1024 columns
-// or more are sliced in two streaming passes (row exponents, then digits over row chunks).
-// kind: -1 by kmax as above, 0 the warp-per-row kernel, 1 the two streaming passes (both give
-// the same digits; the choice is for the kernel tests).
+// Block plan of the two-pass slicer over slabs sorted by row0 (device copy of slice_plan's
+// prefix: plan[i] = first digit-pass block of slab i, plan[nslabs] = blocks).
+constexpr int kPlanGroups = 2048;   // 4-column groups per digit-pass block
+struct SlicePlan {
+  const int* plan = nullptr;
+  int blocks = 0;
+};
+std::vector<int> slice_plan(const std::vector<GSlab>& sorted);
+// With a plan: two passes, row exponents (a warp per row) and then the digits over the plan's
+// blocks (each slab's rows x K elements in row-major order); without one: a warp per row that
+// reads the row twice.  kind: -1 by the plan, 0 / 1 to choose (both give the same digits; the
+// choice is for the kernel tests).
 template <typename TI>
 void launch_slice_rows_grouped(int S, const GSlab* slabs, int nslabs, int64_t total_rows, I8Slices out,
-                               bool want_neg_im, cudaStream_t s, int64_t kmax = 0, int kind = -1);
+                               bool want_neg_im, cudaStream_t s, SlicePlan plan = SlicePlan(), int kind = -1);
 // In place A <- (A + A^T) / 2 of an n x n plane (exact symmetry of a result known to be
 // symmetric in exact arithmetic).
 template <typename T>

@@ -219,9 +219,9 @@ const char* fx_product_error(void);
 /* Diagnostics (no counterpart in the reference): the grouped int8 slicer of the product kernels
  * on one block of `rows` rows of FP64 planes (device buffers, row pitch ld elements).  Each row
  * is scaled by 2^(7S - e), e its exponent (as the products use it), and cut into S signed
- * digits from the top with round-half-even.  kind 0: warp-per-row kernel, 1: the two streaming
- * passes (row exponents, then digits over row chunks) that rows of 1024 columns or more take;
- * both give the same digits.  im may be null; split_diag (single plane, dg non-null) leaves row
+ * digits from the top with round-half-even.  kind 0: warp-per-row kernel, 1: the two passes the
+ * products use (row exponents by a warp per row, then the digits over a block plan of the rows'
+ * elements); both give the same digits.  im may be null; split_diag (single plane, dg non-null) leaves row
  * r's element at column r out of the slices and writes it to dg[r]; neg (im non-null) also
  * writes the digits of -im.  out: 3 S planes of rows x ldo bytes (re digits 0..S-1, im, -im;
  * ldo >= K, a multiple of 16), exps: rows int32.  Messages through fx_product_error. */

@@ -3,11 +3,12 @@
 Every FP64 row is scaled by 2^(7S - e), e the row exponent (frexp of the row maximum, raised by
 one when the mantissa would round to 128 at 7 bits), and cut into S signed digits from the top
 with round-half-even: d_0 = rint(v / 2^7(S-1)), then the remainders.  The two kernels (a warp per
-row for narrow rows; two streaming passes, row exponents and then digits over row chunks, for
-rows of 1024 columns or more) must give the same digits, bit for bit, and both must equal this
-rule restated in numpy below; the product kernels rely on both (exactness of the int32 level
-sums, symmetric digits).  Rows cover zero, tiny (the two-step scaling), ragged widths, exact
-half-way values and the split-off diagonal.
+row that reads the row twice; and the two passes the products use, row exponents by a warp per
+row and then the digits over a block plan of the rows' elements) must give the same digits, bit
+for bit, and both must equal this rule restated in numpy below; the product kernels rely on it
+(exactness of the int32 level sums, symmetric digits).  Rows cover zero, tiny (the two-step
+scaling), ragged widths (K not a multiple of 4 included), exact half-way values and the
+split-off diagonal.
 """
 import numpy as np
 import pytest
@@ -48,7 +49,7 @@ def _rows(rows, K, seed):
     return x
 
 
-@pytest.mark.parametrize("K", [1024, 3000, 2050, 96])
+@pytest.mark.parametrize("K", [1024, 3000, 2050, 96, 4097])
 @pytest.mark.parametrize("S", [3, 4, 5])
 def test_slicers_agree_with_the_digit_rule(K, S):
     import torch
