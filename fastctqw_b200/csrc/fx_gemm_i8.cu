@@ -840,6 +840,7 @@ __global__ void __launch_bounds__(256, 3) k_slice_digits_planned(const GSlab* sl
   const bool vec = ((reinterpret_cast<uintptr_t>(re0) | reinterpret_cast<uintptr_t>(im0) |
                      (uintptr_t)(sb.ld * (int64_t)sizeof(TI))) & 15) == 0;
   const int64_t ld = out.ld;
+  const double inv_gpr = 1.0 / (double)gpr;
 #pragma unroll 1
   for (uint32_t g0 = first; g0 < first + kPlanGroups && g0 < total; g0 += 512) {
     double x[2][2][4] = {};
@@ -849,7 +850,13 @@ __global__ void __launch_bounds__(256, 3) k_slice_digits_planned(const GSlab* sl
     for (int h = 0; h < 2; ++h) {
       const uint32_t g = g0 + 256u * h;
       ok[h] = g < total && g < first + kPlanGroups;
-      rr[h] = ok[h] ? g / gpr : 0;
+      uint32_t q = 0;
+      if (ok[h]) {   // g / gpr through the reciprocal (the FP64 pipe has room, the integer ALU not)
+        q = (uint32_t)((double)g * inv_gpr);
+        if (q * gpr > g) --q;
+        else if ((q + 1) * gpr <= g) ++q;
+      }
+      rr[h] = q;
       kk[h] = ok[h] ? 4 * (g - rr[h] * gpr) : 0;
       if (ok[h]) {
         load4<TI>(re0 + (int64_t)rr[h] * sb.ld, kk[h], sb.K, vec, x[h][0]);
