@@ -780,7 +780,7 @@ def main():
                        "n": n, "t": args.t, "form": args.form, "selector": args.selector,
                        "selection_outcome": st["sel_outcome"], "m": st["m"], "s": st["s"],
                        "plain_m": st["plain_m"], "plain_s": st["plain_s"],
-                       "solver": "cholesky(Q^H Q)" if st["solver"] == 1 else "pivoted LU",
+                       "solver": {0: "pivoted LU", 1: "cholesky(Q^H Q)", 2: "newton-schulz(Q^H Q)"}[st["solver"]],
                        "l2": "working set ~25 GB >> 126 MB L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
             "clocks": clk, "e2e": e2e, "gpu_launches": int(st["launches"]) * args.steps,

@@ -1156,7 +1156,7 @@ class BatchPipeline {
     st->structured = 1;
     st->rank1_shift = rank1_[w];
     st->symmetric = 1;
-    st->solver = 1;
+    st->solver = uses_newton(w) ? 2 : 1;
     st->norm1 = norms_[8 * w];
     st->d[0] = std::pow(norms_[8 * w + 1], 0.25);
     st->d[1] = std::pow(norms_[8 * w + 2], 1.0 / 6);
@@ -2328,10 +2328,7 @@ class BatchPipeline {
     // block steps); smaller walks, whose few steps run grouped over the batch, keep the
     // Cholesky solve
     std::vector<int> ns_list, ch_list;
-    for (int w = 0; w < W; ++w) {
-      const bool ns = solve_mode_ == 2 || (solve_mode_ == 0 && walks_[w].np >= kNewtonMinNp);
-      (ns ? ns_list : ch_list).push_back(w);
-    }
+    for (int w = 0; w < W; ++w) (uses_newton(w) ? ns_list : ch_list).push_back(w);
     by_slices(ns_list, ps, [&](const std::vector<int>& l) { newton_solve(st, r, l); });   // R re -> A4, im -> A2
     by_slices(ch_list, ps, [&](const std::vector<int>& l) {
       tag_ = kTagCholesky;
@@ -2624,6 +2621,10 @@ class BatchPipeline {
     }
   }
 
+  // Walk w solves the Pade step by Newton-Schulz (else Cholesky).
+  bool uses_newton(int w) const {
+    return solve_mode_ == 2 || (solve_mode_ == 0 && walks_[w].np >= kNewtonMinNp);
+  }
   // Walk w takes the mixed form's reduced slice counts (powers, squarings, early Newton-Schulz
   // steps; the Pade and solve products by pade_slices_of).
   bool reduced(int w) const { return form_ == 1 && walks_[w].np >= kMixedMinNp; }

@@ -139,7 +139,8 @@ typedef struct fx_stats {
   int32_t symmetric;    /* 1 if X^T == X (no transposes needed)          */
   int32_t gemm_launches;/* matrix-product kernel launches in the run     */
   int32_t launches;     /* all kernel launches of the run                */
-  int32_t solver;       /* 0 pivoted LU, 1 Cholesky of Q^H Q (normal Q)  */
+  int32_t solver;       /* 0 pivoted LU, 1 Cholesky of Q^H Q (normal Q), 2 Newton-Schulz
+                           inverse of Q^H Q                                            */
   int32_t reserved;
   double norm1;         /* ||X - shifts||_1                              */
   double d[5];          /* d4, d6, d8, d10, log2 ||(|A|)^27||_1          */
