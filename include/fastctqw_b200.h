@@ -60,7 +60,7 @@ enum fx_form {
                          Ozaki slices, exact int32 accumulation; default for complex64.
                          Walk generators: the powers, Pade and solve products split
                          their operands' diagonals off (added in FP64); walks padded to
-                         4096 or more, or needing 12 or more squarings, square as three
+                         4096 or more, or needing 8 or more squarings, square as three
                          split products Re^2, Im^2, (Re+Im)^2, the others as the exact
                          complex square                                               */
   FX_FORM_MIXED = 1,  /* reduced-precision products (complex64 / float32 handles).  Walk

@@ -54,3 +54,32 @@ def test_long_time_walks_meet_the_bar(form):
         q = q.to(torch.complex128)
         inf = float(1.0 - torch.vdot(ref, q).abs() ** 2 / (torch.vdot(q, q).real * torch.vdot(ref, ref).real))
         assert inf <= 1e-10, (form, walks[k][1], int(s[k]), inf)
+
+
+def test_regular_laplacian_walk_with_nine_squarings():
+    """A 3-regular Laplacian walk (N = 2784, graph seed 2034370348, t = 583.08..., the selector
+    family's generator; 9 squarings) on which the exact complex square reached 2.6e-9: its
+    iterates' dominant diagonal costs the unsplit slices their bits, and the chain amplifies
+    that 2^9.  Both forms now square it as three split products."""
+    import torch
+    from fastctqw_b200 import graphs
+    from fastctqw_b200.batch import WalkBatch
+    dev = torch.device("cuda", 0)
+    n, d, gseed, t = 2784, 3, 2034370348, 583.0815413536579
+    A = graphs.random_regular(n, d, gseed, np.float64)
+    X = np.asarray(-1j * (-(np.diag(A.sum(axis=1)) - A)) * t, dtype=np.complex64)
+    lam, V = torch.linalg.eigh(torch.from_numpy(np.ascontiguousarray(X.imag, dtype=np.float64)).to(dev))
+    Vc = V.to(torch.complex128)
+    for form in ("plain", "mixed"):
+        for a, b in ((0, -1), (0, 1), (-2, -1)):   # pairs of eigenvectors at the spectrum's ends
+            p0 = (V[:, a] + V[:, b]) / math.sqrt(2.0)
+            ref = Vc @ (torch.exp(1j * lam) * (Vc.T @ p0.to(torch.complex128)))
+            out = [torch.empty(n, dtype=torch.complex64, device=dev)]
+            with WalkBatch([n], form=form) as bt:
+                bt.run_device([torch.from_numpy(X).to(dev)], [p0.to(torch.complex64)], out)
+                torch.cuda.synchronize()
+                _, s = bt.selection()
+            q = out[0].to(torch.complex128)
+            inf = float(1.0 - torch.vdot(ref, q).abs() ** 2 / (torch.vdot(q, q).real * torch.vdot(ref, ref).real))
+            assert inf <= 1e-10, (form, a, b, int(s[0]), inf)
+
