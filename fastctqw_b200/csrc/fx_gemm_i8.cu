@@ -386,8 +386,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_i8(const __grid_constant__
     constexpr int kW = kEpiWarps == 16 ? 8 : 16;
     constexpr int kChunks = kCols / kW;
     static_assert(kCols % kW == 0, "epilogue chunks");
-    // drain all of a warp's columns before handing TMEM back when they fit in registers
-    constexpr bool kEarly = kCols <= (kEpiWarps == 16 ? 24 : 48);
+    // drain all of a warp's columns before handing TMEM back when they fit in registers: with
+    // 16 epilogue warps up to 32 folded columns (the 128-column tiles of 4 slices too, whose
+    // few spills cost less than an MMA warp idle for the whole epilogue: products of the
+    // N = 10000 walk 167 -> 153 ms)
+    constexpr bool kEarly = kCols <= (kEpiWarps == 16 ? 32 : 48);
     int it = 0;
     for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++it) {
       if constexpr (G) {
