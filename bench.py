@@ -357,12 +357,12 @@ def bench_batch(args, dev):
         return ev0.elapsed_time(ev1) / reps
 
     plain_batch_ms = None
-    if args.selector != "plain" or args.form != "plain":
+    if args.selector != "plain" or args.form != "plain" or args.approx != "pade":
         bpl = WalkBatch(ns, autotune=not args.no_autotune)
         plain_batch_ms = timed(bpl)
         _, s_plain = bpl.selection()
         bpl.close()
-    b = WalkBatch(ns, selector=args.selector, form=args.form,
+    b = WalkBatch(ns, selector=args.selector, form=args.form, approx=args.approx,
                   autotune=not args.no_autotune)   # tuned in the warm-up
     batch_ms = timed(b)
     info = b.info()
@@ -411,6 +411,7 @@ def bench_batch(args, dev):
         "launches_per_batch": info["launches"], "algorithmic_tflops": round(info["flops"] / (batch_ms * 1e-3) / 1e12, 1),
         "selector": args.selector,
         "form": args.form,
+        "approx": args.approx,
         "plain_form_ms": round(plain_batch_ms, 2) if plain_batch_ms else None,
         "plain_form_walks_per_s": round(walks / (plain_batch_ms * 1e-3), 1) if plain_batch_ms else None,
         "squarings_chosen": int(s.sum()), "squarings_plain": int(s_plain.sum()) if plain_batch_ms else None,
@@ -439,7 +440,8 @@ def bench_batch_sharded(args, dev, rank, world):
     def runner(xs, ps):
         key = tuple(X.shape[0] for X in xs)
         if key not in cache:
-            cache[key] = WalkBatch(list(key), np.complex64, selector=args.selector, form=args.form)
+            cache[key] = WalkBatch(list(key), np.complex64, selector=args.selector, form=args.form,
+                                   approx=args.approx)
         return cache[key].run(xs, ps)
 
     if args.selector == "learned":
@@ -542,6 +544,9 @@ def main():
                     help="precision form of the timed walk; the plain form is timed beside it")
     ap.add_argument("--selector", default="learned", choices=["plain", "certified", "estimated", "learned"],
                     help="(m, s) selection of the timed walk; the plain selection is timed beside it")
+    ap.add_argument("--approx", default="pade", choices=["pade", "chebyshev"],
+                    help="approximant of the timed walk before its squarings (Pade + solve, or the "
+                         "Chebyshev-Bessel polynomial); the plain form beside it is Pade")
     ap.add_argument("--ref-sample-n", type=int, default=1024,
                     help="size of the small sample behind the flop-model cross-check of the reference arm")
     ap.add_argument("--ref-budget-s", type=float, default=150.0,
@@ -599,7 +604,7 @@ def main():
         from fastctqw_b200 import selector as sel
         sel.set_weights()
     eng = Engine(n, np.complex64)
-    eng.configure(form=args.form, selector=args.selector)
+    eng.configure(form=args.form, selector=args.selector, approx=args.approx)
     stream = torch.cuda.current_stream(dev)
 
     def step():
@@ -661,7 +666,9 @@ def main():
     traffic = product_traffic_per_launch(args.form)
     roofline = {
         "bound": "tensor",
-        "kernel": ("k_gemm_i8<4,double> and <3,double> (int8 Ozaki-slice products, exact accumulation; "
+        "kernel": ("k_gemm_i8<4,double> (int8 Ozaki-slice products, exact accumulation; 4 slices)"
+                   if args.form == "mixed" and args.approx == "chebyshev" else
+                   "k_gemm_i8<4,double> and <3,double> (int8 Ozaki-slice products, exact accumulation; "
                    "4 slices, the early Newton-Schulz steps 3)" if args.form == "mixed" else
                    "k_gemm_i8<5,double> (int8 Ozaki-slice product, exact accumulation)"),
         "achieved": round(achieved, 1) if achieved else None, "peak": round(int8_peak, 1), "unit": "TOP/s (int8)",
@@ -684,8 +691,8 @@ def main():
     # Higham) selection on the same walk, timed the same way
     plain = None
     psi_plain = None
-    if args.selector != "plain" or args.form != "plain":
-        eng.configure(form="plain", selector="plain")
+    if args.selector != "plain" or args.form != "plain" or args.approx != "pade":
+        eng.configure(form="plain", selector="plain", approx="pade")
         dU_plain = torch.empty_like(dX)      # dU keeps the timed walk's U for the accuracy check
 
         def step_plain():
@@ -704,7 +711,7 @@ def main():
         psi_plain = dpsi.clone()
         del dU_plain
         torch.cuda.empty_cache()
-        eng.configure(form=args.form, selector=args.selector)
+        eng.configure(form=args.form, selector=args.selector, approx=args.approx)
 
     # ---- accuracy of both against the FP64 eigendecomposition propagator
     accuracy = None
@@ -717,7 +724,7 @@ def main():
     if rank == 0 and not args.no_e2e:
         X_pinned = torch.from_numpy(X).pin_memory().numpy()
         em = fastexpm.ExpMatComplex64(n)
-        em.configure(form=args.form, selector=args.selector)
+        em.configure(form=args.form, selector=args.selector, approx=args.approx)
         em.run(X_pinned)
         e_steps = max(1, min(args.steps, 3))
         t0 = time.perf_counter()
@@ -778,9 +785,11 @@ def main():
             "data": "synthetic (seeded G(n,0.5) Laplacian)",
             "config": {"workload": f"dense ER G(n={n}, p=0.5) Laplacian, t={args.t}, complex64 expm + U psi0, psi0=|0>",
                        "n": n, "t": args.t, "form": args.form, "selector": args.selector,
+                       "approx": args.approx, "degree": st["degree"],
                        "selection_outcome": st["sel_outcome"], "m": st["m"], "s": st["s"],
                        "plain_m": st["plain_m"], "plain_s": st["plain_s"],
-                       "solver": {0: "pivoted LU", 1: "cholesky(Q^H Q)", 2: "newton-schulz(Q^H Q)"}[st["solver"]],
+                       "solver": {0: "pivoted LU", 1: "cholesky(Q^H Q)", 2: "newton-schulz(Q^H Q)",
+                                  3: "none (Chebyshev polynomial)"}[st["solver"]],
                        "l2": "working set ~25 GB >> 126 MB L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
             "clocks": clk, "e2e": e2e, "gpu_launches": int(st["launches"]) * args.steps,

@@ -23,8 +23,9 @@ FORM_PLAIN, FORM_MIXED, FORM_SIMT, FORM_FP64 = 0, 1, 2, 3
 FORMS = {"plain": FORM_PLAIN, "mixed": FORM_MIXED, "simt": FORM_SIMT, "fp64": FORM_FP64}
 (OPT_FORM, OPT_SHIFT, OPT_STRUCTURE, OPT_FORCE_S, OPT_FORCE_M, OPT_TIMEOUT_MS, OPT_IPE, OPT_REFINE,
  OPT_DEBUG_STAGE, OPT_PROFILE, OPT_SELECTOR, OPT_INJECT_STALL, OPT_SQ_N4, OPT_SQ_N3, OPT_DRIFT,
- OPT_PADE_SLICES, OPT_NEWTON_SLICES, OPT_SOLVE) = range(18)
+ OPT_PADE_SLICES, OPT_NEWTON_SLICES, OPT_SOLVE, OPT_APPROX) = range(19)
 SOLVES = {"auto": 0, "cholesky": 1, "newton": 2}
+APPROXES = {"pade": 0, "chebyshev": 1}
 SELECTORS = {"plain": 0, "certified": 1, "learned": 2, "estimated": 3}
 
 OK, ERR_TYPE, ERR_VALUE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_NONFINITE, ERR_SINGULAR, ERR_NODEV, ERR_FREED = range(10)
@@ -35,7 +36,7 @@ class FxStats(ctypes.Structure):
                 ("structured", ctypes.c_int32), ("rank1_shift", ctypes.c_int32),
                 ("symmetric", ctypes.c_int32), ("gemm_launches", ctypes.c_int32),
                 ("launches", ctypes.c_int32), ("solver", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("norm1", ctypes.c_double),
+                ("degree", ctypes.c_int32), ("norm1", ctypes.c_double),
                 ("d", ctypes.c_double * 5), ("ms_total", ctypes.c_double),
                 ("flops", ctypes.c_double), ("prod_ms", ctypes.c_double),
                 ("prod_ops", ctypes.c_double), ("prod_flops", ctypes.c_double),
@@ -44,7 +45,7 @@ class FxStats(ctypes.Structure):
                 ("plain_m", ctypes.c_int32), ("plain_s", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
-        out = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("d", "reserved", "reserved2")}
+        out = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("d", "reserved2")}
         out["d4"], out["d6"], out["d8"], out["d10"], out["log2_abs27"] = list(self.d)
         return out
 
@@ -63,6 +64,9 @@ SIGNATURES = {
     "fx_spectral_radius": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
     "fx_batch_force_selection": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
     "fx_batch_spectral": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+    "fx_chebyshev_plan": [ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_int32),
+                          ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                          ctypes.POINTER(ctypes.c_int32)],
     "fx_unitarity_drift": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int32,
                            ctypes.POINTER(ctypes.c_int32)],
     "fx_batch_drift": [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double), ctypes.c_int32,
@@ -226,6 +230,18 @@ def tensor_peak(kind: str = "int8", iters: int = 50000, reps: int = 5, stream=No
             "all_tops": [round(v[0], 1) for v in vals]}
 
 
+def chebyshev_plan(rho: float, tol: float = 1e-6) -> dict:
+    """The Chebyshev approximant's plan for a spectral bound rho (fx_chebyshev_plan; host
+    arithmetic, no device): squarings s, degree, baby steps and matrix products of the walk."""
+    s, d, m, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    rc = lib().fx_chebyshev_plan(float(rho), float(tol), ctypes.byref(s), ctypes.byref(d),
+                                 ctypes.byref(m), ctypes.byref(c))
+    if rc != OK:
+        msg = lib().fx_batch_last_error(None)
+        raise ValueError(msg.decode() if msg else f"error code {rc}")
+    return {"s": s.value, "degree": d.value, "baby": m.value, "cost": c.value}
+
+
 def device_ok() -> bool:
     return bool(lib().fx_device_ok())
 
@@ -256,7 +272,8 @@ class Engine:
                   profile: bool | None = None, selector: str | None = None,
                   inject_stall: int | None = None, sq_n4: int | None = None, sq_n3: int | None = None,
                   drift: bool | None = None, pade_slices: int | None = None,
-                  newton_slices: int | None = None, solve: str | None = None) -> None:
+                  newton_slices: int | None = None, solve: str | None = None,
+                  approx: str | None = None) -> None:
         if form is not None:
             if form not in FORMS:
                 raise ValueError(f"form must be one of {sorted(FORMS)}")
@@ -297,6 +314,10 @@ class Engine:
             if solve not in SOLVES:
                 raise ValueError(f"solve must be one of {sorted(SOLVES)}")
             self.set_option(OPT_SOLVE, SOLVES[solve])
+        if approx is not None:
+            if approx not in APPROXES:
+                raise ValueError(f"approx must be one of {sorted(APPROXES)}")
+            self.set_option(OPT_APPROX, APPROXES[approx])
 
     def spectral_radius(self) -> dict:
         """Lanczos estimate and rigorous upper bound of the shifted generator's spectral radius

@@ -23,9 +23,11 @@ from ._native import check, lib
 OPT_GRAPH, OPT_TIMEOUT_MS, OPT_FORCE_M, OPT_SELECTOR, OPT_ANALYZE_ONLY, OPT_DIAG_SPLIT = 0, 1, 2, 3, 4, 5
 OPT_AUTOTUNE, OPT_TILE_GROUP, OPT_TILE_ORDER, OPT_SAMPLE_WALKS = 6, 7, 8, 9
 OPT_FORM, OPT_SQ_N4, OPT_SQ_N3, OPT_DRIFT, OPT_PADE_SLICES, OPT_NEWTON_SLICES, OPT_SOLVE = 10, 11, 12, 13, 14, 15, 16
+OPT_APPROX = 17
 OUTCOMES = {0: "plain", 1: "certified", 2: "learned", 3: "estimated",
             -1: "learned rejected by the bound, plain (m, s) kept",
-            -2: "failed an a-posteriori check, redone with the plain (m, s)", 4: "forced (m, s)"}
+            -2: "failed an a-posteriori check, redone with the plain (m, s)", 4: "forced (m, s)",
+            5: "Chebyshev polynomial"}
 
 
 def _check(rc: int, h) -> None:
@@ -54,7 +56,7 @@ class WalkBatch:
                  analyze_only: bool = False, diag_split: int = 7, autotune: bool = False,
                  form: str = "plain", sq_n4: int | None = None, sq_n3: int | None = None,
                  drift: bool = False, pade_slices: int | None = None,
-                 newton_slices: int | None = None, solve: str = "auto") -> None:
+                 newton_slices: int | None = None, solve: str = "auto", approx: str = "pade") -> None:
         self.ns = [int(n) for n in ns]
         self.dtype = np.dtype(dtype)
         if self.dtype not in (np.dtype(np.complex64), np.dtype(np.complex128)):
@@ -83,6 +85,10 @@ class WalkBatch:
             self.set_option(OPT_NEWTON_SLICES, newton_slices)
         if solve != "auto":
             self.set_option(OPT_SOLVE, _native.SOLVES[solve])
+        if approx != "pade":
+            if approx not in _native.APPROXES:
+                raise ValueError(f"approx must be one of {sorted(_native.APPROXES)}")
+            self.set_option(OPT_APPROX, _native.APPROXES[approx])
         if form != "plain":
             if form != "mixed":
                 raise ValueError("batched walks take form 'plain' or 'mixed'")

@@ -66,9 +66,6 @@ struct BWalk {
 };
 
 // ------------------------------------------------------------------ grouped elementwise
-struct Planes4 {
-  const double* m[4];
-};
 struct Planes5 {
   const double* m[5];
 };
@@ -80,22 +77,27 @@ struct RChunk {
   int w, r0, r1, pad;   // walk, rows [r0, r1)
 };
 
-// D = sum_k c_k M_k + g I on the np x np block of every chunk's walk; coef[w] = (c0..c3, g).
-// Two elements per thread (np is even); 32-bit indices within the chunk.
-__global__ void kb_combo(double* D, Planes4 M, const RChunk* ch, const BWalk* wk, const double* coef) {
+// D = sum_k c_k M_k + g I on the np x np block of every chunk's walk; coef[(NP + 1) w ..] =
+// (c_0..c_{NP-1}, g).  Two elements per thread (np is even); 32-bit indices within the chunk.
+template <int NP>
+struct PlanesN {
+  const double* m[NP];
+};
+template <int NP>
+__global__ void kb_combo(double* D, PlanesN<NP> M, const RChunk* ch, const BWalk* wk, const double* coef) {
   const RChunk q = ch[blockIdx.x];
   const BWalk b = wk[q.w];
-  const double* c = coef + 5 * q.w;
+  const double* c = coef + (NP + 1) * q.w;
   const uint32_t half = (uint32_t)b.np / 2, total = (uint32_t)(q.r1 - q.r0) * half;
-  const double2* src[4];
-  double cc[4];
+  const double2* src[NP];
+  double cc[NP];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {   // a zero coefficient skips the term: its plane may be unset
+  for (int k = 0; k < NP; ++k) {   // a zero coefficient skips the term: its plane may be unset
     const bool on = M.m[k] && c[k] != 0.0;
     cc[k] = on ? c[k] : 0.0;
     src[k] = on ? reinterpret_cast<const double2*>(M.m[k] + b.off) : nullptr;
   }
-  const double g = c[4];
+  const double g = c[NP];
   double2* dst = reinterpret_cast<double2*>(D + b.off);
   for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
     const uint32_t rr = t / half, c2 = t - rr * half;
@@ -103,7 +105,7 @@ __global__ void kb_combo(double* D, Planes4 M, const RChunk* ch, const BWalk* wk
     const int64_t e2 = r * half + c2;   // double2 index of (r, 2 c2)
     double vx = 0.0, vy = 0.0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < NP; ++k)
       if (src[k]) {
         const double2 m = src[k][e2];
         vx += cc[k] * m.x;
@@ -114,6 +116,7 @@ __global__ void kb_combo(double* D, Planes4 M, const RChunk* ch, const BWalk* wk
     dst[e2] = make_double2(vx, vy);
   }
 }
+using Planes4 = PlanesN<4>;
 
 // Two linear combinations of the same planes in one pass: D1 = sum_k c_k M_k (+ g1 on the
 // diagonal), D2 = sum_k d_k M_k (+ g2); coef[12 w ..] = (c_0..c_4, g1, d_0..d_4, g2).  A plane
@@ -947,6 +950,164 @@ constexpr double kLanMargin = 0.10;
 // gives an infidelity of at most sin^2(phi) for any state, so 1e-5 keeps it below 1e-10.
 constexpr double kGateTol = 1e-5;
 
+}  // namespace
+
+// ---- Chebyshev-Bessel polynomial stage for walk generators Y = i B (FX_OPT_APPROX = 1).
+// On [-1, 1], e^{iaz} = J_0(a) + 2 sum_{k>=1} i^k J_k(a) T_k(z) (Jacobi-Anger; Tal-Ezer &
+// Kosloff 1984).  With rho >= the spectral radius of B, Z = B / rho and a = rho / 2^s, the
+// polynomial truncated after degree D approximates e^{iB/2^s} to 2 sum_{k>D} |J_k(a)| on the
+// whole spectrum, and the s squarings multiply that by at most 2^s.  No Pade solve: every step
+// is a product of two commuting real symmetric matrices (polynomials in B).
+//
+// Evaluation: even part sum_j e_j T_j(C) with C = T_2(Z) = 2Z^2 - I (T_2j(Z) = T_j(C)); odd part
+// Z sum_j b_j T_j(C), its coefficients moved from T_2k+1(Z) onto Z T_j(C) =
+// (T_2j+1(Z) + T_2j-1(Z)) / 2; each part written as sum_g T_g(G) r_g(C) with G = T_m(C) and
+// deg r_g < m (baby steps T_1..T_m of C; T_g(T_m) = T_gm) and summed by Clenshaw's recurrence in
+// G.  The plan (s, D, m) is the cheapest in matrix products, kChebSquareProducts per squaring.
+constexpr int kChebMaxBaby = 5;          // baby steps T_1..T_5 of C (arenas)
+constexpr int kChebSquareProducts = 3;   // cost of one squaring in the plan
+constexpr double kChebMaxA = 1024.0;     // larger a would need hundreds of products: skipped
+// Margin on the Lanczos estimate where the selection uses it: outside [-1, 1] the truncated
+// series grows like cosh(D acosh|z|), so the interval must hold the whole spectrum.
+constexpr double kChebLanMargin = 0.25;
+
+// J_0(a) .. J_kmax(a), a >= 0, by Miller's backward recurrence J_{k-1} = (2k / a) J_k - J_{k+1}
+// from far above max(kmax, a), normalised by J_0 + 2 sum_{k>=1} J_2k = 1 (Abramowitz & Stegun
+// 9.1.27, 9.1.46).
+std::vector<double> bessel_j(double a, int kmax) {
+  std::vector<double> out((size_t)kmax + 1, 0.0);
+  if (a == 0.0) {
+    out[0] = 1.0;
+    return out;
+  }
+  int top = std::max(kmax, (int)a) + 20 + (int)std::sqrt(40.0 * std::max((double)kmax, a));
+  top += top & 1;
+  std::vector<double> v((size_t)top + 1, 0.0);
+  double jp = 0.0, j = 1e-300;
+  v[top] = j;
+  for (int k = top; k > 0; --k) {
+    const double jm = (2.0 * k / a) * j - jp;
+    jp = j;
+    j = jm;
+    v[k - 1] = j;
+    if (std::fabs(j) > 1e250) {
+      for (int i = k - 1; i <= top; ++i) v[i] *= 1e-250;
+      jp *= 1e-250;
+      j *= 1e-250;
+    }
+  }
+  double norm = 0.0;
+  for (int k = 2; k <= top; k += 2) norm += v[k];
+  norm = v[0] + 2.0 * norm;
+  for (int k = 0; k <= kmax; ++k) out[k] = v[k] / norm;
+  return out;
+}
+// Smallest D with 2 sum_{k>D} |J_k(a)| <= tol.
+int cheb_degree(double a, double tol) {
+  const int kmax = (int)a + 80 + (int)(8.0 * std::pow(std::max(a, 1.0), 1.0 / 3.0));
+  const std::vector<double> J = bessel_j(a, kmax);
+  std::vector<double> tail((size_t)kmax + 2, 0.0);
+  for (int k = kmax; k >= 0; --k) tail[k] = tail[k + 1] + std::fabs(J[k]);
+  for (int d = 0; d < kmax; ++d)
+    if (2.0 * tail[d + 1] <= tol) return d;
+  return kmax;
+}
+// Degrees in C of the even part and of the odd part's cofactor (-1: none).
+void cheb_parts(int D, int* je, int* jo) {
+  *je = D / 2;
+  *jo = D >= 1 ? (D - 1) / 2 : -1;
+}
+// Highest baby step T_k(C) the plan computes: G = T_m when a chain has a giant step, else the
+// parts' own degree (their sums are then linear combinations of T_0..T_top).
+int cheb_baby_top(int D, int m) {
+  int je, jo;
+  cheb_parts(D, &je, &jo);
+  if (D <= 1) return 0;
+  if (je / m >= 1 || (jo >= 0 && jo / m >= 1)) return m;
+  return std::max(je, jo);
+}
+// Products of the polynomial stage: baby steps T_2..T_top, the two Clenshaw chains (floor(j / m)
+// products each) and the product by Z of the odd chain (none when its degree is 0).
+int cheb_plan_cost(int D, int m) {
+  int je, jo;
+  cheb_parts(D, &je, &jo);
+  if (D <= 1) return 0;
+  return std::max(cheb_baby_top(D, m) - 1, 0) + je / m + (jo >= 1 ? jo / m + 1 : 0);
+}
+struct ChebPlan {
+  int s = 0, degree = 0, baby = 1, cost = 0;
+  double a = 0.0;
+  bool ok = false;   // false: rho / 2^60 above kChebMaxA (no plan)
+};
+// The cheapest (s, D, m) for the spectral bound rho at error tol after the squarings (ties to
+// the smaller s and the smaller m).
+ChebPlan cheb_plan(double rho, double tol) {
+  ChebPlan best;
+  bool have = false;
+  for (int s = 0; s <= 60; ++s) {
+    const double a = std::ldexp(rho, -s);
+    if (a > kChebMaxA) continue;
+    const int D = cheb_degree(a, std::ldexp(tol, -s));
+    int bc = 0, bm = 1;
+    for (int m = 1; m <= kChebMaxBaby; ++m) {
+      const int c = cheb_plan_cost(D, m);
+      if (m == 1 || c < bc) {
+        bc = c;
+        bm = m;
+      }
+    }
+    const int tot = bc + kChebSquareProducts * s;
+    if (!have || tot < best.cost) {
+      best.s = s;
+      best.degree = D;
+      best.baby = bm;
+      best.cost = tot;
+      best.a = a;
+      best.ok = have = true;
+    }
+    if (a < 1e-3) break;
+  }
+  return best;
+}
+// Coefficients of the plan's two parts: e_j of sum_j e_j T_j(C) (even) and b_j of
+// Z sum_j b_j T_j(C) (odd): b_jo = 2 o_jo, b_k = 2 o_k - b_{k+1}, b_0 = o_0 - b_1 / 2, with
+// o_k = 2 (-1)^k J_2k+1(a) the coefficient of T_2k+1(Z).
+void cheb_split(double a, int D, std::vector<double>* e, std::vector<double>* b) {
+  const std::vector<double> J = bessel_j(a, std::max(D, 1));
+  int je, jo;
+  cheb_parts(D, &je, &jo);
+  e->assign((size_t)je + 1, 0.0);
+  (*e)[0] = J[0];
+  for (int j = 1; j <= je; ++j) (*e)[j] = 2.0 * ((j & 1) ? -1.0 : 1.0) * J[2 * j];
+  b->clear();
+  if (jo < 0) return;
+  std::vector<double> o((size_t)jo + 1), bb((size_t)jo + 2, 0.0);
+  for (int k = 0; k <= jo; ++k) o[k] = 2.0 * ((k & 1) ? -1.0 : 1.0) * J[2 * k + 1];
+  for (int k = jo; k >= 1; --k) bb[k] = 2.0 * o[k] - bb[k + 1];
+  bb[0] = o[0] - 0.5 * bb[1];
+  b->assign(bb.begin(), bb.begin() + jo + 1);
+}
+// r[g][j] (j < m) with sum_k x_k T_k(C) = sum_g T_g(T_m(C)) sum_j r[g][j] T_j(C): from the top
+// degree down, r[g][j] = 2 x_k and x_{gm-j} -= x_k for g, j >= 1 (T_gm T_j = (T_gm+j + T_gm-j) / 2),
+// else r[g][j] = x_k.
+std::vector<std::array<double, kChebMaxBaby>> cheb_blocks(std::vector<double> x, int m) {
+  const int L = ((int)x.size() - 1) / m;
+  std::vector<std::array<double, kChebMaxBaby>> r((size_t)L + 1);
+  for (auto& row : r) row.fill(0.0);
+  for (int k = (int)x.size() - 1; k >= 0; --k) {
+    const int g = k / m, j = k % m;
+    if (g == 0 || j == 0) {
+      r[g][j] = x[k];
+    } else {
+      r[g][j] = 2.0 * x[k];
+      x[g * m - j] -= x[k];
+    }
+  }
+  return r;
+}
+
+namespace {
+
 // Process-wide weights of the learned selector (device copy; fx_selector_set_weights).
 std::mutex g_sel_mu;
 float* g_sel_weights = nullptr;
@@ -1011,7 +1172,7 @@ class BatchPipeline {
     elems_ = off;
     rows_ = row;
     pitch_ = maxnp_;
-    for (int a = 0; a < kArenas; ++a) arena_[a].alloc(sizeof(double) * (size_t)std::max<int64_t>(elems_, 1));
+    for (int a = 0; a < kBaseArenas; ++a) arena_[a].alloc(sizeof(double) * (size_t)std::max<int64_t>(elems_, 1));
     // int8 slice planes: A re (2 rows per walk row: the two planes of a complex left factor
     // side by side), A im, A -im, B re; 5 slices each.
     a_rows_ = 2 * rows_;
@@ -1030,6 +1191,9 @@ class BatchPipeline {
     ptrs_.alloc(sizeof(void*) * 4 * W);
     sel_m_.assign(W, 13);
     sel_s_.assign(W, 0);
+    cheb_deg_.assign(W, -1);
+    cheb_baby_.assign(W, 1);
+    cheb_rho_.assign(W, 0.0);
     rank1_.assign(W, 0);
     mu_.assign(W, {0, 0});
     nu_.assign(W, {0, 0});
@@ -1141,6 +1305,14 @@ class BatchPipeline {
     solve_mode_ = mode;
     key2_.clear();
   }
+  // Approximant of the walk generators' exponential before the squarings: 0 Pade with its
+  // solve, 1 the Chebyshev-Bessel polynomial (products only) with its own (s, degree) plan.
+  void set_approx(int a) {
+    if (a == approx_) return;
+    approx_ = a;
+    key2_.clear();
+  }
+  int approx() const { return approx_; }
   int form() const { return form_; }
   // Diagnostics: the unitarity residual ||U_k^H U_k - I||_F / sqrt(n) of the iterate after every
   // squaring k = 0..s (k = 0: the Pade result), from two extra 5-slice products per squaring.
@@ -1173,7 +1345,8 @@ class BatchPipeline {
     st->structured = 1;
     st->rank1_shift = rank1_[w];
     st->symmetric = 1;
-    st->solver = uses_newton(w) ? 2 : 1;
+    st->solver = cheb_deg_[w] >= 0 ? 3 : uses_newton(w) ? 2 : 1;
+    st->degree = cheb_deg_[w] >= 0 ? cheb_deg_[w] : 0;
     st->norm1 = norms_[8 * w];
     st->d[0] = std::pow(norms_[8 * w + 1], 0.25);
     st->d[1] = std::pow(norms_[8 * w + 2], 1.0 / 6);
@@ -1343,14 +1516,35 @@ class BatchPipeline {
       if (force_m_ > 0) m = force_m_;
       if (force_s_ >= 0 && m == 13) sq = force_s_;
       if (m != 13 && force_s_ < 0 && outcome_[w] <= 0) sq = 0;
-      if (!pw_m_.empty() && pw_m_[w] > 0) {   // per-walk forced (m, s): measured sweeps
+      const bool pw = !pw_m_.empty() && pw_m_[w] > 0;
+      if (pw) {   // per-walk forced (m, s): measured sweeps
         m = pw_m_[w];
         sq = std::max(0, pw_s_[w]);
         outcome_[w] = 4;
       }
+      const double N3 = (double)walks_[w].n * walks_[w].n * walks_[w].n;
+      cheb_deg_[w] = -1;
+      if (approx_ == 1 && !pw && force_m_ <= 0 && force_s_ < 0) {
+        // the polynomial on the rigorous bound, or (estimated and learned selections) on the
+        // Lanczos estimate with its margin when that is smaller
+        const double rho_c = selector_ >= 2 && rho_lan_[w] > 0.0
+                                 ? std::min(rho_up, rho_lan_[w] * (1.0 + kChebLanMargin))
+                                 : rho_up;
+        const ChebPlan cp = cheb_plan(rho_c, kPhaseTol);
+        if (!cp.ok) throw Error{FX_ERR_VALUE, "walk " + std::to_string(w) + ": no Chebyshev plan for a spectral bound this large"};
+        m = 0;
+        sq = cp.s;
+        cheb_deg_[w] = cp.degree;
+        cheb_baby_[w] = cp.baby;
+        cheb_rho_[w] = rho_c;
+        outcome_[w] = 5;
+        sel_m_[w] = m;
+        sel_s_[w] = sq;
+        flops_ += 2.0 * N3 * (cp.cost - kChebSquareProducts * cp.s) + 8.0 * N3 * sq + 8.0 * N3;
+        continue;
+      }
       sel_m_[w] = m;
       sel_s_[w] = sq;
-      const double N3 = (double)walks_[w].n * walks_[w].n * walks_[w].n;
       flops_ += 8.0 * N3 * (pade_products(m) + sq) + (8.0 / 3.0) * N3 + 8.0 * N3;
     }
     if (analyze_only_) return;
@@ -1437,7 +1631,7 @@ class BatchPipeline {
                              mu_[w].imag(), nu_[w].real(), nu_[w].imag(), tab[W + w] ? 1.0 : 0.0,
                              tab[2 * W + w] ? 1.0 : 0.0, tab[3 * W + w] ? 1.0 : 0.0});
       // the Newton-Schulz solve takes its step count and scaling from these
-      key.insert(key.end(), {rho_up_[w], rho_lan_[w]});
+      key.insert(key.end(), {rho_up_[w], rho_lan_[w], (double)cheb_deg_[w], cheb_rho_[w]});
     }
     if (key != key2_ || profile_) {
       st2_ = Staging();
@@ -1592,7 +1786,10 @@ class BatchPipeline {
   }
 
  private:
-  enum { kY, kA2, kA4, kA6, kT1, kT2, kW, kV, kArenas };
+  // kX1, kX2: the Chebyshev stage's baby steps T_4, T_5 of C, allocated at the first plan that
+  // needs them; the others from the start
+  enum { kY, kA2, kA4, kA6, kT1, kT2, kW, kV, kX1, kX2, kArenas };
+  static constexpr int kBaseArenas = kX1;
   struct Rec {
     std::vector<std::function<void()>> ops;
     int launches = 0, gemms = 0;
@@ -1637,6 +1834,9 @@ class BatchPipeline {
   int pade_S_ = kS;                        // mixed form: slices of the Pade and solve products
   int newton_S_ = kS;                      // mixed form: slices of the early Newton-Schulz steps
   int solve_mode_ = 0;                     // 0 by form and size, 1 Cholesky, 2 Newton-Schulz
+  int approx_ = 0;                         // 0 Pade, 1 Chebyshev-Bessel polynomial
+  std::vector<int> cheb_deg_, cheb_baby_;  // per walk: the polynomial's degree (-1: Pade), m
+  std::vector<double> cheb_rho_;           // per walk: the spectral bound of the polynomial
   int gS_ = kS;                            // slices of the grouped products being recorded
   DevArena lanc_;                          // Lanczos coefficients (W x 2 runs x kLanSteps x 2)
   std::vector<double> lan_host_, rho_lan_, rho_up_;
@@ -2170,7 +2370,27 @@ class BatchPipeline {
     const unsigned nch = (unsigned)ch.size();
     r.launches += 1;
     r.ops.push_back([=]() {
-      kb_combo<<<nch, 256, 0, stream_>>>(D, M, dev<RChunk>(o_ch), (const BWalk*)d_walks_.p, dev<double>(o_c));
+      kb_combo<4><<<nch, 256, 0, stream_>>>(D, M, dev<RChunk>(o_ch), (const BWalk*)d_walks_.p, dev<double>(o_c));
+      FX_LAUNCH_CHECK();
+    });
+  }
+
+  // D = sum_k c_k M_k + g I over five arenas (kb_combo<5>); coef[w] = (c_0..c_4, g).
+  void combo5(Staging& st, Rec& r, const std::vector<int>& list, int d_arena, const int m_arena[5],
+              const std::vector<std::array<double, 6>>& coef) {
+    if (list.empty()) return;
+    std::vector<double> c(6 * count(), 0.0);
+    for (int w : list)
+      for (int k = 0; k < 6; ++k) c[6 * w + k] = coef[w][k];
+    const std::vector<RChunk> ch = row_chunks(list, false);
+    const size_t o_ch = st.put(ch), o_c = st.put(c);
+    PlanesN<5> M{};
+    for (int k = 0; k < 5; ++k) M.m[k] = m_arena[k] >= 0 ? A(m_arena[k]) : nullptr;
+    double* D = A(d_arena);
+    const unsigned nch = (unsigned)ch.size();
+    r.launches += 1;
+    r.ops.push_back([=]() {
+      kb_combo<5><<<nch, 256, 0, stream_>>>(D, M, dev<RChunk>(o_ch), (const BWalk*)d_walks_.p, dev<double>(o_c));
       FX_LAUNCH_CHECK();
     });
   }
@@ -2250,13 +2470,20 @@ class BatchPipeline {
   // Everything after the selection.
   void record_rest(Staging& st, Rec& r) {
     const int W = count();
-    std::vector<int> all, m13, m9, mlt13, rank1;
+    // all: every walk; pd: the walks of the Pade stage and its solve (below it leaves E = R - I
+    // in A4 / A2); cw: the walks of the Chebyshev polynomial stage (which leaves E there too)
+    std::vector<int> all, pd, cw, m13, m9, mlt13, rank1;
     for (int w = 0; w < W; ++w) {
       all.push_back(w);
+      if (rank1_[w]) rank1.push_back(w);
+      if (cheb_deg_[w] >= 0) {
+        cw.push_back(w);
+        continue;
+      }
+      pd.push_back(w);
       if (sel_m_[w] == 13) m13.push_back(w);
       else mlt13.push_back(w);
       if (sel_m_[w] == 9) m9.push_back(w);
-      if (rank1_[w]) rank1.push_back(w);
     }
     // ---- Pade numerator / denominator (powers scaled by 2^-s folded into the coefficients)
     std::vector<std::array<double, 5>> cf(W), cg(W);
@@ -2284,7 +2511,7 @@ class BatchPipeline {
     });
     // odd part: T1 = [T2] + b7 A6 + b5 A4 + b3 A2 + b1 I  (T2 = W1 for m = 13, A8 for m = 9)
     const int m_t2642[4] = {kT2, kA6, kA4, kA2};
-    for (int w = 0; w < W; ++w) {
+    for (int w : pd) {
       const int m = sel_m_[w];
       const auto b = pade_coeffs(m);
       // powers of the scaled generator Y / 2^s: A_k -> 2^(-k s) A_k (s = 0 for the plain
@@ -2296,9 +2523,9 @@ class BatchPipeline {
       else cf[w] = {0.0, 0.0, 0.0, b[3] * cs(w, 2), b[1]};
       al[w] = cs(w, 1);
     }
-    combo(st, r, all, kT1, m_t2642, cf);
+    combo(st, r, pd, kT1, m_t2642, cf);
     // U = i W with W = c Yim T1
-    by_slices(all, ps, [&](const std::vector<int>& l) {
+    by_slices(pd, ps, [&](const std::vector<int>& l) {
       product(st, r, l, kY, kT1, 1.0, -1, 0.0, 0.0, kW, true, &al, nullptr, psplit);
     });
     // even part.  m = 13: T1 = b12 A6 + b10 A4 + b8 A2, T2 = b6 A6 + b4 A4 + b2 A2,
@@ -2328,7 +2555,7 @@ class BatchPipeline {
     // ---- solve: G = V^2 + W^2 = L L^T, P2 = (V + iW)^2, R = G^-1 P2
     // V ~ b_0 I once scaled: these products and the complex ones below split the diagonals off
     tag_ = kTagSolve;
-    by_slices(all, ps, [&](const std::vector<int>& l) {
+    by_slices(pd, ps, [&](const std::vector<int>& l) {
       product(st, r, l, kV, kV, 1.0, -1, 0.0, 0.0, kT1, true, nullptr, nullptr, true);    // VV
       product(st, r, l, kW, kW, 1.0, -1, 0.0, 0.0, kT2, true, nullptr, nullptr, true);    // WW
       product(st, r, l, kV, kW, 1.0, -1, 0.0, 0.0, kA2, true, nullptr, nullptr, true);    // VW
@@ -2336,16 +2563,16 @@ class BatchPipeline {
     const int m_12[4] = {kT1, kT2, -1, -1};
     const int m_a2[4] = {kA2, -1, -1, -1};
     for (int w = 0; w < W; ++w) cf[w] = {1.0, 1.0, 0.0, 0.0, 0.0};
-    combo(st, r, all, kA4, m_12, cf);                             // G -> A4
+    combo(st, r, pd, kA4, m_12, cf);                              // G -> A4
     for (int w = 0; w < W; ++w) cf[w] = {1.0, -1.0, 0.0, 0.0, 0.0};
-    combo(st, r, all, kA6, m_12, cf);                             // P2 re -> A6
+    combo(st, r, pd, kA6, m_12, cf);                              // P2 re -> A6
     for (int w = 0; w < W; ++w) cf[w] = {2.0, 0.0, 0.0, 0.0, 0.0};
-    combo(st, r, all, kY, m_a2, cf);                              // P2 im -> Y
+    combo(st, r, pd, kY, m_a2, cf);                               // P2 im -> Y
     // large walks solve by Newton-Schulz (their Cholesky would be a long chain of dependent
     // block steps); smaller walks, whose few steps run grouped over the batch, keep the
     // Cholesky solve
     std::vector<int> ns_list, ch_list;
-    for (int w = 0; w < W; ++w) (uses_newton(w) ? ns_list : ch_list).push_back(w);
+    for (int w : pd) (uses_newton(w) ? ns_list : ch_list).push_back(w);
     by_slices(ns_list, ps, [&](const std::vector<int>& l) { newton_solve(st, r, l); });   // R re -> A4, im -> A2
     by_slices(ch_list, ps, [&](const std::vector<int>& l) {
       tag_ = kTagCholesky;
@@ -2365,7 +2592,9 @@ class BatchPipeline {
     // ---- squarings in I + E form: E = R - I, E <- 2E + E^2
     for (int w = 0; w < W; ++w) cf[w] = {1.0, 0.0, 0.0, 0.0, -1.0};
     const int m_a4[4] = {kA4, -1, -1, -1};
-    combo(st, r, all, kA4, m_a4, cf);
+    combo(st, r, pd, kA4, m_a4, cf);
+    // the Chebyshev walks: E = p(Z) - I straight into A4 / A2
+    chebyshev(st, r, cw);
     std::vector<int> er(W, kA4), ei(W, kA2), tr(W, kT1), ti(W, kT2);
     project_pair(st, r, rank1, er, ei);
     int smax = 0;
@@ -2648,6 +2877,126 @@ class BatchPipeline {
   // Slice count of walk w's Pade and solve products.
   int pade_slices_of(int w) const { return reduced(w) && sel_s_[w] <= kMixedMaxPadeS ? pade_S_ : kS; }
   // Walk w squares as three split products (square3), else as the exact complex square.
+  // Chebyshev-Bessel polynomial stage of the listed walks (cheb_plan above): E = p(Z) - I with
+  // Z = B / rho, B = Im Y in arena Y, A2 = -B^2 from phase 1.  Real part into A4, imaginary part
+  // into A2, where the Pade walks leave their E.  Arenas: the baby steps T_1..T_5 of C in kBaby
+  // (C = T_1 from A2 by a combination; T_2 = 2 C^2 - I, T_3 = 2 C T_2 - C, T_4 = 2 T_2^2 - I,
+  // T_5 = 2 T_2 T_3 - C); the Clenshaw chains roll b_g over (A4, T1, T2) by g mod 3 with the
+  // C-term r_g - b_{g+2} in A2 (odd chain) or Y (even chain, after the odd one has used B); the
+  // odd chain ends in A4 and Z times it goes to A2, the even chain ends in A4.  The products take
+  // the Pade stage's slice count and diagonal split.
+  static constexpr int kBaby[kChebMaxBaby + 1] = {-1, kA6, kW, kV, kX1, kX2};
+  void chebyshev(Staging& st, Rec& r, const std::vector<int>& cw) {
+    if (cw.empty()) return;
+    const int W = count();
+    tag_ = kTagPade;
+    const bool psplit = form_ == 1 || (split_ & 4);
+    const auto ps = [&](int w) { return pade_slices_of(w); };
+    std::vector<std::vector<std::array<double, kChebMaxBaby>>> re(W), ro(W);
+    std::vector<int> lin, poly, odd0, odd;   // D <= 1; D >= 2; odd cofactor of degree 0; >= 1
+    std::vector<int> top(W, 0);
+    std::vector<double> inv_rho(W, 0.0);
+    int topmax = 0;
+    for (int w : cw) {
+      const int D = cheb_deg_[w], m = cheb_baby_[w];
+      std::vector<double> e, b;
+      cheb_split(std::ldexp(cheb_rho_[w], -sel_s_[w]), D, &e, &b);
+      e[0] -= 1.0;   // E = p - I: the identity term of r_0 (T_0 = I, and T_g(G) r_0 = r_0 at g = 0)
+      inv_rho[w] = cheb_rho_[w] > 0.0 ? 1.0 / cheb_rho_[w] : 0.0;
+      re[w] = cheb_blocks(e, m);
+      if (!b.empty()) ro[w] = cheb_blocks(b, m);
+      top[w] = cheb_baby_top(D, m);
+      topmax = std::max(topmax, top[w]);
+      if (D <= 1) lin.push_back(w);
+      else poly.push_back(w);
+      if (D >= 2) (b.size() == 1 ? odd0 : odd).push_back(w);
+    }
+    for (int k = 4; k <= topmax; ++k)   // the extra baby-step arenas, once
+      if (!arena_[kBaby[k]].p) arena_[kBaby[k]].alloc(sizeof(double) * (size_t)std::max<int64_t>(elems_, 1));
+    std::vector<std::array<double, 6>> cf(W);
+    const int m_none[5] = {-1, -1, -1, -1, -1};
+    const int m_y[5] = {kY, -1, -1, -1, -1};
+    // D <= 1: E = (e_0 - 1) I + i (b_0 / rho) B, no products
+    for (int w : lin) cf[w] = {0.0, 0.0, 0.0, 0.0, 0.0, re[w][0][0]};
+    combo5(st, r, lin, kA4, m_none, cf);
+    for (int w : lin) cf[w] = {ro[w].empty() ? 0.0 : ro[w][0][0] * inv_rho[w], 0.0, 0.0, 0.0, 0.0, 0.0};
+    combo5(st, r, lin, kA2, m_y, cf);
+    if (poly.empty()) return;
+    // baby steps: C = 2 Z^2 - I = -(2 / rho^2) A2 - I, then T_2..T_top by products
+    const int m_a2[5] = {kA2, -1, -1, -1, -1};
+    for (int w : poly) cf[w] = {-2.0 * inv_rho[w] * inv_rho[w], 0.0, 0.0, 0.0, 0.0, -1.0};
+    combo5(st, r, poly, kBaby[1], m_a2, cf);
+    // T_k = 2 T_i T_j - T_|i-j| (i + j = k): (i, j) = (1, 1), (1, 2), (2, 2), (2, 3)
+    static const int kPair[kChebMaxBaby + 1][2] = {{0, 0}, {0, 0}, {1, 1}, {1, 2}, {2, 2}, {2, 3}};
+    for (int k = 2; k <= kChebMaxBaby; ++k) {
+      std::vector<int> l;
+      for (int w : poly)
+        if (top[w] >= k) l.push_back(w);
+      const int i = kPair[k][0], j = kPair[k][1], d = j - i;
+      by_slices(l, ps, [&](const std::vector<int>& ls) {
+        product(st, r, ls, kBaby[i], kBaby[j], 2.0, d > 0 ? kBaby[d] : -1, d > 0 ? -1.0 : 0.0, d > 0 ? 0.0 : -1.0,
+                kBaby[k], true, nullptr, nullptr, psplit);
+      });
+    }
+    // odd cofactor of degree 0: Im E = (b_0 / rho) B
+    for (int w : odd0) cf[w] = {ro[w][0][0] * inv_rho[w], 0.0, 0.0, 0.0, 0.0, 0.0};
+    combo5(st, r, odd0, kA2, m_y, cf);
+    // odd chain -> A4, then Im E = (1 / rho) B (chain) -> A2
+    clenshaw(st, r, odd, ro, kA2);
+    std::vector<double> al(W, 1.0);
+    for (int w : odd) al[w] = inv_rho[w];
+    by_slices(odd, ps, [&](const std::vector<int>& l) {
+      product(st, r, l, kY, kA4, 1.0, -1, 0.0, 0.0, kA2, true, &al, nullptr, psplit);
+    });
+    // even chain (with -I in r_0) -> A4 = Re E
+    clenshaw(st, r, poly, re, kY);
+  }
+  // Clenshaw's recurrence in G = T_m(C) over the listed walks' blocks r[w][g][j]:
+  // b_L = r_L; b_g = 2 G b_{g+1} - b_{g+2} + r_g (g = L-1 .. 1); result G b_1 - b_2 + r_0 (or r_0
+  // when L = 0), which ends in A4.  b_g lives in the arena kRoll[g mod 3], so that a step never
+  // writes an arena it reads; `tmp` holds the C-term r_g - b_{g+2} of each step's product.
+  void clenshaw(Staging& st, Rec& r, const std::vector<int>& list,
+                const std::vector<std::vector<std::array<double, kChebMaxBaby>>>& blk, int tmp) {
+    if (list.empty()) return;
+    static const int kRoll[3] = {kA4, kT1, kT2};
+    const int W = count();
+    const auto ps = [&](int w) { return pade_slices_of(w); };
+    const bool psplit = form_ == 1 || (split_ & 4);
+    int Lmax = 0;
+    for (int w : list) Lmax = std::max(Lmax, (int)blk[w].size() - 1);
+    std::vector<std::array<double, 6>> cf(W);
+    // r_g = sum_{j < m} r[g][j] T_j(C): planes T_1..T_4 (T_0 = I on the diagonal)
+    const auto rg = [&](int w, int g, double last) {
+      const auto& x = blk[w][g];
+      return std::array<double, 6>{x[1], x[2], x[3], x[4], last, x[0]};
+    };
+    for (int g = Lmax; g >= 0; --g) {
+      std::vector<int> start, step;
+      for (int w : list) {
+        const int L = (int)blk[w].size() - 1;
+        if (L == g) start.push_back(w);
+        else if (L > g) step.push_back(w);
+      }
+      // walks whose chain starts here: b_L = r_L
+      const int m_t[5] = {kBaby[1], kBaby[2], kBaby[3], kBaby[4], -1};
+      for (int w : start) cf[w] = rg(w, g, 0.0);
+      combo5(st, r, start, kRoll[g % 3], m_t, cf);
+      if (step.empty()) continue;
+      // C-term r_g - b_{g+2} (b_{g+2} = 0 above the chain's top), then b_g = alpha G b_{g+1} + C-term
+      const int m_c[5] = {kBaby[1], kBaby[2], kBaby[3], kBaby[4], kRoll[(g + 2) % 3]};
+      for (int w : step) cf[w] = rg(w, g, g + 2 <= (int)blk[w].size() - 1 ? -1.0 : 0.0);
+      combo5(st, r, step, tmp, m_c, cf);
+      for (int m = 1; m <= kChebMaxBaby; ++m) {
+        std::vector<int> l;
+        for (int w : step)
+          if (cheb_baby_[w] == m) l.push_back(w);
+        by_slices(l, ps, [&](const std::vector<int>& ls) {
+          product(st, r, ls, kBaby[m], kRoll[(g + 1) % 3], g >= 1 ? 2.0 : 1.0, tmp, 1.0, 0.0, kRoll[g % 3], true,
+                  nullptr, nullptr, psplit);
+        });
+      }
+    }
+  }
   bool use_square3(int w) const {
     return walks_[w].np >= kSquare3MinNp || sel_s_[w] >= kSquare3MinS || (split_ & 8);
   }
@@ -2986,6 +3335,7 @@ void batch_pipeline_run(BatchPipeline* p, const void* dX, const void* dpsi0, voi
   p->set_inject_stall(o.inject_stall);
   p->set_form(o.form == FX_FORM_MIXED ? 1 : 0, o.sq_n4, o.sq_n3, o.pade_slices, o.newton_slices);
   p->set_solve(o.solve);
+  p->set_approx(o.approx);
   p->set_drift(o.drift);
   p->run(x, p0, p1, u, s);
 }
@@ -3185,6 +3535,11 @@ int fx_batch_set_option(fx_batch_handle b, int key, double value) {
       b->p->set_form(b->p->form(), b->sq_n4, b->sq_n3, b->pade_slices, b->newton_slices);
       return FX_OK;
     case FX_BATCH_OPT_DRIFT: b->p->set_drift(value != 0.0); return FX_OK;
+    case FX_BATCH_OPT_APPROX:
+      if (value != 0 && value != 1)
+        return bfail(b, fx::Error{FX_ERR_VALUE, "approximant must be 0 (Pade) or 1 (Chebyshev)"});
+      b->p->set_approx((int)value);
+      return FX_OK;
   }
   return bfail(b, fx::Error{FX_ERR_VALUE, "unknown batch option"});
 }
@@ -3262,6 +3617,19 @@ int fx_batch_drift(fx_batch_handle b, int64_t w, double* out, int32_t cap, int32
   const std::vector<double> v = b->p->drift_curve((int)w);
   for (int32_t i = 0; i < cap && i < (int32_t)v.size(); ++i) out[i] = v[i];
   *count = (int32_t)v.size();
+  return FX_OK;
+}
+
+int fx_chebyshev_plan(double rho, double tol, int32_t* s, int32_t* degree, int32_t* baby, int32_t* cost) {
+  if (!s || !degree || !baby || !cost) return bfail(nullptr, fx::Error{FX_ERR_VALUE, "null argument"});
+  if (!(rho >= 0.0) || !std::isfinite(rho) || !(tol > 0.0))
+    return bfail(nullptr, fx::Error{FX_ERR_VALUE, "the plan needs a finite rho >= 0 and tol > 0"});
+  const fx::ChebPlan p = fx::cheb_plan(rho, tol);
+  if (!p.ok) return bfail(nullptr, fx::Error{FX_ERR_VALUE, "no plan: rho / 2^60 is above 1024"});
+  *s = p.s;
+  *degree = p.degree;
+  *baby = p.baby;
+  *cost = p.cost;
   return FX_OK;
 }
 

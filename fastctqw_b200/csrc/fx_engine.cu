@@ -94,6 +94,7 @@ struct RunOpts {
   int newton_slices; // mixed form of the grouped path: slices of the early Newton-Schulz steps
   int solve;         // grouped path: Pade solve, 0 by form and size, 1 Cholesky, 2 Newton-Schulz
   int drift;         // diagnostics of the grouped path: unitarity residual after every squaring
+  int approx;        // grouped path: 0 Pade, 1 Chebyshev-Bessel polynomial
 };
 
 // Planar complex matrix view over owned storage; a missing plane is identically zero.
@@ -1048,7 +1049,7 @@ struct fx_engine {
   void* check_buf = nullptr;              // input statistics of the routing check
   fx::HostStage stage;                    // page-locked chunks for copies of host buffers
   fx::RunOpts opts{FX_FORM_PLAIN, 2, 1, -1, -1, 2000, 1, 0, 0, 0, -1, fx::kMixedN4, fx::kMixedN3, fx::kMixedPade,
-                      fx::kMixedNewton, 0, 0};
+                      fx::kMixedNewton, 0, 0, 0};
   fx_stats stats{};
   std::string last_error;
 };
@@ -1143,6 +1144,7 @@ void run_device(fx_handle h, const void* dA, void* dU, const void* dpsi0, void* 
     po.pade_slices = h->opts.pade_slices;
     po.newton_slices = h->opts.newton_slices;
     po.solve = h->opts.solve;
+    po.approx = h->opts.approx;
     po.drift = h->opts.drift != 0;
     fx::batch_pipeline_run(h->grouped, dA, dpsi0, dpsi, dU, po, s);
     FX_CUDA(cudaEventRecord(h->ev1, s));
@@ -1317,6 +1319,10 @@ int fx_set_option(fx_handle h, int key, double value) {
     case FX_OPT_NEWTON_SLICES:
       if (v != 3 && v != 4 && v != 5) return fail(h, fx::Error{FX_ERR_VALUE, "Newton slice count must be 3, 4 or 5"});
       h->opts.newton_slices = v;
+      return FX_OK;
+    case FX_OPT_APPROX:
+      if (v != 0 && v != 1) return fail(h, fx::Error{FX_ERR_VALUE, "approximant must be 0 (Pade) or 1 (Chebyshev)"});
+      h->opts.approx = v;
       return FX_OK;
   }
   return fail(h, fx::Error{FX_ERR_VALUE, "unknown option"});

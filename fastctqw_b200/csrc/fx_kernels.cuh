@@ -260,6 +260,7 @@ struct PipeOpts {
                              // above 1e-3 (the later ones take pade_slices)
   int solve = 0;             // Pade solve: 0 by form and size, 1 Cholesky, 2 Newton-Schulz
   bool drift = false;        // diagnostics: unitarity residual after every squaring
+  int approx = 0;            // 0 Pade, 1 Chebyshev-Bessel polynomial (walk generators)
 };
 // Default slice schedule of the mixed form (see fx_batch.cu, BatchPipeline::sq_slices and
 // BatchPipeline::newton_solve).

@@ -124,9 +124,20 @@ enum fx_option {
                              the solve whose model residual stays above 1e-4 (3 default,
                              4 or 5; the later steps take the Pade products' count: the
                              iteration corrects the early steps' rounding)             */
-  FX_OPT_SOLVE = 17       /* walk generators: solve of the Pade step R = G^-1 P^2 (G SPD):
+  FX_OPT_SOLVE = 17,      /* walk generators: solve of the Pade step R = G^-1 P^2 (G SPD):
                              0 (default) Newton-Schulz for walks padded to 4096 or more,
                              blocked Cholesky otherwise; 1 Cholesky; 2 Newton-Schulz  */
+  FX_OPT_APPROX = 18      /* walk generators X = iB: approximant of exp(X / 2^s) before the
+                             squarings.  0 (default) the [m/m] Pade approximant and its
+                             solve; 1 the Chebyshev-Bessel polynomial sum_k (2 - [k=0])
+                             i^k J_k(a) T_k(B / rho), a = rho / 2^s, evaluated with
+                             products of commuting real symmetric matrices only (no
+                             solve); rho is the rigorous spectral bound min(||Y||_1, d4,
+                             d6), or for the estimated and learned selections
+                             min(that, 1.25 x the Lanczos estimate); (s, degree) are the
+                             cheapest plan of fx_chebyshev_plan at error 1e-6.  Reported
+                             as m = 0, solver 3, fx_stats.degree, sel_outcome 5.  No
+                             counterpart in the reference                             */
 };
 
 /* What the last run did. */
@@ -140,8 +151,8 @@ typedef struct fx_stats {
   int32_t gemm_launches;/* matrix-product kernel launches in the run     */
   int32_t launches;     /* all kernel launches of the run                */
   int32_t solver;       /* 0 pivoted LU, 1 Cholesky of Q^H Q (normal Q), 2 Newton-Schulz
-                           inverse of Q^H Q                                            */
-  int32_t reserved;
+                           inverse of Q^H Q, 3 none (Chebyshev polynomial, FX_OPT_APPROX) */
+  int32_t degree;       /* degree of the Chebyshev polynomial (FX_OPT_APPROX = 1), else 0  */
   double norm1;         /* ||X - shifts||_1                              */
   double d[5];          /* d4, d6, d8, d10, log2 ||(|A|)^27||_1          */
   double ms_total;      /* device time of the last run (CUDA events)     */
@@ -288,7 +299,9 @@ enum fx_batch_option {
                                  /* FX_OPT_PADE_SLICES)                                         */
   FX_BATCH_OPT_NEWTON_SLICES = 15, /* mixed form: slices of the early Newton-Schulz steps (as    */
                                   /* FX_OPT_NEWTON_SLICES)                                      */
-  FX_BATCH_OPT_SOLVE = 16         /* solve of the Pade step (as FX_OPT_SOLVE)                   */
+  FX_BATCH_OPT_SOLVE = 16,        /* solve of the Pade step (as FX_OPT_SOLVE)                   */
+  FX_BATCH_OPT_APPROX = 17        /* approximant: 0 Pade, 1 Chebyshev polynomial (as           */
+                                  /* FX_OPT_APPROX)                                             */
 };
 /* count walks of sizes n[0..count); dtype FX_C64 or FX_C128 (of X, psi0 and psi). */
 int fx_batch_create(size_t count, const int64_t* n, int dtype, fx_batch_handle* out);
@@ -311,7 +324,14 @@ int fx_batch_force_selection(fx_batch_handle b, const int32_t* m, const int32_t*
 /* Per walk of the last run (arrays of `count`): the Lanczos spectral-radius estimate and the
  * rigorous bound (as fx_spectral_radius). */
 int fx_batch_spectral(fx_batch_handle b, double* rho_lanczos, double* rho_up);
-/* (m, s) chosen for every walk by the last run (arrays of `count`). */
+/* The plan of the Chebyshev approximant (FX_OPT_APPROX = 1) for a spectral bound rho >= 0 of B
+ * and an error bound tol > 0 after the squarings: the number of squarings s, the degree D of
+ * the polynomial in B / rho (its truncation error 2 sum_{k>D} |J_k(rho / 2^s)| <= tol / 2^s),
+ * the baby steps m (T_1..T_m of C = 2 (B / rho)^2 - I) and the matrix products of the whole
+ * walk (3 per squaring), the cheapest such plan; host arithmetic only, no device needed.  No
+ * counterpart in the reference. */
+int fx_chebyshev_plan(double rho, double tol, int32_t* s, int32_t* degree, int32_t* baby, int32_t* cost);
+/* (m, s) chosen for every walk by the last run (arrays of `count`; m = 0: Chebyshev). */
 int fx_batch_selection(fx_batch_handle b, int32_t* m, int32_t* s);
 /* Device time (ms, CUDA events), algorithmic flops and kernel launches of the last run. */
 int fx_batch_info(fx_batch_handle b, double* ms, double* flops, int32_t* launches);
