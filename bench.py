@@ -247,7 +247,8 @@ def accuracy_vs_eigh(H: np.ndarray, t: float, dU, psi_e0, psi_e0_plain, dev, see
 def bench_stress(args, dev) -> dict:
     """The large-norm stress workload: dense symmetric weighted graph, N = 16384, weights uniform
     in [0, 1) from a fixed seed (zero diagonal), H = weighted Laplacian D - W, t = 100, X = -1j H t
-    (FastCTQW/Operator.py:49-56).  Runs complex64 in the plain and mixed forms and complex128
+    (FastCTQW/Operator.py:49-56).  Runs complex64 in the plain and mixed forms (the mixed form
+    with the Pade and with the Chebyshev approximant) and complex128
     (int8 slices on FP64 masters), each timed with CUDA events, with the unitarity residual
     ||U_k^H U_k - I||_F / sqrt(N) after every squaring k (FX_OPT_DRIFT) and the final accuracy
     against the FP64 eigendecomposition of the same generator (the complex64 input is itself a
@@ -264,7 +265,8 @@ def bench_stress(args, dev) -> dict:
            "oracle": "FP64 eigendecomposition of the (rounded) generator on the device"}
     stream = torch.cuda.current_stream(dev)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    for dt, forms in ((np.complex64, ("plain", "mixed")), (np.complex128, ("plain",))):
+    for dt, forms in ((np.complex64, (("plain", "pade"), ("mixed", "pade"), ("mixed", "chebyshev"))),
+                      (np.complex128, (("plain", "pade"),))):
         X = np.asarray(-1j * (-1.0 * L) * t, dtype=dt)
         lam, V = torch.linalg.eigh(torch.from_numpy(np.ascontiguousarray(X.imag, dtype=np.float64)).to(dev))
         Vc = V.to(torch.complex128)
@@ -279,8 +281,8 @@ def bench_stress(args, dev) -> dict:
         dp = torch.empty_like(p0)
         dU = torch.empty_like(dX)
         eng = Engine(n, dt)
-        for form in forms:
-            eng.configure(form=form, drift=False)
+        for form, approx in forms:
+            eng.configure(form=form, approx=approx, drift=False)
             eng.walk_device(dX, p0, dp, dU, stream)
             torch.cuda.synchronize()
             ev[0].record(stream)
@@ -288,7 +290,7 @@ def bench_stress(args, dev) -> dict:
             ev[1].record(stream)
             torch.cuda.synchronize()
             st = eng.stats()
-            rec = {"ms": round(ev[0].elapsed_time(ev[1]), 2), "m": st["m"], "s": st["s"]}
+            rec = {"ms": round(ev[0].elapsed_time(ev[1]), 2), "m": st["m"], "s": st["s"], "degree": st["degree"]}
             U = dU.to(torch.complex128)
             rec["u_rel_error"] = float(torch.linalg.matrix_norm(U - Uref) / torch.linalg.matrix_norm(Uref))
             rec["infidelity_e0"] = eo.infidelity(dp.cpu().numpy(), Uref[:, 0].cpu().numpy())
@@ -305,7 +307,7 @@ def bench_stress(args, dev) -> dict:
             torch.cuda.synchronize()
             rec["drift_per_squaring"] = [float("%.4g" % x) for x in eng.unitarity_drift()]
             eng.configure(drift=False)
-            out[f"{np.dtype(dt).name}_{form}"] = rec
+            out[f"{np.dtype(dt).name}_{form}" + ("_chebyshev" if approx == "chebyshev" else "")] = rec
         eng.close()
         del dX, dU, Uref
         torch.cuda.empty_cache()
@@ -542,9 +544,9 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--form", default="mixed", choices=["plain", "mixed", "simt"],
                     help="precision form of the timed walk; the plain form is timed beside it")
-    ap.add_argument("--selector", default="learned", choices=["plain", "certified", "estimated", "learned"],
+    ap.add_argument("--selector", default="estimated", choices=["plain", "certified", "estimated", "learned"],
                     help="(m, s) selection of the timed walk; the plain selection is timed beside it")
-    ap.add_argument("--approx", default="pade", choices=["pade", "chebyshev"],
+    ap.add_argument("--approx", default="chebyshev", choices=["pade", "chebyshev"],
                     help="approximant of the timed walk before its squarings (Pade + solve, or the "
                          "Chebyshev-Bessel polynomial); the plain form beside it is Pade")
     ap.add_argument("--ref-sample-n", type=int, default=1024,
