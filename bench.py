@@ -34,11 +34,11 @@ METRIC = "expm(-iHt) ms at N=10k c64; batched walks/s; chosen vs plain @ infid<=
 
 
 def product_traffic_per_launch(form: str):
-    """DRAM bytes (read + write) per k_gemm_i8 launch of the benchmark walk in the given form, from
-    the committed summary of an ncu capture of one walk's product launches
-    (dram__bytes_read.sum + dram__bytes_write.sum, averaged over the walk's launches): the line
-    `dram_bytes_per_launch[<form>]: <bytes>` of profiles/k_gemm_i8_walk_traffic.md.  None when
-    the summary has no line for the form."""
+    """DRAM bytes (read + write) per k_gemm_i8 launch of the benchmark walk in the given form
+    ("mixed/chebyshev", "mixed", ...), from the committed summary of an ncu capture of one walk's
+    product launches (dram__bytes_read.sum + dram__bytes_write.sum, averaged over the walk's
+    launches): the line `dram_bytes_per_launch[<form>]: <bytes>` of
+    profiles/k_gemm_i8_walk_traffic.md.  None when the summary has no line for the form."""
     import re
     path = os.path.join(REPO, "profiles", "k_gemm_i8_walk_traffic.md")
     try:
@@ -665,7 +665,7 @@ def main():
     bf = _native.tensor_peak("bf16")
     int8_peak = i8["tops"]
     achieved = pst["prod_ops"] / (pst["prod_ms"] * 1e-3) / 1e12 if pst["prod_ms"] > 0 else None
-    traffic = product_traffic_per_launch(args.form)
+    traffic = product_traffic_per_launch(args.form + ("/chebyshev" if args.approx == "chebyshev" else ""))
     roofline = {
         "bound": "tensor",
         "kernel": ("k_gemm_i8<4,double> (int8 Ozaki-slice products, exact accumulation; 4 slices)"

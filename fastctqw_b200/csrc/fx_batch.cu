@@ -240,25 +240,39 @@ __global__ void kb_walk_reduce(const int* list, const BWalk* wk, const double* r
     dev = fmax(dev, fmax(fabs(r[kRS * i] - c0r), fabs(r[kRS * i + 1] - c0i)));
     nz = fmax(nz, r[kRS * i + 6]);
   }
+  // the trace and ||X||_F^2: per-thread sums over rows i = t mod blockDim in order, then a fixed
+  // tree (the same association every run)
+  __shared__ double s_tr[256];
+  __shared__ double s_ti[256];
+  __shared__ double s_fr[256];
+  double tr = 0, ti = 0, fro2 = 0;
+  for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
+    tr += r[kRS * i + 2];
+    ti += r[kRS * i + 3];
+    fro2 += r[kRS * i + 5];
+  }
   s_max[threadIdx.x] = mx;
   s_dev[threadIdx.x] = dev;
   s_nz[threadIdx.x] = nz;
+  s_tr[threadIdx.x] = tr;
+  s_ti[threadIdx.x] = ti;
+  s_fr[threadIdx.x] = fro2;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
     if (threadIdx.x < o) {
       s_max[threadIdx.x] = fmax(s_max[threadIdx.x], s_max[threadIdx.x + o]);
       s_dev[threadIdx.x] = fmax(s_dev[threadIdx.x], s_dev[threadIdx.x + o]);
       s_nz[threadIdx.x] = fmax(s_nz[threadIdx.x], s_nz[threadIdx.x + o]);
+      s_tr[threadIdx.x] += s_tr[threadIdx.x + o];
+      s_ti[threadIdx.x] += s_ti[threadIdx.x + o];
+      s_fr[threadIdx.x] += s_fr[threadIdx.x + o];
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    double tr = 0, ti = 0, fro2 = 0;
-    for (int i = 0; i < b.n; ++i) {
-      tr += r[kRS * i + 2];
-      ti += r[kRS * i + 3];
-      fro2 += r[kRS * i + 5];
-    }
+    tr = s_tr[0];
+    ti = s_ti[0];
+    fro2 = s_fr[0];
     const double n = b.n;
     const double mur = tr / n, mui = ti / n;
     const bool rank1 = b.n > 1 && s_dev[0] <= 4.0 * n * 0x1p-53 * s_max[0];
@@ -282,7 +296,8 @@ __global__ void kb_walk_reduce(const int* list, const BWalk* wk, const double* r
 // shifted generator; its real plane is zero for X = i*(real symmetric)).  sh[kWO w + 5, 6] =
 // (mu_im, nu_im/n) as written by kb_walk_reduce.
 template <typename C>
-__global__ void kb_load_imag(const void* const* X, const int* list, const BWalk* wk, const double* sh, double* Y) {
+__global__ void kb_load_imag(const void* const* X, const int* list, const BWalk* wk, const double* sh, double* Y,
+                             float* Y32) {
   const int w = list[blockIdx.y];
   const BWalk b = wk[w];
   const C* x = (const C*)X[w];
@@ -294,6 +309,7 @@ __global__ void kb_load_imag(const void* const* X, const int* list, const BWalk*
     double v = 0.0;
     if (i < b.n && j < b.n) v = (double)x[i * b.n + j].y - (i == j ? mu : 0.0) - nun;
     Y[b.off + idx] = v;
+    if (Y32) Y32[b.off + idx] = (float)v;
   }
 }
 
@@ -475,13 +491,36 @@ __global__ void kb_apply(const double* const* Ere, const double* const* Eim, con
   const double* ei = Eim[w] + b.off;
   const int lane = threadIdx.x & 31, wpb = blockDim.x / 32;
   const double* o = om + 4 * w;
+  // pairs of columns per lane: 16-byte loads of E's FP64 planes (rows start 16-byte aligned,
+  // np even) and of two psi0 entries when psi0 allows it; column n of a row is padding (zero off
+  // the diagonal block) and its psi0 entry is taken as 0
+  const bool vec = sizeof(C) == 8 && (reinterpret_cast<uintptr_t>(p0) & 15) == 0;
   for (int64_t i = (int64_t)blockIdx.x * wpb + threadIdx.x / 32; i < b.n; i += (int64_t)gridDim.x * wpb) {
     double yr = 0, yi = 0;
-    for (int64_t j = lane; j < b.n; j += 32) {
-      const double a = er[i * b.np + j], c = ei[i * b.np + j];
-      const double x = (double)p0[j].x, y = (double)p0[j].y;
-      yr += a * x - c * y;
-      yi += a * y + c * x;
+    const double2* ra = reinterpret_cast<const double2*>(er + i * b.np);
+    const double2* rc = reinterpret_cast<const double2*>(ei + i * b.np);
+#pragma unroll 4
+    for (int64_t j = 2 * lane; j < b.n; j += 64) {
+      const double2 a = ra[j >> 1], c = rc[j >> 1];
+      double x0, y0, x1 = 0.0, y1 = 0.0;
+      if (vec && j + 1 < b.n) {
+        const float4 q = *reinterpret_cast<const float4*>(p0 + j);
+        x0 = q.x;
+        y0 = q.y;
+        x1 = q.z;
+        y1 = q.w;
+      } else {
+        x0 = (double)p0[j].x;
+        y0 = (double)p0[j].y;
+        if (j + 1 < b.n) {
+          x1 = (double)p0[j + 1].x;
+          y1 = (double)p0[j + 1].y;
+        }
+      }
+      yr += a.x * x0 - c.x * y0;
+      yi += a.x * y0 + c.x * x0;
+      yr += a.y * x1 - c.y * y1;
+      yi += a.y * y1 + c.y * x1;
     }
 #pragma unroll
     for (int k = 16; k > 0; k >>= 1) {
@@ -536,16 +575,30 @@ __global__ void kb_psi_norms(const void* const* psi0, void* const* psi, const in
 template <typename C>
 __global__ void kb_psi_sum(const void* const* psi0, const int* list, const BWalk* wk, double* psum) {
   const int w = list[blockIdx.x];
-  if (threadIdx.x != 0) return;
   const C* p = (const C*)psi0[w];
   if (!p) return;
+  // per-thread sums over j = t mod blockDim in order, then a fixed tree (blockDim = 256)
+  __shared__ double s_r[256];
+  __shared__ double s_i[256];
   double sr = 0, si = 0;
-  for (int j = 0; j < wk[w].n; ++j) {
+  for (int j = threadIdx.x; j < wk[w].n; j += blockDim.x) {
     sr += (double)p[j].x;
     si += (double)p[j].y;
   }
-  psum[2 * w] = sr;
-  psum[2 * w + 1] = si;
+  s_r[threadIdx.x] = sr;
+  s_i[threadIdx.x] = si;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s_r[threadIdx.x] += s_r[threadIdx.x + o];
+      s_i[threadIdx.x] += s_i[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    psum[2 * w] = s_r[0];
+    psum[2 * w + 1] = s_i[0];
+  }
 }
 
 // ------------------------------------------------------------------ block 1-norm estimator
@@ -623,6 +676,52 @@ __global__ void kb_est_matvec(const double* M, const RChunk* ch, const BWalk* wk
     }
   }
 }
+// The same pair of mat-vecs from an FP32 copy of M (the Lanczos steps: half the bytes of the
+// FP64 plane; the rounding moves the spectrum by ~1e-7 of its radius, far inside the margins
+// the estimate is used with).  16-byte loads of four values, FP64 accumulation.
+__global__ void kb_est_matvec32(const float* M, const RChunk* ch, const BWalk* wk, double* scr, const double* est,
+                                int in0, int out0) {
+  const RChunk q = ch[blockIdx.x];
+  const int w = q.w;
+  if (est[4 * w + 2] != 0.0) return;
+  const BWalk b = wk[w];
+  const double* x0 = est_vec(scr, b, in0);
+  const double* x1 = est_vec(scr, b, in0 + 1);
+  double* y0 = est_vec(scr, b, out0);
+  double* y1 = est_vec(scr, b, out0 + 1);
+  const float* A = M + b.off;
+  const int lane = threadIdx.x & 31, wpb = blockDim.x / 32;
+  const int64_t h = b.np / 4;   // np is a multiple of 128: rows start 16-byte aligned
+  const double2* u0 = reinterpret_cast<const double2*>(x0);
+  const double2* u1 = reinterpret_cast<const double2*>(x1);
+  for (int64_t i = q.r0 + threadIdx.x / 32; i < q.r1; i += wpb) {
+    const float4* row = reinterpret_cast<const float4*>(A + i * b.np);
+    double a = 0, c = 0;
+#pragma unroll 2
+    for (int64_t j = lane; j < h; j += 32) {
+      const float4 m = row[j];
+      const double2 p0 = u0[2 * j], p1 = u0[2 * j + 1], r0 = u1[2 * j], r1 = u1[2 * j + 1];
+      a += (double)m.x * p0.x;
+      a += (double)m.y * p0.y;
+      a += (double)m.z * p1.x;
+      a += (double)m.w * p1.y;
+      c += (double)m.x * r0.x;
+      c += (double)m.y * r0.y;
+      c += (double)m.z * r1.x;
+      c += (double)m.w * r1.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0) {
+      y0[i] = a;
+      y1[i] = c;
+    }
+  }
+}
+
 // ---- Lanczos estimate of the spectral radius of every walk's real symmetric generator B
 // (the imaginary plane of the shifted Y): two independent runs of kLanSteps steps from
 // pseudo-random sign vectors, sharing kb_est_matvec (X0, X1 -> T0, T1), without
@@ -1119,7 +1218,7 @@ struct DevArena {
   void alloc(size_t b) {
     release();
     if (b == 0) return;
-    if (cudaMalloc(&p, b) != cudaSuccess) {
+    if (inject_alloc_failure() || cudaMalloc(&p, b) != cudaSuccess) {
       p = nullptr;
       cudaGetLastError();
       throw Error{FX_ERR_NOMEM, "device allocation of " + std::to_string(b) + " bytes failed"};
@@ -1232,7 +1331,20 @@ class BatchPipeline {
   }
   bool needs_lanczos() const { return selector_ >= 2 || form_ == 1 || analyze_only_; }
   bool needs_estimates() const { return selector_ <= 1 || analyze_only_; }
-  int phase1_needs() const { return (needs_lanczos() ? 1 : 0) | (needs_estimates() ? 2 : 0); }
+  // A^4 and A^6 are products of phase 1 for the exact norms d4, d6 (the Al-Mohy & Higham
+  // selection, the rigorous spectral bound, the Pade stage's operands).  When every walk takes
+  // the Chebyshev polynomial on the Lanczos bound (estimated or learned selection, nothing
+  // forced), they serve only as the cap min(||Y||_1, d4, d6) of that bound, and phase 1 computes
+  // A2 alone: the cap is then min(||Y||_1, ||A2||_1^(1/2)) (||A^4|| <= ||A2||^2 and
+  // ||A^6|| <= ||A2||^3 stand in for the exact norms), still a rigorous bound.
+  bool needs_powers46() const {
+    bool forced = force_m_ > 0 || force_s_ >= 0;
+    for (int m : pw_m_) forced = forced || m > 0;
+    return !(approx_ == 1 && selector_ >= 2 && !analyze_only_ && !forced);
+  }
+  int phase1_needs() const {
+    return (needs_lanczos() ? 1 : 0) | (needs_estimates() ? 2 : 0) | (needs_powers46() ? 4 : 0);
+  }
   void rerecord_phase1() {
     if (graph1_) cudaGraphExecDestroy(graph1_);
     graph1_ = nullptr;
@@ -1309,8 +1421,10 @@ class BatchPipeline {
   // solve, 1 the Chebyshev-Bessel polynomial (products only) with its own (s, degree) plan.
   void set_approx(int a) {
     if (a == approx_) return;
+    const int before = phase1_needs();
     approx_ = a;
     key2_.clear();
+    if (phase1_needs() != before) rerecord_phase1();
   }
   int approx() const { return approx_; }
   int form() const { return form_; }
@@ -1403,6 +1517,11 @@ class BatchPipeline {
     for (int w = 0; w < W && lan; ++w) {
       const double* base = lan_host_.data() + (size_t)w * 4 * kLanSteps;
       rho_lan_[w] = std::max(tridiag_radius(base, kLanSteps), tridiag_radius(base + 2 * kLanSteps, kLanSteps));
+    }
+    for (int w = 0; w < W && !p46_recorded_; ++w) {   // bounds in place of ||A^4||, ||A^6||
+      double* nw = norms_.data() + 8 * w;
+      nw[1] = nw[5] * nw[5];
+      nw[2] = nw[5] * nw[5] * nw[5];
     }
     for (int w = 0; w < W && !est_recorded_; ++w) {   // bounds in place of the estimates
       double* nw = norms_.data() + 8 * w;
@@ -1813,6 +1932,7 @@ class BatchPipeline {
   std::vector<cudaEvent_t> phase_ev_;   // profile mode: the run's timeline events
   bool lan_recorded_ = false;   // phase 1 as recorded runs the Lanczos estimate
   bool est_recorded_ = true;    // phase 1 as recorded runs the 1-norm estimates of A^8, A^10
+  bool p46_recorded_ = true;    // phase 1 as recorded computes A^4 and A^6
   bool analyze_only_ = false;
   int split_ = 7;
   int tile_group_ = 8, tile_order_ = 0;   // phase-2 schedule of the grouped products
@@ -1835,6 +1955,7 @@ class BatchPipeline {
   int newton_S_ = kS;                      // mixed form: slices of the early Newton-Schulz steps
   int solve_mode_ = 0;                     // 0 by form and size, 1 Cholesky, 2 Newton-Schulz
   int approx_ = 0;                         // 0 Pade, 1 Chebyshev-Bessel polynomial
+  bool nvtx_open_ = false;                 // a phase's NVTX range is open
   std::vector<int> cheb_deg_, cheb_baby_;  // per walk: the polynomial's degree (-1: Pade), m
   std::vector<double> cheb_rho_;           // per walk: the spectral bound of the polynomial
   int gS_ = kS;                            // slices of the grouped products being recorded
@@ -1866,19 +1987,23 @@ class BatchPipeline {
 
  public:
   void force(int m, int s) {
+    const int before = phase1_needs();
     force_m_ = m;
     force_s_ = s;
+    if (phase1_needs() != before) rerecord_phase1();
   }
   // Per-walk (m, s) for the next runs (m <= 0: that walk's own selection); empty clears.
   void force_each(const int* m, const int* s) {
     const int W = count();
+    const int before = phase1_needs();
     if (!m) {
       pw_m_.clear();
       pw_s_.clear();
-      return;
+    } else {
+      pw_m_.assign(m, m + W);
+      pw_s_.assign(s, s + W);
     }
-    pw_m_.assign(m, m + W);
-    pw_s_.assign(s, s + W);
+    if (phase1_needs() != before) rerecord_phase1();
   }
 
  private:
@@ -1950,7 +2075,16 @@ class BatchPipeline {
 
   // Profile mode: event k of the run's timeline (0 start, 1 after phase 1, 2 before phase 2,
   // 3 after phase 2, 4 end).
+  // Phase boundaries of a run: an NVTX range per phase (phase 1, selection and recording,
+  // phase 2, the a-posteriori checks) and, in profile mode, a CUDA event at each boundary.
   void phase_mark(int k) {
+    static const char* kNames[4] = {"fx batch: phase 1 (statistics, powers, norms, Lanczos)",
+                                    "fx batch: selection and phase-2 recording",
+                                    "fx batch: phase 2 (approximant, squarings, outputs)",
+                                    "fx batch: a-posteriori checks"};
+    if (nvtx_open_) nvtxRangePop();
+    nvtx_open_ = k < 4;
+    if (nvtx_open_) nvtxRangePushA(kNames[k]);
     if (!profile_) return;
     while ((int)phase_ev_.size() < 5) {
       cudaEvent_t e;
@@ -2048,6 +2182,7 @@ class BatchPipeline {
     const size_t o_all = st.put(all);
     const dim3 g_rows(grid_x_for(maxnp_ * 32, W), W), g_el(grid_x_for(maxnp_ * maxnp_, W), W);
     const int dt = dtype_;
+    const bool lan = needs_lanczos();
     r.ops.push_back([=]() {
       const BWalk* wk = (const BWalk*)d_walks_.p;
       if (dt == FX_C64)
@@ -2057,10 +2192,13 @@ class BatchPipeline {
       FX_LAUNCH_CHECK();
       kb_walk_reduce<<<W, 256, 0, stream_>>>(dev<int>(o_all), wk, rowstat(), walkout());
       FX_LAUNCH_CHECK();
+      // with the Lanczos estimate recorded, an FP32 copy of Y for its mat-vecs (arena T1, free
+      // until phase 2)
+      float* y32 = lan ? (float*)A(kT1) : nullptr;
       if (dt == FX_C64)
-        kb_load_imag<float2><<<g_el, 256, 0, stream_>>>(dX(), dev<int>(o_all), wk, walkout(), A(kY));
+        kb_load_imag<float2><<<g_el, 256, 0, stream_>>>(dX(), dev<int>(o_all), wk, walkout(), A(kY), y32);
       else
-        kb_load_imag<double2><<<g_el, 256, 0, stream_>>>(dX(), dev<int>(o_all), wk, walkout(), A(kY));
+        kb_load_imag<double2><<<g_el, 256, 0, stream_>>>(dX(), dev<int>(o_all), wk, walkout(), A(kY), y32);
       FX_LAUNCH_CHECK();
     });
     r.launches += 3;
@@ -2068,22 +2206,27 @@ class BatchPipeline {
     // the mixed form's slice count, with the diagonals split off (the shifted generator's rows
     // are dominated by their diagonal, and its powers' even more)
     const bool psplit = form_ == 1 || (split_ & 4);
+    p46_recorded_ = needs_powers46();
+    const bool p46 = p46_recorded_;
     by_slices(all, [&](int w) { return reduced(w) ? pade_S_ : kS; }, [&](const std::vector<int>& l) {
       product(st, r, l, kY, kY, -1.0, -1, 0.0, 0.0, kA2, true, nullptr, nullptr, psplit);
+      if (!p46) return;
       product(st, r, l, kA2, kA2, 1.0, -1, 0.0, 0.0, kA4, true, nullptr, nullptr, psplit);
       product(st, r, l, kA4, kA2, 1.0, -1, 0.0, 0.0, kA6, true, nullptr, nullptr, psplit);
     });
-    const int arenas[3] = {kY, kA4, kA6};
+    // exact 1-norms of Y, A4, A6 into norms slots 0, 1, 2 (or of Y and A2 into slots 0 and 5)
+    const int arenas[3] = {kY, p46 ? kA4 : kA2, kA6}, slots[3] = {0, p46 ? 1 : 5, 2};
+    const int nnorm = p46 ? 3 : 2;
     r.ops.push_back([=]() {
       const BWalk* wk = (const BWalk*)d_walks_.p;
-      for (int k = 0; k < 3; ++k) {
+      for (int k = 0; k < nnorm; ++k) {
         kb_abs_rowsums<<<g_rows, 256, 0, stream_>>>(A(arenas[k]), dev<int>(o_all), wk, rsum());
         FX_LAUNCH_CHECK();
-        kb_walk_vec_reduce<<<W, 256, 0, stream_>>>(rsum(), dev<int>(o_all), wk, 1, 0, norms(), 8, k);
+        kb_walk_vec_reduce<<<W, 256, 0, stream_>>>(rsum(), dev<int>(o_all), wk, 1, 0, norms(), 8, slots[k]);
         FX_LAUNCH_CHECK();
       }
     });
-    r.launches += 6;
+    r.launches += 2 * nnorm;
     est_recorded_ = needs_estimates();
     if (est_recorded_) {
       estimate(st, r, all, kA4, kA4, 3);
@@ -2110,7 +2253,8 @@ class BatchPipeline {
       kb_lan_init<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), estst());
       FX_LAUNCH_CHECK();
       for (int j = 0; j < kLanSteps; ++j) {
-        kb_est_matvec<<<g_rows, 256, 0, stream_>>>(A(kY), dev<RChunk>(o_ch), wk, est_scr(), estst(), kEX0, kET0);
+        kb_est_matvec32<<<g_rows, 256, 0, stream_>>>((const float*)A(kT1), dev<RChunk>(o_ch), wk, est_scr(),
+                                                    estst(), kEX0, kET0);
         kb_lan_step<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), (double*)lanc_.p, j);
       }
       FX_LAUNCH_CHECK();
@@ -2656,13 +2800,13 @@ class BatchPipeline {
       const double* const* er_ = dev<const double*>(o_pre);
       const double* const* ei_ = dev<const double*>(o_pim);
       if (dt == FX_C64) {
-        kb_psi_sum<float2><<<W, 32, 0, stream_>>>(dP0(), l, wk, psum);
+        kb_psi_sum<float2><<<W, 256, 0, stream_>>>(dP0(), l, wk, psum);
         FX_LAUNCH_CHECK();
         kb_apply<float2><<<g_rows, 256, 0, stream_>>>(er_, ei_, dP0(), dP1(), l, wk, dev<double>(o_om), psum);
         FX_LAUNCH_CHECK();
         kb_output<float2><<<g_el, 256, 0, stream_>>>(er_, ei_, dUo(), l, wk, dev<double>(o_om));
       } else {
-        kb_psi_sum<double2><<<W, 32, 0, stream_>>>(dP0(), l, wk, psum);
+        kb_psi_sum<double2><<<W, 256, 0, stream_>>>(dP0(), l, wk, psum);
         FX_LAUNCH_CHECK();
         kb_apply<double2><<<g_rows, 256, 0, stream_>>>(er_, ei_, dP0(), dP1(), l, wk, dev<double>(o_om), psum);
         FX_LAUNCH_CHECK();
@@ -3568,9 +3712,9 @@ int fx_batch_walk_host(fx_batch_handle b, const void* const* X, const void* cons
       b->h_in.assign(3 * W, nullptr);
       for (size_t w = 0; w < W; ++w) {
         const size_t n = (size_t)b->ns[w];
-        FX_CUDA(cudaMalloc(&b->h_in[w], n * n * es));
-        FX_CUDA(cudaMalloc(&b->h_in[W + w], n * es));
-        FX_CUDA(cudaMalloc(&b->h_in[2 * W + w], n * es));
+        fx::dev_malloc(&b->h_in[w], n * n * es);
+        fx::dev_malloc(&b->h_in[W + w], n * es);
+        fx::dev_malloc(&b->h_in[2 * W + w], n * es);
       }
     }
     for (size_t w = 0; w < W; ++w) {

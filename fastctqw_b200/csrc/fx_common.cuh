@@ -3,8 +3,11 @@
 
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
+#include <mutex>
 #include <string>
 
 #include "fastctqw_b200.h"
@@ -39,6 +42,45 @@ struct Error {
   } while (0)
 
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+// Host-side fault injection for the failure-path tests: with FX_INJECT_ALLOC_FAIL=k in the
+// environment, the k-th workspace allocation (k = 0, 1, ...; counted from the first allocation
+// after the variable took its current value) fails as if the device were out of memory, so the
+// call returns FX_ERR_NOMEM.  Unset (or empty), nothing is injected.  No GPU fault is involved.
+inline bool inject_alloc_failure() {
+  static std::mutex mu;
+  static std::string last;
+  static long count = 0;
+  const char* v = getenv("FX_INJECT_ALLOC_FAIL");
+  std::lock_guard<std::mutex> lk(mu);
+  if (!v || !*v) {
+    last.clear();
+    return false;
+  }
+  if (last != v) {
+    last = v;
+    count = 0;
+  }
+  return count++ == strtol(v, nullptr, 10);
+}
+
+// cudaMalloc of a workspace: FX_ERR_NOMEM (not a CUDA error) when the device has no room, or
+// when FX_INJECT_ALLOC_FAIL selects this allocation.
+inline void dev_malloc(void** p, size_t bytes) {
+  if (inject_alloc_failure() || cudaMalloc(p, bytes) != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    throw Error{FX_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed"};
+  }
+}
+
+// NVTX range over a scope (named phases of a run in an Nsight timeline; free without a tool).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Device-side error word shared by all kernels of a handle (bit flags).
 enum DevErr : int {

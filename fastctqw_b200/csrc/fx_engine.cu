@@ -64,7 +64,7 @@ struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
   void alloc(size_t b) {
-    if (cudaMalloc(&p, b) != cudaSuccess) {
+    if (inject_alloc_failure() || cudaMalloc(&p, b) != cudaSuccess) {
       p = nullptr;
       cudaGetLastError();
       throw Error{FX_ERR_NOMEM, "device allocation of " + std::to_string(b) + " bytes failed"};
@@ -1115,7 +1115,7 @@ bool grouped_eligible(fx_handle h) {
 }
 bool input_is_walk_generator(fx_handle h, const void* dA, cudaStream_t s) {
   const int64_t n = h->n;
-  if (!h->check_buf) FX_CUDA(cudaMalloc(&h->check_buf, sizeof(double) * (6 * (size_t)n + 16)));
+  if (!h->check_buf) fx::dev_malloc(&h->check_buf, sizeof(double) * (6 * (size_t)n + 16));
   double* b = (double*)h->check_buf;
   fx::InputStats is{b, b + 2 * n, b + 4 * n, (int*)(b + 6 * n)};
   FX_CUDA(cudaMemsetAsync(is.flags, 0, sizeof(int) * 8, s));
@@ -1393,11 +1393,18 @@ int fx_run_host(fx_handle h, const void* A, void* U) {
     if (h->freed) throw fx::Error{FX_ERR_FREED, "handle was freed"};
     if (h->n == 0) return;
     const size_t bytes = (size_t)h->n * h->n * h->elem;
-    if (!h->h_in) FX_CUDA(cudaMalloc(&h->h_in, bytes));
-    if (!h->h_out) FX_CUDA(cudaMalloc(&h->h_out, bytes));
-    h->stage.h2d(h->h_in, A, bytes, h->stream);
+    if (!h->h_in) fx::dev_malloc(&h->h_in, bytes);
+    if (!h->h_out) fx::dev_malloc(&h->h_out, bytes);
+    {
+      fx::NvtxRange nr("fx_run_host: copy in");
+      h->stage.h2d(h->h_in, A, bytes, h->stream);
+    }
     h->u_valid = false;
-    run_device(h, h->h_in, h->h_out, nullptr, nullptr, h->stream);
+    {
+      fx::NvtxRange nr("fx_run_host: expm");
+      run_device(h, h->h_in, h->h_out, nullptr, nullptr, h->stream);
+    }
+    fx::NvtxRange nr("fx_run_host: copy out");
     h->stage.d2h(U, h->h_out, bytes, h->stream);
   });
 }
@@ -1409,9 +1416,9 @@ int fx_walk_host(fx_handle h, const void* A, const void* psi0, void* psi) {
     if (h->n == 0) return;
     const size_t bytes = (size_t)h->n * h->n * h->elem;
     const size_t vbytes = (size_t)h->n * ((h->dtype == FX_C128 || h->dtype == FX_F64) ? 16 : 8);
-    if (!h->h_in) FX_CUDA(cudaMalloc(&h->h_in, bytes));
-    if (!h->h_out) FX_CUDA(cudaMalloc(&h->h_out, bytes));
-    if (!h->h_psi) FX_CUDA(cudaMalloc(&h->h_psi, 2 * vbytes));
+    if (!h->h_in) fx::dev_malloc(&h->h_in, bytes);
+    if (!h->h_out) fx::dev_malloc(&h->h_out, bytes);
+    if (!h->h_psi) fx::dev_malloc(&h->h_psi, 2 * vbytes);
     char* dpsi0 = (char*)h->h_psi;
     char* dpsi = dpsi0 + vbytes;
     h->stage.h2d(h->h_in, A, bytes, h->stream);

@@ -97,6 +97,9 @@ def test_estimated_selection_takes_the_lanczos_bound():
     mu = float(np.trace(X.imag.astype(np.float64))) / n
     rho_true = float(np.max(np.abs(np.delete(lamn, np.argmin(np.abs(lamn))) - mu)))
     assert sp["lanczos"] <= rho_true * (1 + 1e-9) and rho_true <= rho
+    # phase 1 computed A2 only: the cap is min(||Y||_1, ||A2||_1^(1/2)), still rigorous
+    assert rho_true <= sp["upper_bound"]
+    assert st["gemm_launches"] < _walk(X, "plain", "chebyshev", selector="plain")[2]["gemm_launches"]
     plan = _native.chebyshev_plan(rho)
     assert (st["s"], st["degree"]) == (plan["s"], plan["degree"]), (st, plan)
     assert eo.rel_error(U, Uref) <= C64_REL

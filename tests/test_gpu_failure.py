@@ -44,3 +44,34 @@ def test_bounded_wait_runs_out_and_the_handle_recovers(launch):
     ref = (V * np.exp(1j * lam * float(np.float32(t)))) @ (V.T @ p0.astype(np.complex128))
     assert eo.infidelity(dp.cpu().numpy(), ref) <= 1e-10
     e.close()
+
+
+@pytest.mark.parametrize("k", [0, 1, 5])
+def test_injected_allocation_failure_is_a_memory_error(k, monkeypatch):
+    """FX_INJECT_ALLOC_FAIL=k makes the k-th workspace allocation fail as if the device were
+    full: the call raises MemoryError (FX_ERR_NOMEM), nothing is left half-built, and the same
+    handle (and a new batch) work once the variable is gone.  Host-side only: no GPU fault."""
+    from fastctqw_b200 import graphs
+    from fastctqw_b200.batch import WalkBatch
+    from fastctqw_b200.fastexpm import ExpMatComplex64
+    n, t = 200, 1.5
+    A = graphs.random_regular(n, 4, seed=3)
+    X = np.asarray(1j * A * np.float32(t), dtype=np.complex64)
+    ref = eo.propagator_eigh(-A.astype(np.float64), t)
+    e = ExpMatComplex64(n)
+    monkeypatch.setenv("FX_INJECT_ALLOC_FAIL", str(k))
+    with pytest.raises(MemoryError):
+        e.run(X)
+        for _ in range(8):   # later allocations of the first runs, until the k-th
+            e.run(X)
+    monkeypatch.delenv("FX_INJECT_ALLOC_FAIL")
+    assert eo.rel_error(e.run(X), ref) <= 1e-5
+    e.free()
+    monkeypatch.setenv("FX_INJECT_ALLOC_FAIL", str(k))
+    with pytest.raises(MemoryError):
+        b = WalkBatch([n, n // 2])
+        b.run([X, X[: n // 2, : n // 2]])
+    monkeypatch.delenv("FX_INJECT_ALLOC_FAIL")
+    with WalkBatch([n]) as b:
+        psi = b.run([X], [graphs.uniform_state(n)])[0]
+    assert eo.infidelity(psi.astype(np.complex128), ref @ graphs.uniform_state(n).astype(np.complex128)) <= 1e-10
