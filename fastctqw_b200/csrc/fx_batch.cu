@@ -424,6 +424,96 @@ __global__ void kb_apply_proj(double* E, const RChunk* ch, const BWalk* wk, cons
   }
 }
 
+// kb_combo2 by whole rows, a warp per row (chunks of whole rows, 8 warps per CTA), with the
+// signed row sums of D1 and D2 over the n x n block: rs1[row0 + i], rs2[row0 + i] (each lane sums
+// its columns in order, then a fixed shuffle tree: the same sums every run).
+__global__ void kb_combo2_rs(double* D1, double* D2, Planes5 M, const RChunk* ch, const BWalk* wk, const double* coef,
+                             double* rs1, double* rs2) {
+  const RChunk q = ch[blockIdx.x];
+  const BWalk b = wk[q.w];
+  const double* c = coef + 12 * q.w;
+  const double2* src[5];
+  double c1[5], c2[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const bool on = M.m[k] && (c[k] != 0.0 || c[6 + k] != 0.0);
+    c1[k] = on ? c[k] : 0.0;
+    c2[k] = on ? c[6 + k] : 0.0;
+    src[k] = on ? reinterpret_cast<const double2*>(M.m[k] + b.off) : nullptr;
+  }
+  const double g1 = c[5], g2 = c[11];
+  double2* d1 = reinterpret_cast<double2*>(D1 + b.off);
+  double2* d2 = reinterpret_cast<double2*>(D2 + b.off);
+  const int lane = threadIdx.x & 31, wpb = blockDim.x / 32;
+  const int64_t half = b.np / 2;
+  for (int64_t i = q.r0 + threadIdx.x / 32; i < q.r1; i += wpb) {
+    double s1 = 0.0, s2 = 0.0;
+    for (int64_t c2i = lane; c2i < half; c2i += 32) {
+      const int64_t e2 = i * half + c2i;   // double2 index of (i, 2 c2i)
+      double ax = 0.0, ay = 0.0, bx = 0.0, by = 0.0;
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        if (src[k]) {
+          const double2 m = src[k][e2];
+          ax += c1[k] * m.x;
+          ay += c1[k] * m.y;
+          bx += c2[k] * m.x;
+          by += c2[k] * m.y;
+        }
+      if (2 * c2i == i) {
+        ax += g1;
+        bx += g2;
+      } else if (2 * c2i + 1 == i) {
+        ay += g1;
+        by += g2;
+      }
+      d1[e2] = make_double2(ax, ay);
+      d2[e2] = make_double2(bx, by);
+      if (2 * c2i < b.n) {
+        s1 += ax;
+        s2 += bx;
+      }
+      if (2 * c2i + 1 < b.n) {
+        s1 += ay;
+        s2 += by;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0 && i < b.n) {
+      rs1[b.row0 + i] = s1;
+      rs2[b.row0 + i] = s2;
+    }
+  }
+}
+// The projection of both planes, E <- E - (r_i + r_j)/n + T/n^2 on the n x n block, over the
+// chunk's rows of the np x np block; with V, also V = E1 + E2 on the whole np x np block.
+__global__ void kb_apply_proj2(double* E1, double* E2, double* V, const RChunk* ch, const BWalk* wk, const double* rs1,
+                               const double* rs2, const double* tot1, const double* tot2) {
+  const RChunk q = ch[blockIdx.x];
+  const BWalk b = wk[q.w];
+  const double inv = 1.0 / b.n, sig1 = tot1[q.w] * inv * inv, sig2 = tot2[q.w] * inv * inv;
+  const double* r1 = rs1 + b.row0;
+  const double* r2 = rs2 + b.row0;
+  const uint32_t np = (uint32_t)b.np, total = (uint32_t)(q.r1 - q.r0) * np;
+  for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
+    const uint32_t ii = t / np, j = t - ii * np;
+    const int64_t i = q.r0 + (int64_t)ii;
+    const int64_t e = b.off + i * b.np + j;
+    double x = E1[e], y = E2[e];
+    if (i < b.n && j < (uint32_t)b.n) {
+      x = x - r1[i] * inv - r1[j] * inv + sig1;
+      y = y - r2[i] * inv - r2[j] * inv + sig2;
+      E1[e] = x;
+      E2[e] = y;
+    }
+    if (V) V[e] = x + y;
+  }
+}
+
 // Out-of-place transpose of every listed walk's np x np block (32 x 32 tiles).
 __global__ void kb_transpose(const double* in, double* out, const int* list, const BWalk* wk, int tiles_max) {
   const int w = list[blockIdx.z];
@@ -751,36 +841,35 @@ __global__ void kb_lan_init(const int* list, const BWalk* wk, double* scr, doubl
 }
 // After T_r = B X_r: alpha = T.v, w = T - alpha v - beta_prev v_prev, beta = |w|, v_prev <- v,
 // v <- w / beta (v <- 0 once the Krylov space is exhausted).
+// One block per (walk, run): blockIdx.x = 2 * (index in list) + run; blockDim a power of two up
+// to 1024.
 __global__ void kb_lan_step(const int* list, const BWalk* wk, double* scr, double* lan, int j) {
-  const int w = list[blockIdx.x];
+  const int w = list[blockIdx.x >> 1], r = blockIdx.x & 1;
   const BWalk b = wk[w];
-  __shared__ double sh[256];
-  for (int r = 0; r < 2; ++r) {
-    double* v = est_vec(scr, b, kEX0 + r);
-    const double* t = est_vec(scr, b, kET0 + r);
-    double* vp = est_vec(scr, b, kEY0 + r);
-    double* rec = lan + ((int64_t)w * 2 + r) * 2 * kLanSteps;
-    const double bprev = j > 0 ? rec[2 * (j - 1) + 1] : 0.0;
-    double a = 0.0;
-    for (int i = threadIdx.x; i < b.n; i += blockDim.x) a += t[i] * v[i];
-    a = block_reduce(a, sh, false);
-    double nn = 0.0;
-    for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
-      const double x = t[i] - a * v[i] - bprev * vp[i];
-      nn += x * x;
-    }
-    const double beta = sqrt(block_reduce(nn, sh, false));
-    const double scale = beta > 1e-300 ? 1.0 / beta : 0.0;
-    for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
-      const double x = t[i] - a * v[i] - bprev * vp[i];
-      vp[i] = v[i];
-      v[i] = x * scale;
-    }
-    if (threadIdx.x == 0) {
-      rec[2 * j] = a;
-      rec[2 * j + 1] = beta;
-    }
-    __syncthreads();
+  __shared__ double sh[1024];
+  double* v = est_vec(scr, b, kEX0 + r);
+  const double* t = est_vec(scr, b, kET0 + r);
+  double* vp = est_vec(scr, b, kEY0 + r);
+  double* rec = lan + ((int64_t)w * 2 + r) * 2 * kLanSteps;
+  const double bprev = j > 0 ? rec[2 * (j - 1) + 1] : 0.0;
+  double a = 0.0;
+  for (int i = threadIdx.x; i < b.n; i += blockDim.x) a += t[i] * v[i];
+  a = block_reduce(a, sh, false);
+  double nn = 0.0;
+  for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
+    const double x = t[i] - a * v[i] - bprev * vp[i];
+    nn += x * x;
+  }
+  const double beta = sqrt(block_reduce(nn, sh, false));
+  const double scale = beta > 1e-300 ? 1.0 / beta : 0.0;
+  for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
+    const double x = t[i] - a * v[i] - bprev * vp[i];
+    vp[i] = v[i];
+    v[i] = x * scale;
+  }
+  if (threadIdx.x == 0) {
+    rec[2 * j] = a;
+    rec[2 * j + 1] = beta;
   }
 }
 __device__ double block_reduce(double v, double* sh, bool take_max) {
@@ -1283,7 +1372,7 @@ class BatchPipeline {
     lanc_.alloc(sizeof(double) * (size_t)W * 4 * kLanSteps);
     // small: rowstat (kRS per row), estimator vectors (kEstScratch per row), row sums (1 per
     // row), per-walk records (8 + 8 + 4 + 8 + W ints)
-    small_.alloc(sizeof(double) * (size_t)(rows_ * (kRS + kEstScratch + 1) + (kWO + 8 + 4 + 8 + 8) * W + 64));
+    small_.alloc(sizeof(double) * (size_t)(rows_ * (kRS + kEstScratch + 2) + (kWO + 8 + 4 + 8 + 8) * W + 64));
     err_.alloc(sizeof(int) * 8);
     d_walks_.alloc(sizeof(BWalk) * W);
     FX_CUDA(cudaMemcpy(d_walks_.p, walks_.data(), sizeof(BWalk) * W, cudaMemcpyHostToDevice));
@@ -2012,7 +2101,8 @@ class BatchPipeline {
   double* rowstat() const { return (double*)small_.p; }
   double* est_scr() const { return rowstat() + kRS * rows_; }
   double* rsum() const { return est_scr() + kEstScratch * rows_; }
-  double* walkout() const { return rsum() + rows_; }
+  double* rsum2() const { return rsum() + rows_; }   // the imaginary plane's row sums
+  double* walkout() const { return rsum2() + rows_; }
   double* norms() const { return walkout() + kWO * count(); }
   double* estst() const { return norms() + 8 * count(); }
   double* misc() const { return estst() + 4 * count(); }   // 8 per walk: psum, projection totals
@@ -2255,7 +2345,7 @@ class BatchPipeline {
       for (int j = 0; j < kLanSteps; ++j) {
         kb_est_matvec32<<<g_rows, 256, 0, stream_>>>((const float*)A(kT1), dev<RChunk>(o_ch), wk, est_scr(),
                                                     estst(), kEX0, kET0);
-        kb_lan_step<<<nl, 256, 0, stream_>>>(l, wk, est_scr(), (double*)lanc_.p, j);
+        kb_lan_step<<<2 * nl, 1024, 0, stream_>>>(l, wk, est_scr(), (double*)lanc_.p, j);
       }
       FX_LAUNCH_CHECK();
     });
@@ -2611,6 +2701,71 @@ class BatchPipeline {
     r.launches += 3;
   }
 
+  // combo2 by whole rows (kb_combo2_rs) with the signed row sums of both outputs over the n x n
+  // block into rsum() and rsum2(), for the projection that follows a three-product squaring.
+  void combo2_rs(Staging& st, Rec& r, const std::vector<int>& list, int d1, int d2, const int m_arena[5],
+                 const std::vector<std::array<double, 12>>& coef) {
+    if (list.empty()) return;
+    std::vector<double> c(12 * count(), 0.0);
+    for (int w : list)
+      for (int k = 0; k < 12; ++k) c[12 * w + k] = coef[w][k];
+    std::vector<RChunk> ch;   // rows per chunk: a multiple of the 8 warps of a CTA
+    for (int w : list) {
+      const int np = walks_[w].np, R = std::max(8, (kChunkElems / np) & ~7);
+      for (int r0 = 0; r0 < np; r0 += R) ch.push_back(RChunk{w, r0, std::min(np, r0 + R), 0});
+    }
+    const size_t o_ch = st.put(ch), o_c = st.put(c);
+    Planes5 M{};
+    for (int k = 0; k < 5; ++k) M.m[k] = m_arena[k] >= 0 ? A(m_arena[k]) : nullptr;
+    double* D1 = A(d1);
+    double* D2 = A(d2);
+    const unsigned nch = (unsigned)ch.size();
+    r.launches += 1;
+    r.ops.push_back([=]() {
+      kb_combo2_rs<<<nch, 256, 0, stream_>>>(D1, D2, M, dev<RChunk>(o_ch), (const BWalk*)d_walks_.p, dev<double>(o_c),
+                                             rsum(), rsum2());
+      FX_LAUNCH_CHECK();
+    });
+  }
+
+  // Exact projection E 1 = 0 = 1^T E of both planes of the listed walks' iterates, from the row
+  // sums their squaring's combination wrote (combo2_rs), in one pass; walks with vready[w] also
+  // get Er + Ei in arena V for their next squaring (the same sums combo would form).
+  void project_fused(Staging& st, Rec& r, const std::vector<int>& list, const std::vector<int>& er,
+                     const std::vector<int>& ei, const std::vector<char>& vready) {
+    if (list.empty()) return;
+    const int W = count();
+    double* tot = misc();        // W doubles: the real plane's total
+    double* tot2 = misc() + W;   // W doubles: the imaginary plane's total
+    for (int pa : {kA4, kT1}) {
+      for (int withv = 0; withv < 2; ++withv) {
+        std::vector<int> l;
+        for (int w : list)
+          if (er[w] == pa && (int)vready[w] == withv) l.push_back(w);
+        if (l.empty()) continue;
+        const size_t o_l = st.put(l);
+        const int nl = (int)l.size();
+        double* E1 = A(er[l[0]]);
+        double* E2 = A(ei[l[0]]);
+        double* V = withv ? A(kV) : nullptr;
+        const std::vector<RChunk> ch = row_chunks(l, false);
+        const size_t o_ch = st.put(ch);
+        const unsigned nch = (unsigned)ch.size();
+        r.ops.push_back([=]() {
+          const BWalk* wk = (const BWalk*)d_walks_.p;
+          kb_walk_vec_reduce<<<nl, 256, 0, stream_>>>(rsum(), dev<int>(o_l), wk, 0, 1, tot, 1, 0);
+          FX_LAUNCH_CHECK();
+          kb_walk_vec_reduce<<<nl, 256, 0, stream_>>>(rsum2(), dev<int>(o_l), wk, 0, 1, tot2, 1, 0);
+          FX_LAUNCH_CHECK();
+          kb_apply_proj2<<<nch, 256, 0, stream_>>>(E1, E2, V, dev<RChunk>(o_ch), wk, rsum(), rsum2(), tot, tot2);
+          FX_LAUNCH_CHECK();
+        });
+        r.launches += 3;
+        (void)W;
+      }
+    }
+  }
+
   // Everything after the selection.
   void record_rest(Staging& st, Rec& r) {
     const int W = count();
@@ -2749,6 +2904,7 @@ class BatchPipeline {
       r.ops.push_back([=]() { FX_CUDA(cudaMemsetAsync(drift_buf_.p, 0, bytes, stream_)); });
     }
     tag_ = kTagSquare;
+    std::vector<char> vready(W, 0);   // walks whose Er + Ei (arena V) the projection formed
     for (int k = 0; k < smax; ++k) {
       std::vector<int> act;
       for (int w = 0; w < W; ++w)
@@ -2756,16 +2912,24 @@ class BatchPipeline {
       if (drift_) drift(st, r, act, er, ei, std::vector<int>(W, std::min(k, kDriftMax - 1)));
       std::vector<int> act3, act4;
       for (int w : act) (use_square3(w) ? act3 : act4).push_back(w);
-      if (!act3.empty()) square3(st, r, act3, er, ei, tr, ti, k);
+      if (!act3.empty()) square3(st, r, act3, er, ei, tr, ti, k, vready);
       if (!act4.empty()) square(st, r, act4, er, ei, tr, ti);
       for (int w : act) {
         std::swap(er[w], tr[w]);
         std::swap(ei[w], ti[w]);
       }
-      std::vector<int> pj;
-      for (int w : act)
-        if (rank1_[w]) pj.push_back(w);
-      project_pair(st, r, pj, er, ei);
+      // the projection of rank-one walks: after a three-product squaring with the row sums its
+      // combination took, both planes in one pass that also forms the next squaring's Er + Ei
+      // (not with the drift diagnostics, whose products use that arena in between)
+      std::vector<int> pj3, pj4;
+      std::fill(vready.begin(), vready.end(), 0);
+      for (int w : act) {
+        if (!rank1_[w]) continue;
+        (use_square3(w) ? pj3 : pj4).push_back(w);
+        if (use_square3(w) && !drift_ && sel_s_[w] > k + 1) vready[w] = 1;
+      }
+      project_fused(st, r, pj3, er, ei, vready);
+      project_pair(st, r, pj4, er, ei);
     }
     if (drift_) {
       std::vector<int> last(W);
@@ -3189,7 +3353,8 @@ class BatchPipeline {
   // would otherwise set the row exponent and cost the off-diagonal entries as many bits.
   // Scratch arenas (free during the squarings): V = Er + Ei, Y = t1, A6 = t2, W = t3.
   void square3(Staging& st, Rec& r, const std::vector<int>& act, const std::vector<int>& er,
-               const std::vector<int>& ei, const std::vector<int>& tr, const std::vector<int>& ti, int k) {
+               const std::vector<int>& ei, const std::vector<int>& tr, const std::vector<int>& ti, int k,
+               const std::vector<char>& vready) {
     const int W = count();
     for (int pa : {kA4, kT1}) {
       for (int S : {5, 4, 3}) {
@@ -3200,7 +3365,10 @@ class BatchPipeline {
         const int re = er[l[0]], im = ei[l[0]], ore = tr[l[0]], oim = ti[l[0]];
         std::vector<std::array<double, 5>> cf(W, {1.0, 1.0, 0.0, 0.0, 0.0});
         const int m_sum[4] = {re, im, -1, -1};
-        combo(st, r, l, kV, m_sum, cf);
+        std::vector<int> lv;   // Er + Ei not yet formed by the last projection
+        for (int w : l)
+          if (!vready[w]) lv.push_back(w);
+        combo(st, r, lv, kV, m_sum, cf);
         gS_ = S;
         product(st, r, l, re, re, 1.0, -1, 0.0, 0.0, kY, true, nullptr, nullptr, true);    // t1
         product(st, r, l, im, im, 1.0, -1, 0.0, 0.0, kA6, true, nullptr, nullptr, true);   // t2
@@ -3210,7 +3378,7 @@ class BatchPipeline {
         const int m_out[5] = {re, im, kY, kA6, kW};
         const std::vector<std::array<double, 12>> c2(
             W, std::array<double, 12>{2.0, 0.0, 1.0, -1.0, 0.0, 0.0, 0.0, 2.0, -1.0, -1.0, 1.0, 0.0});
-        combo2(st, r, l, ore, oim, m_out, c2);
+        combo2_rs(st, r, l, ore, oim, m_out, c2);
       }
     }
   }
