@@ -844,15 +844,19 @@ __global__ void __launch_bounds__(256, 3) k_slice_digits_planned(const GSlab* sl
                      (uintptr_t)(sb.ld * (int64_t)sizeof(TI))) & 15) == 0;
   const int64_t ld = out.ld;
   const double inv_gpr = 1.0 / (double)gpr;
+  // each thread takes two adjacent groups (8 columns) per step: when they lie in one row and
+  // its column offset is a multiple of 8, the digits of both go out as one 8-byte store per
+  // plane; otherwise group by group
+  const uint32_t end = min(first - threadIdx.x + (uint32_t)kPlanGroups, total);
 #pragma unroll 1
-  for (uint32_t g0 = first; g0 < first + kPlanGroups && g0 < total; g0 += 512) {
+  for (uint32_t g0 = first - threadIdx.x + 2u * threadIdx.x; g0 < end; g0 += 512) {
     double x[2][2][4] = {};
     uint32_t rr[2], kk[2];
     bool ok[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const uint32_t g = g0 + 256u * h;
-      ok[h] = g < total && g < first + kPlanGroups;
+      const uint32_t g = g0 + (uint32_t)h;
+      ok[h] = g < end;
       uint32_t q = 0;
       if (ok[h]) {   // g / gpr through the reciprocal (the FP64 pipe has room, the integer ALU not)
         q = (uint32_t)((double)g * inv_gpr);
@@ -866,33 +870,50 @@ __global__ void __launch_bounds__(256, 3) k_slice_digits_planned(const GSlab* sl
         if (im0) load4<TI>(im0 + (int64_t)rr[h] * sb.ld, kk[h], sb.K, vec, x[h][1]);
       }
     }
+    const bool pair = ok[1] && rr[0] == rr[1] && (kk[0] & 7) == 0;
+    double sc[2];
+    bool one[2];
+    int ex[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      if (!ok[h]) continue;
-      const int64_t row = (int64_t)sb.row0 + rr[h], k0 = kk[h];
-      const int64_t dcol = split ? (int64_t)rr[h] + sb.diag0 : -1;
-      const int e = out.exp[row];
-      bool one;
-      const double sc = scale_for(S, e, one);
+      ex[h] = ok[h] ? out.exp[(int64_t)sb.row0 + rr[h]] : 0;
+      sc[h] = scale_for(S, ex[h], one[h]);
+    }
 #pragma unroll
-      for (int plane = 0; plane < 2; ++plane) {
-        if (plane == 1 && !im0) continue;
-        uint32_t pk[kMaxSlices];
+    for (int plane = 0; plane < 2; ++plane) {
+      if (plane == 1 && !im0) continue;
+      uint32_t pk[2][kMaxSlices];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (!ok[h]) continue;
+        const int64_t dcol = split ? (int64_t)rr[h] + sb.diag0 : -1;
         double xs[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           double v = x[h][plane][j];
-          if (plane == 0 && k0 + j == dcol) v = 0.0;
-          xs[j] = one ? v * sc : ldexp(ldexp(v, -e), 7 * S);
+          if (plane == 0 && (int64_t)kk[h] + j == dcol) v = 0.0;
+          xs[j] = one[h] ? v * sc[h] : ldexp(ldexp(v, -ex[h]), 7 * S);
         }
-        cut_digits4(xs, S, pk);
+        cut_digits4(xs, S, pk[h]);
+      }
 #pragma unroll
-        for (int q = 0; q < kMaxSlices; ++q) {
-          if (q >= S) continue;
-          int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
-          if (dst) *reinterpret_cast<uint32_t*>(dst + row * ld + k0) = pk[q];
-          if (NEG && plane == 1 && out.neg_im[q])
-            *reinterpret_cast<uint32_t*>(out.neg_im[q] + row * ld + k0) = __vneg4(pk[q]);
+      for (int q = 0; q < kMaxSlices; ++q) {
+        if (q >= S) continue;
+        int8_t* dst = plane == 0 ? out.re[q] : out.im[q];
+        int8_t* ndst = (NEG && plane == 1) ? out.neg_im[q] : nullptr;
+        if (pair) {
+          const int64_t o = ((int64_t)sb.row0 + rr[0]) * ld + kk[0];
+          const uint2 v = make_uint2(pk[0][q], pk[1][q]);
+          if (dst) *reinterpret_cast<uint2*>(dst + o) = v;
+          if (ndst) *reinterpret_cast<uint2*>(ndst + o) = make_uint2(__vneg4(v.x), __vneg4(v.y));
+        } else {
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            if (!ok[h]) continue;
+            const int64_t o = ((int64_t)sb.row0 + rr[h]) * ld + kk[h];
+            if (dst) *reinterpret_cast<uint32_t*>(dst + o) = pk[h][q];
+            if (ndst) *reinterpret_cast<uint32_t*>(ndst + o) = __vneg4(pk[h][q]);
+          }
         }
       }
     }
