@@ -1748,7 +1748,8 @@ class BatchPipeline {
         outcome_[w] = 5;
         sel_m_[w] = m;
         sel_s_[w] = sq;
-        flops_ += 2.0 * N3 * (cp.cost - kChebSquareProducts * cp.s) + 8.0 * N3 * sq + 8.0 * N3;
+        // as for the Pade stage, every product counts as one generic complex GEMM
+        flops_ += 8.0 * N3 * (cp.cost - kChebSquareProducts * cp.s + sq) + 8.0 * N3;
         continue;
       }
       sel_m_[w] = m;
@@ -2471,9 +2472,13 @@ class BatchPipeline {
   // Real product D_w = alpha_w A_w B_w + beta_w C_w + gamma_w I on np x np blocks of the listed
   // walks (arenas; B symmetric so Bt = B); c_arena < 0: no C.
   // split: take the diagonals out of the int8 slices (operands close to a multiple of I).
+  // b_cached (a_cached): walks whose B (A) slices, exponents and split-off diagonals from an
+  // earlier product of the same operand, slice count and split are still in the B (A) planes:
+  // not sliced again.
   void product(Staging& st, Rec& r, const std::vector<int>& list, int a, int b, double alpha, int c_arena,
                double beta, double gamma, int d_arena, bool sym, const std::vector<double>* alpha_w = nullptr,
-               const std::vector<double>* gamma_w = nullptr, bool split = false) {
+               const std::vector<double>* gamma_w = nullptr, bool split = false,
+               const std::vector<char>* b_cached = nullptr, const std::vector<char>* a_cached = nullptr) {
     std::vector<GSlab> sa, sb;
     std::vector<GProblem> pr;
     const bool same = a == b;
@@ -2481,8 +2486,10 @@ class BatchPipeline {
     for (int w : list) {
       const BWalk& bw = walks_[w];
       const int dg = split ? 0 : kNoDiag;
-      sa.push_back(GSlab{A(a) + bw.off, nullptr, bw.np, bw.np, bw.np, (int)bw.row0, dg});
-      if (!same) sb.push_back(GSlab{A(b) + bw.off, nullptr, bw.np, bw.np, bw.np, (int)bw.row0, dg});
+      if (!(a_cached && (*a_cached)[w] && !same))
+        sa.push_back(GSlab{A(a) + bw.off, nullptr, bw.np, bw.np, bw.np, (int)bw.row0, dg});
+      if (!same && !(b_cached && (*b_cached)[w]))
+        sb.push_back(GSlab{A(b) + bw.off, nullptr, bw.np, bw.np, bw.np, (int)bw.row0, dg});
       GProblem p{};
       p.a_row0 = p.b_row0 = (int)bw.row0;
       p.M = p.N = p.K = bw.np;
@@ -3234,8 +3241,11 @@ class BatchPipeline {
     const int m_a2[5] = {kA2, -1, -1, -1, -1};
     for (int w : poly) cf[w] = {-2.0 * inv_rho[w] * inv_rho[w], 0.0, 0.0, 0.0, 0.0, -1.0};
     combo5(st, r, poly, kBaby[1], m_a2, cf);
-    // T_k = 2 T_i T_j - T_|i-j| (i + j = k): (i, j) = (1, 1), (1, 2), (2, 2), (2, 3)
+    // T_k = 2 T_i T_j - T_|i-j| (i + j = k): (i, j) = (1, 1), (1, 2), (2, 2), (2, 3).  T_2 and T_4
+    // square one operand (its slices in the A planes), which is then the A operand of T_3 and
+    // T_5: not sliced again
     static const int kPair[kChebMaxBaby + 1][2] = {{0, 0}, {0, 0}, {1, 1}, {1, 2}, {2, 2}, {2, 3}};
+    const std::vector<char> a_in(W, 1);
     for (int k = 2; k <= kChebMaxBaby; ++k) {
       std::vector<int> l;
       for (int w : poly)
@@ -3243,7 +3253,7 @@ class BatchPipeline {
       const int i = kPair[k][0], j = kPair[k][1], d = j - i;
       by_slices(l, ps, [&](const std::vector<int>& ls) {
         product(st, r, ls, kBaby[i], kBaby[j], 2.0, d > 0 ? kBaby[d] : -1, d > 0 ? -1.0 : 0.0, d > 0 ? 0.0 : -1.0,
-                kBaby[k], true, nullptr, nullptr, psplit);
+                kBaby[k], true, nullptr, nullptr, psplit, nullptr, i != j ? &a_in : nullptr);
       });
     }
     // odd cofactor of degree 0: Im E = (b_0 / rho) B
@@ -3273,6 +3283,10 @@ class BatchPipeline {
     int Lmax = 0;
     for (int w : list) Lmax = std::max(Lmax, (int)blk[w].size() - 1);
     std::vector<std::array<double, 6>> cf(W);
+    // G is the B operand of every step's product (G b = b G: both are polynomials in B): its
+    // slices, written to the B planes by a walk's first step, serve that walk's later steps
+    // (between them only combinations run, and they write no slices and not G)
+    std::vector<char> gsliced(W, 0);
     // r_g = sum_{j < m} r[g][j] T_j(C): planes T_1..T_4 (T_0 = I on the diagonal)
     const auto rg = [&](int w, int g, double last) {
       const auto& x = blk[w][g];
@@ -3299,8 +3313,9 @@ class BatchPipeline {
         for (int w : step)
           if (cheb_baby_[w] == m) l.push_back(w);
         by_slices(l, ps, [&](const std::vector<int>& ls) {
-          product(st, r, ls, kBaby[m], kRoll[(g + 1) % 3], g >= 1 ? 2.0 : 1.0, tmp, 1.0, 0.0, kRoll[g % 3], true,
-                  nullptr, nullptr, psplit);
+          product(st, r, ls, kRoll[(g + 1) % 3], kBaby[m], g >= 1 ? 2.0 : 1.0, tmp, 1.0, 0.0, kRoll[g % 3], true,
+                  nullptr, nullptr, psplit, &gsliced);
+          for (int w : ls) gsliced[w] = 1;
         });
       }
     }
