@@ -15,7 +15,10 @@
 #include <sched.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -37,23 +40,86 @@ int host_threads() {
   return std::max(1, std::min(n, 16));
 }
 
+// Process-wide workers for the host side of the chunked copies: started once, so that a
+// copy of N = 10000 (25 chunks of 32 MiB) does not start and join hundreds of threads.
+// run(n, f) calls f(0) .. f(n - 1), piece 0 on the caller's thread and the others on the
+// workers, and returns when all are done; one run at a time.
+class CopyPool {
+ public:
+  static CopyPool& get() {
+    static CopyPool pool(host_threads() - 1);
+    return pool;
+  }
+  int size() const { return (int)workers_.size() + 1; }
+  void run(int n, const std::function<void(int)>& f) {
+    std::lock_guard<std::mutex> one(run_mu_);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      job_ = &f;
+      pieces_ = n;
+      next_ = 1;
+      left_ = n - 1;
+      ++gen_;
+    }
+    cv_.notify_all();
+    if (n > 0) f(0);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return left_ <= 0; });
+    job_ = nullptr;
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : workers_) t.join();
+  }
+
+ private:
+  explicit CopyPool(int nworkers) {
+    for (int i = 0; i < nworkers; ++i) workers_.emplace_back([this] { loop(); });
+  }
+  void loop() {
+    unsigned long seen = 0;
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      cv_.wait(lk, [&] { return stop_ || (gen_ != seen && next_ < pieces_); });
+      if (stop_) return;
+      seen = gen_;
+      while (job_ && next_ < pieces_) {
+        const int i = next_++;
+        const std::function<void(int)>* f = job_;
+        lk.unlock();
+        (*f)(i);
+        lk.lock();
+        if (--left_ <= 0) done_cv_.notify_all();
+      }
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::mutex run_mu_, mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(int)>* job_ = nullptr;
+  int pieces_ = 0, next_ = 0, left_ = 0;
+  unsigned long gen_ = 0;
+  bool stop_ = false;
+};
+
 // memcpy split over up to host_threads() threads (page-aligned pieces).
 void parallel_memcpy(void* dst, const void* src, size_t bytes) {
-  const int nt = bytes < kParallelMin ? 1 : host_threads();
+  CopyPool& pool = CopyPool::get();
+  const int nt = bytes < kParallelMin ? 1 : pool.size();
   if (nt == 1) {
     std::memcpy(dst, src, bytes);
     return;
   }
   const size_t per = ((bytes + nt - 1) / nt + 4095) & ~(size_t)4095;
-  std::vector<std::thread> th;
-  th.reserve(nt);
-  for (int i = 0; i < nt; ++i) {
+  const int pieces = (int)((bytes + per - 1) / per);
+  pool.run(pieces, [&](int i) {
     const size_t o = (size_t)i * per;
-    if (o >= bytes) break;
-    const size_t len = std::min(per, bytes - o);
-    th.emplace_back([=] { std::memcpy((char*)dst + o, (const char*)src + o, len); });
-  }
-  for (auto& t : th) t.join();
+    std::memcpy((char*)dst + o, (const char*)src + o, std::min(per, bytes - o));
+  });
 }
 
 }  // namespace
