@@ -1158,6 +1158,10 @@ constexpr double kChebMaxA = 1024.0;     // larger a would need hundreds of prod
 // Margin on the Lanczos estimate where the selection uses it: outside [-1, 1] the truncated
 // series grows like cosh(D acosh|z|), so the interval must hold the whole spectrum.
 constexpr double kChebLanMargin = 0.25;
+// Error bound of the polynomial after the squarings: the phase tolerance of the selections
+// (1e-6) for complex64 walks; for complex128 walks one that leaves the int8 products' own
+// rounding (about 1e-11 per product) the larger error.
+constexpr double kChebTolC128 = 1e-12;
 
 // J_0(a) .. J_kmax(a), a >= 0, by Miller's backward recurrence J_{k-1} = (2k / a) J_k - J_{k+1}
 // from far above max(kmax, a), normalised by J_0 + 2 sum_{k>=1} J_2k = 1 (Abramowitz & Stegun
@@ -1738,7 +1742,7 @@ class BatchPipeline {
         const double rho_c = selector_ >= 2 && rho_lan_[w] > 0.0
                                  ? std::min(rho_up, rho_lan_[w] * (1.0 + kChebLanMargin))
                                  : rho_up;
-        const ChebPlan cp = cheb_plan(rho_c, kPhaseTol);
+        const ChebPlan cp = cheb_plan(rho_c, dtype_ == FX_C128 ? kChebTolC128 : kPhaseTol);
         if (!cp.ok) throw Error{FX_ERR_VALUE, "walk " + std::to_string(w) + ": no Chebyshev plan for a spectral bound this large"};
         m = 0;
         sq = cp.s;

@@ -135,7 +135,8 @@ enum fx_option {
                              solve); rho is the rigorous spectral bound min(||Y||_1, d4,
                              d6), or for the estimated and learned selections
                              min(that, 1.25 x the Lanczos estimate); (s, degree) are the
-                             cheapest plan of fx_chebyshev_plan at error 1e-6.  Reported
+                             cheapest plan of fx_chebyshev_plan at error 1e-6 (1e-12 for
+                             complex128 walks).  Reported
                              as m = 0, solver 3, fx_stats.degree, sel_outcome 5.  No
                              counterpart in the reference                             */
 };

@@ -163,3 +163,30 @@ def test_chebyshev_small_and_degenerate_walks():
         plan = co.plan(float(sp["upper_bound"][k]))
         assert int(s[k]) == plan["s"] and m[k] == 0, (k, s[k], plan)
     assert int(s[-1]) == 0 and np.allclose(outs[-1], graphs.uniform_state(33), atol=0, rtol=0)
+
+
+def test_chebyshev_complex128_walk_plans_a_tighter_bound():
+    """complex128 walks plan the polynomial at error 1e-12 (complex64 at 1e-6), so that the int8
+    products' own rounding stays the larger error: U within 1e-9 of the FP64 propagator."""
+    import torch
+    from fastctqw_b200 import _native, graphs
+    from fastctqw_b200._native import Engine
+    n = 600
+    A = graphs.erdos_renyi(n, 0.3, seed=8, dtype=np.float64)
+    L = np.diag(A.sum(axis=1)) - A
+    X = np.asarray(-1j * (-1.0 * L) * 3.0, dtype=np.complex128)
+    lam, V = np.linalg.eigh(X.imag)
+    Uref = (V * np.exp(1j * lam)) @ V.T
+    dev = torch.device("cuda", 0)
+    dX = torch.from_numpy(X).to(dev)
+    dU = torch.empty_like(dX)
+    e = Engine(n, np.complex128)
+    e.configure(form="plain", approx="chebyshev")
+    e.run_device(dX, dU)
+    torch.cuda.synchronize()
+    st, sp = e.stats(), e.spectral_radius()
+    e.close()
+    plan = _native.chebyshev_plan(sp["upper_bound"], 1e-12)
+    assert st["m"] == 0 and (st["s"], st["degree"]) == (plan["s"], plan["degree"]), (st, plan)
+    assert plan["cost"] >= _native.chebyshev_plan(sp["upper_bound"])["cost"]
+    assert eo.rel_error(dU.cpu().numpy(), Uref) <= 1e-9
