@@ -683,6 +683,12 @@ def main():
                        "shared memory, one CTA per SM, median of 5 launches; the higher of a measurement "
                        "before and one after the timed steps)",
         "peak_measurements": [round(i8_pre["tops"], 1), round(i8["tops"], 1)],
+        # under the 1000 W cap the random-operand measurement can run at a lower clock than the
+        # products (whose slices toggle fewer bits), so the line also gives the nominal dense int8
+        # rate (4.5 POP/s at 1965 MHz) scaled to the median SM clock of the timed steps
+        "nominal_at_clock": round(4500.0 * clk["sm_mhz"] / 1965.0, 1) if clk.get("sm_mhz") else None,
+        "frac_of_nominal_at_clock": (round(achieved / (4500.0 * clk["sm_mhz"] / 1965.0), 3)
+                                     if achieved and clk.get("sm_mhz") else None),
         "traffic": traffic["bytes"] if traffic else None,
         "traffic_source": traffic["source"] if traffic else None,
         "launches": pst["prod_launches"], "kernel_ms_per_walk": round(pst["prod_ms"], 3),

@@ -118,51 +118,6 @@ __global__ void kb_combo(double* D, PlanesN<NP> M, const RChunk* ch, const BWalk
 }
 using Planes4 = PlanesN<4>;
 
-// Two linear combinations of the same planes in one pass: D1 = sum_k c_k M_k (+ g1 on the
-// diagonal), D2 = sum_k d_k M_k (+ g2); coef[12 w ..] = (c_0..c_4, g1, d_0..d_4, g2).  A plane
-// whose coefficients are both zero is not read.
-__global__ void kb_combo2(double* D1, double* D2, Planes5 M, const RChunk* ch, const BWalk* wk, const double* coef) {
-  const RChunk q = ch[blockIdx.x];
-  const BWalk b = wk[q.w];
-  const double* c = coef + 12 * q.w;
-  const uint32_t half = (uint32_t)b.np / 2, total = (uint32_t)(q.r1 - q.r0) * half;
-  const double2* src[5];
-  double c1[5], c2[5];
-#pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    const bool on = M.m[k] && (c[k] != 0.0 || c[6 + k] != 0.0);
-    c1[k] = on ? c[k] : 0.0;
-    c2[k] = on ? c[6 + k] : 0.0;
-    src[k] = on ? reinterpret_cast<const double2*>(M.m[k] + b.off) : nullptr;
-  }
-  const double g1 = c[5], g2 = c[11];
-  double2* d1 = reinterpret_cast<double2*>(D1 + b.off);
-  double2* d2 = reinterpret_cast<double2*>(D2 + b.off);
-  for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
-    const uint32_t rr = t / half, c2i = t - rr * half;
-    const int64_t r = q.r0 + (int64_t)rr;
-    const int64_t e2 = r * half + c2i;   // double2 index of (r, 2 c2i)
-    double ax = 0.0, ay = 0.0, bx = 0.0, by = 0.0;
-#pragma unroll
-    for (int k = 0; k < 5; ++k)
-      if (src[k]) {
-        const double2 m = src[k][e2];
-        ax += c1[k] * m.x;
-        ay += c1[k] * m.y;
-        bx += c2[k] * m.x;
-        by += c2[k] * m.y;
-      }
-    if (2 * (int64_t)c2i == r) {
-      ax += g1;
-      bx += g2;
-    } else if (2 * (int64_t)c2i + 1 == r) {
-      ay += g1;
-      by += g2;
-    }
-    d1[e2] = make_double2(ax, ay);
-    d2[e2] = make_double2(bx, by);
-  }
-}
 
 // Statistics of the interleaved input of each walk, warp per row i < n:
 // rowstat[kRS * (row0 + i)] = (Re row sum, Im row sum, Re X_ii, Im X_ii, sum |Re| + |Im|,
@@ -424,9 +379,12 @@ __global__ void kb_apply_proj(double* E, const RChunk* ch, const BWalk* wk, cons
   }
 }
 
-// kb_combo2 by whole rows, a warp per row (chunks of whole rows, 8 warps per CTA), with the
-// signed row sums of D1 and D2 over the n x n block: rs1[row0 + i], rs2[row0 + i] (each lane sums
-// its columns in order, then a fixed shuffle tree: the same sums every run).
+// Two linear combinations of the same planes in one pass, D1 = sum_k c_k M_k (+ g1 on the
+// diagonal), D2 = sum_k d_k M_k (+ g2), coef[12 w ..] = (c_0..c_4, g1, d_0..d_4, g2) (a plane whose
+// coefficients are both zero is not read), by whole rows: a warp per row (chunks of whole rows,
+// 8 warps per CTA), with the signed row sums of D1 and D2 over the n x n block, rs1[row0 + i],
+// rs2[row0 + i] (each lane sums its columns in order, then a fixed shuffle tree: the same sums
+// every run).
 __global__ void kb_combo2_rs(double* D1, double* D2, Planes5 M, const RChunk* ch, const BWalk* wk, const double* coef,
                              double* rs1, double* rs2) {
   const RChunk q = ch[blockIdx.x];
@@ -1159,8 +1117,8 @@ constexpr double kChebMaxA = 1024.0;     // larger a would need hundreds of prod
 // series grows like cosh(D acosh|z|), so the interval must hold the whole spectrum.
 constexpr double kChebLanMargin = 0.25;
 // Error bound of the polynomial after the squarings: the phase tolerance of the selections
-// (1e-6) for complex64 walks; for complex128 walks one that leaves the int8 products' own
-// rounding (about 1e-11 per product) the larger error.
+// (1e-6) for complex64 walks; for complex128 walks a bound far below the int8 products' own
+// rounding (35-bit slices), so that the truncation never adds to it.
 constexpr double kChebTolC128 = 1e-12;
 
 // J_0(a) .. J_kmax(a), a >= 0, by Miller's backward recurrence J_{k-1} = (2k / a) J_k - J_{k+1}
@@ -1684,7 +1642,8 @@ class BatchPipeline {
       f[7] = std::log2(d6 + 1e-300);
     }
     std::vector<float> prop;
-    if (selector_ == 2) prop = infer_proposals();
+    // the network proposes Pade (m, s): not needed when every walk takes the polynomial
+    if (selector_ == 2 && needs_powers46()) prop = infer_proposals();
     for (int w = 0; w < W; ++w) {
       int m = plain_m_[w], sq = plain_s_[w];
       const double* nw = norms_.data() + 8 * w;
@@ -1704,7 +1663,7 @@ class BatchPipeline {
           sq = es;
           outcome_[w] = 3;
         }
-        if (selector_ == 2) {
+        if (selector_ == 2 && !prop.empty()) {
           // the learned proposal replaces the estimated choice when it is cheaper still and
           // passes the gate: the same phase bound at the phase error that keeps the
           // infidelity of every state below 1e-10
@@ -2640,26 +2599,7 @@ class BatchPipeline {
     });
   }
 
-  // Two combinations of up to five arenas in one pass (kb_combo2); coef per walk as there.
-  void combo2(Staging& st, Rec& r, const std::vector<int>& list, int d1, int d2, const int m_arena[5],
-              const std::vector<std::array<double, 12>>& coef) {
-    if (list.empty()) return;
-    std::vector<double> c(12 * count(), 0.0);
-    for (int w : list)
-      for (int k = 0; k < 12; ++k) c[12 * w + k] = coef[w][k];
-    const std::vector<RChunk> ch = row_chunks(list, false);
-    const size_t o_ch = st.put(ch), o_c = st.put(c);
-    Planes5 M{};
-    for (int k = 0; k < 5; ++k) M.m[k] = m_arena[k] >= 0 ? A(m_arena[k]) : nullptr;
-    double* D1 = A(d1);
-    double* D2 = A(d2);
-    const unsigned nch = (unsigned)ch.size();
-    r.launches += 1;
-    r.ops.push_back([=]() {
-      kb_combo2<<<nch, 256, 0, stream_>>>(D1, D2, M, dev<RChunk>(o_ch), (const BWalk*)d_walks_.p, dev<double>(o_c));
-      FX_LAUNCH_CHECK();
-    });
-  }
+
 
   void transpose(Staging& st, Rec& r, const std::vector<int>& list, int in, int out) {
     if (list.empty()) return;
