@@ -45,7 +45,11 @@ enum fx_status {
   FX_OK = 0,
   FX_ERR_TYPE = 1,      /* bad dtype / handle kind          -> Python TypeError   */
   FX_ERR_VALUE = 2,     /* bad size, shape, option value    -> Python ValueError  */
-  FX_ERR_NOMEM = 3,     /* device or host allocation failed -> Python MemoryError */
+  FX_ERR_NOMEM = 3,     /* device or host allocation failed -> Python MemoryError.  For
+                           tests of that path, the environment variable
+                           FX_INJECT_ALLOC_FAIL=k makes the k-th workspace allocation
+                           (counted from when the variable took its value) fail this
+                           way; no counterpart in the reference */
   FX_ERR_CUDA = 4,      /* CUDA runtime / launch error      -> RuntimeError       */
   FX_ERR_TIMEOUT = 5,   /* a bounded device wait ran out    -> RuntimeError       */
   FX_ERR_NONFINITE = 6, /* NaN/Inf in the input or a norm   -> ValueError         */
