@@ -34,6 +34,8 @@ nonzeros of a row), log2 rho_L, rank-one shift flag, log2 d4, log2 d6.
 """
 from __future__ import annotations
 
+import hashlib
+import json
 import ctypes
 import math
 import os
@@ -153,8 +155,35 @@ def min_certified_s(m: int, rho: float, tol: float = PHASE_TOL) -> int:
     return s
 
 
+CHUNK_KEYS = ("features", "plain_m", "plain_s", "cert_m", "cert_s", "label_m", "label_s", "infidelity_plain")
+
+
+def chunk_cache_path(cache_dir: str, index: int, **args) -> str:
+    """File of one chunk of a measured sweep, keyed by every argument that shapes it (the walks
+    come from a seeded generator, so the same arguments give the same chunk)."""
+    key = json.dumps(args, sort_keys=True)
+    h = hashlib.sha1(key.encode()).hexdigest()[:16]
+    return os.path.join(cache_dir, f"labels_{h}_chunk{index:04d}.npz")
+
+
+def save_chunk(path: str, arrays: dict, meta: list) -> None:
+    """Write a chunk atomically (a sweep killed while writing leaves no partial file)."""
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    tmp = path + ".part.npz"
+    np.savez(tmp, meta=np.array(json.dumps(meta)), **{k: arrays[k] for k in CHUNK_KEYS})
+    os.replace(tmp, path)
+
+
+def load_chunk(path: str) -> tuple[dict, list]:
+    with np.load(path, allow_pickle=False) as z:
+        arrays = {k: np.array(z[k]) for k in CHUNK_KEYS}
+        meta = [tuple(m) for m in json.loads(str(z["meta"]))]   # (kind, n, laplacian, t) per walk
+    return arrays, meta
+
+
 def make_dataset_measured(count: int, seed: int, nmin: int = 64, nmax: int = 2048, tmin: float = 0.1,
-                          tmax: float = 1000.0, chunk: int = 96, depth: int = 5, form: str = "plain") -> dict:
+                          tmax: float = 1000.0, chunk: int = 96, depth: int = 5, form: str = "plain",
+                          cache_dir: str | None = None) -> dict:
     """Walks of ``make_walks`` with labels measured on the GPU.
 
     Per chunk of walks: one analyze-only run (features, the Al-Mohy & Higham and the certified
@@ -165,86 +194,112 @@ def make_dataset_measured(count: int, seed: int, nmin: int = 64, nmax: int = 204
     certifies for that m.  (m, s) passes when the infidelity against the FP64 state is <= 1e-10
     (and no a-posteriori check redid the walk); the label is the cheapest (m, s) (products
     pi_m + s, ties to the larger m) whose s and every larger tested s pass.  The sweeps run in the
-    given precision form (the one the selection will serve)."""
-    import torch
-    from .batch import OPT_SAMPLE_WALKS, WalkBatch
-    dev = torch.device("cuda", 0)
+    given precision form (the one the selection will serve).
+
+    With ``cache_dir``, every finished chunk is written there (``chunk_cache_path``) and a chunk
+    found there is read back instead of measured again, so that an interrupted sweep resumes
+    where it stopped."""
     feats, pm_, ps_, cm_, cs_, lm_, ls_, meta, inf_plain = [], [], [], [], [], [], [], [], []
+    key_args = dict(count=count, seed=seed, nmin=nmin, nmax=nmax, tmin=tmin, tmax=tmax, chunk=chunk,
+                    depth=depth, form=form)
     it = make_walks(count, seed, nmin, nmax, tmin, tmax)
     todo = count
+    index = -1
     while todo > 0:
         k = min(chunk, todo)
         todo -= k
+        index += 1
         Xs, ms = [], []
         for _ in range(k):
             X, mt = next(it)
             Xs.append(X)
             ms.append(mt)
-        ns = [X.shape[0] for X in Xs]
-        with WalkBatch(ns, analyze_only=True) as b:
-            b.run(Xs)
-            d = b.details()
-        ru = rho_up(d["features"])
-        dX = [torch.from_numpy(X).to(dev) for X in Xs]
-        p0s, refs = [], []
-        for X in Xs:
-            lam, V = torch.linalg.eigh(torch.from_numpy(np.ascontiguousarray(X.imag, dtype=np.float64)).to(dev))
-            p = (V[:, -1] + V[:, 0]) / math.sqrt(2.0)
-            ref = (torch.exp(1j * lam[-1]) * V[:, -1] + torch.exp(1j * lam[0]) * V[:, 0]) / math.sqrt(2.0)
-            p0s.append(p.to(torch.complex64))
-            refs.append(ref)
-            del lam, V
-        outs = [torch.empty_like(p) for p in p0s]
-        sweep = WalkBatch(ns, form=form)
-        sweep.set_option(OPT_SAMPLE_WALKS, 0)
-
-        def infidelities():
-            sweep.run_device(dX, p0s, outs)
-            torch.cuda.synchronize()
-            oc = sweep.details()["outcome"]
-            r = []
-            for w in range(k):
-                q = outs[w].to(torch.complex128)
-                ov = torch.vdot(refs[w], q).abs() ** 2 / (torch.vdot(q, q).real * torch.vdot(refs[w], refs[w]).real)
-                r.append(1.0 if oc[w] == -2 else float(1.0 - ov))
-            return np.array(r)
-
-        inf_plain.append(infidelities())   # the plain selection's own result
-        best = [(PRODUCTS[int(d["plain_m"][w])] + int(d["plain_s"][w]), int(d["plain_m"][w]), int(d["plain_s"][w]))
-                for w in range(k)]
-        for m in DEGREES:
-            s_top = np.array([min_certified_s(m, float(r)) for r in ru])
-            ok = np.ones(k, dtype=bool)     # every s tested so far (from the top) passed
-            for kk in range(depth):
-                s_try = s_top - kk
-                active = ok & (s_try >= 0)
-                if not active.any():
-                    break
-                sweep.force_selection(np.full(k, m), np.maximum(s_try, 0))
-                inf = infidelities()
-                for w in np.nonzero(active)[0]:
-                    if inf[w] <= INFID_LABEL:
-                        cost = PRODUCTS[m] + int(s_try[w])
-                        if cost < best[w][0] or (cost == best[w][0] and m > best[w][1]):
-                            best[w] = (cost, m, int(s_try[w]))
-                    else:
-                        ok[w] = False
-        sweep.force_selection()
-        sweep.close()
-        feats.append(d["features"])
-        pm_.append(d["plain_m"])
-        ps_.append(d["plain_s"])
-        cm_.append(d["cert_m"])
-        cs_.append(d["cert_s"])
-        lm_.append(np.array([b_[1] for b_ in best], dtype=np.int32))
-        ls_.append(np.array([b_[2] for b_ in best], dtype=np.int32))
+        path = chunk_cache_path(cache_dir, index, **key_args) if cache_dir else None
+        if path and os.path.exists(path):
+            arrays, mt = load_chunk(path)
+            for lst, key in ((feats, "features"), (pm_, "plain_m"), (ps_, "plain_s"), (cm_, "cert_m"),
+                             (cs_, "cert_s"), (lm_, "label_m"), (ls_, "label_s"), (inf_plain, "infidelity_plain")):
+                lst.append(arrays[key])
+            meta.extend(mt)
+            continue
+        res = _measure_chunk(Xs, depth, form)
+        for lst, key in ((feats, "features"), (pm_, "plain_m"), (ps_, "plain_s"), (cm_, "cert_m"),
+                         (cs_, "cert_s"), (lm_, "label_m"), (ls_, "label_s"), (inf_plain, "infidelity_plain")):
+            lst.append(res[key])
         meta.extend(ms)
-        del dX, p0s, refs, outs
-        torch.cuda.empty_cache()
+        if path:
+            save_chunk(path, res, ms)
     cat = np.concatenate
     return {"features": cat(feats).astype(np.float32), "plain_m": cat(pm_), "plain_s": cat(ps_),
             "cert_m": cat(cm_), "cert_s": cat(cs_), "label_m": cat(lm_), "label_s": cat(ls_),
             "infidelity_plain": cat(inf_plain), "meta": np.array(meta, dtype=object)}
+
+
+def _measure_chunk(Xs: list, depth: int, form: str) -> dict:
+    """Labels of one chunk of walks by forced sweeps on the GPU (make_dataset_measured)."""
+    import torch
+    from .batch import OPT_SAMPLE_WALKS, WalkBatch
+    dev = torch.device("cuda", 0)
+    k = len(Xs)
+    ns = [X.shape[0] for X in Xs]
+    with WalkBatch(ns, analyze_only=True) as b:
+        b.run(Xs)
+        d = b.details()
+    ru = rho_up(d["features"])
+    dX = [torch.from_numpy(X).to(dev) for X in Xs]
+    p0s, refs = [], []
+    for X in Xs:
+        lam, V = torch.linalg.eigh(torch.from_numpy(np.ascontiguousarray(X.imag, dtype=np.float64)).to(dev))
+        p = (V[:, -1] + V[:, 0]) / math.sqrt(2.0)
+        ref = (torch.exp(1j * lam[-1]) * V[:, -1] + torch.exp(1j * lam[0]) * V[:, 0]) / math.sqrt(2.0)
+        p0s.append(p.to(torch.complex64))
+        refs.append(ref)
+        del lam, V
+    outs = [torch.empty_like(p) for p in p0s]
+    sweep = WalkBatch(ns, form=form)
+    sweep.set_option(OPT_SAMPLE_WALKS, 0)
+
+    def infidelities():
+        sweep.run_device(dX, p0s, outs)
+        torch.cuda.synchronize()
+        oc = sweep.details()["outcome"]
+        r = []
+        for w in range(k):
+            q = outs[w].to(torch.complex128)
+            ov = torch.vdot(refs[w], q).abs() ** 2 / (torch.vdot(q, q).real * torch.vdot(refs[w], refs[w]).real)
+            r.append(1.0 if oc[w] == -2 else float(1.0 - ov))
+        return np.array(r)
+
+    inf_plain = infidelities()   # the plain selection's own result
+    best = [(PRODUCTS[int(d["plain_m"][w])] + int(d["plain_s"][w]), int(d["plain_m"][w]), int(d["plain_s"][w]))
+            for w in range(k)]
+    for m in DEGREES:
+        s_top = np.array([min_certified_s(m, float(r)) for r in ru])
+        ok = np.ones(k, dtype=bool)     # every s tested so far (from the top) passed
+        for kk in range(depth):
+            s_try = s_top - kk
+            active = ok & (s_try >= 0)
+            if not active.any():
+                break
+            sweep.force_selection(np.full(k, m), np.maximum(s_try, 0))
+            inf = infidelities()
+            for w in np.nonzero(active)[0]:
+                if inf[w] <= INFID_LABEL:
+                    cost = PRODUCTS[m] + int(s_try[w])
+                    if cost < best[w][0] or (cost == best[w][0] and m > best[w][1]):
+                        best[w] = (cost, m, int(s_try[w]))
+                else:
+                    ok[w] = False
+    sweep.force_selection()
+    sweep.close()
+    res = {"features": np.asarray(d["features"], dtype=np.float32), "plain_m": d["plain_m"],
+           "plain_s": d["plain_s"], "cert_m": d["cert_m"], "cert_s": d["cert_s"],
+           "label_m": np.array([b_[1] for b_ in best], dtype=np.int32),
+           "label_s": np.array([b_[2] for b_ in best], dtype=np.int32),
+           "infidelity_plain": inf_plain}
+    del dX, p0s, refs, outs
+    torch.cuda.empty_cache()
+    return res
 
 
 def merge(*sets: dict) -> dict:

@@ -1,7 +1,7 @@
 """Train the learned (m, s) selector on the GPU from measured labels and write its weights and
 an evaluation report.
 
-    python -m fastctqw_b200.train_selector [--train 2048] [--test 512] [--epochs 120]
+    python -m fastctqw_b200.train_selector [--train 2048] [--test 512] [--epochs 120] [--cache-dir DIR]
 
 1. training and held-out sets from seeded walk generators (selector.make_walks), labelled by
    measured sweeps (selector.make_dataset_measured): every walk runs at a grid of forced (m, s),
@@ -109,14 +109,18 @@ def main(argv=None):
                     help="precision form of the measured sweeps (the form the selection serves)")
     ap.add_argument("--out", default=os.path.join(DATA, "selector_weights.npz"))
     ap.add_argument("--report", default=os.path.join(DATA, "selector_eval.json"))
+    ap.add_argument("--cache-dir", default=None,
+                    help="keep every measured chunk of labels here and read back the ones found, so that an "
+                         "interrupted sweep resumes where it stopped")
     a = ap.parse_args(argv)
     t0 = time.time()
-    ds_train = selector.merge(selector.make_dataset_measured(a.train, seed=1, nmax=a.nmax, form=a.form),
+    c = a.cache_dir
+    ds_train = selector.merge(selector.make_dataset_measured(a.train, seed=1, nmax=a.nmax, form=a.form, cache_dir=c),
                               selector.make_dataset_measured(a.train_large, seed=4, nmin=a.nmax,
-                                                             nmax=a.nmax_large, chunk=16, form=a.form))
-    ds_test = selector.merge(selector.make_dataset_measured(a.test, seed=2, nmax=a.nmax, form=a.form),
+                                                             nmax=a.nmax_large, chunk=16, form=a.form, cache_dir=c))
+    ds_test = selector.merge(selector.make_dataset_measured(a.test, seed=2, nmax=a.nmax, form=a.form, cache_dir=c),
                              selector.make_dataset_measured(a.test_large, seed=5, nmin=a.nmax,
-                                                            nmax=a.nmax_large, chunk=16, form=a.form))
+                                                            nmax=a.nmax_large, chunk=16, form=a.form, cache_dir=c))
     t1 = time.time()
     w, losses = selector.train(ds_train, epochs=a.epochs)
     t2 = time.time()

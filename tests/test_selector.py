@@ -120,3 +120,27 @@ def test_learned_gate_and_estimated_rule_use_the_lanczos_radius():
     cp = selector.PRODUCTS[int(m[0])] + s[0] - 1
     out = selector.gate(f, np.array([13]), np.array([cp - 6]), np.array([pm]), np.array([ps - 1]))
     assert out[0] == (-1 if selector.PRODUCTS[pm] + ps - 1 < cp else 0)
+
+
+def test_label_sweep_resumes_from_its_chunk_cache(tmp_path):
+    """A measured sweep keeps every finished chunk on disk, keyed by the sweep's arguments, and
+    reads back the chunks it finds: here every chunk is already there, so the sweep returns them
+    without touching a GPU, in order, with the walks' descriptions."""
+    from fastctqw_b200 import selector
+    args = dict(count=5, seed=11, nmin=64, nmax=96, tmin=0.1, tmax=1000.0, chunk=2, depth=5, form="plain")
+    walks = [mt for _, mt in selector.make_walks(5, 11, 64, 96, 0.1, 1000.0)]
+    sizes = (2, 2, 1)
+    start = 0
+    for index, k in enumerate(sizes):
+        arr = {key: np.arange(start, start + k, dtype=np.float64) for key in selector.CHUNK_KEYS}
+        arr["features"] = np.full((k, 8), float(index), dtype=np.float32)
+        path = selector.chunk_cache_path(str(tmp_path), index, **args)
+        selector.save_chunk(path, arr, walks[start:start + k])
+        start += k
+    other = selector.chunk_cache_path(str(tmp_path), 0, **dict(args, seed=12))
+    assert other != selector.chunk_cache_path(str(tmp_path), 0, **args)
+    ds = selector.make_dataset_measured(cache_dir=str(tmp_path), **args)
+    assert np.array_equal(ds["label_m"], np.arange(5))
+    assert ds["features"].shape == (5, 8) and list(ds["features"][:, 0]) == [0, 0, 1, 1, 2]
+    assert [tuple(m) for m in ds["meta"]] == walks
+    assert not any(p.name.endswith(".part.npz") for p in tmp_path.iterdir())
