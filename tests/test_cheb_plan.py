@@ -95,6 +95,9 @@ def test_plan_matches_the_cpu_statement():
         _native.chebyshev_plan(float("nan"))
     with pytest.raises(ValueError):
         _native.chebyshev_plan(1.0, 0.0)
+    with pytest.raises(ValueError):   # no s <= 60 brings a = rho / 2^s below 1024
+        _native.chebyshev_plan(1e25)
+    assert _native.chebyshev_plan(1e20)["s"] >= 50
 
 
 def test_plan_is_cheaper_than_pade_on_the_dense_walk():
