@@ -27,6 +27,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -1402,7 +1403,16 @@ int fx_run_host(fx_handle h, const void* A, void* U) {
     h->u_valid = false;
     {
       fx::NvtxRange nr("fx_run_host: expm");
-      run_device(h, h->h_in, h->h_out, nullptr, nullptr, h->stream);
+      // the caller's output array is usually fresh (numpy allocates it untouched): its page
+      // faults are taken on another thread while the device computes
+      std::thread pre([U, bytes] { fx::prefault_host(U, bytes); });
+      try {
+        run_device(h, h->h_in, h->h_out, nullptr, nullptr, h->stream);
+      } catch (...) {
+        pre.join();
+        throw;
+      }
+      pre.join();
     }
     fx::NvtxRange nr("fx_run_host: copy out");
     h->stage.d2h(U, h->h_out, bytes, h->stream);

@@ -133,6 +133,24 @@ bool host_is_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
+// Touches every page of a host buffer (one write per 4 KiB, split over the copy workers), so
+// that a fresh allocation takes its first-touch page faults at this point -- while the device
+// computes, when called from a thread of its own -- instead of inside the copy that fills it.
+// Page-locked and small buffers are left alone.  The bytes written are overwritten by that copy.
+void prefault_host(void* p, size_t bytes) {
+  if (bytes < kParallelMin || host_is_pinned(p)) return;
+  CopyPool& pool = CopyPool::get();
+  const int nt = pool.size();
+  const size_t per = ((bytes + nt - 1) / nt + 4095) & ~(size_t)4095;
+  const int pieces = (int)((bytes + per - 1) / per);
+  pool.run(pieces, [&](int i) {
+    volatile char* b = (volatile char*)p + (size_t)i * per;
+    const size_t len = std::min(per, bytes - (size_t)i * per);
+    for (size_t o = 0; o < len; o += 4096) b[o] = 0;
+    b[len - 1] = 0;
+  });
+}
+
 HostStage::~HostStage() { release(); }
 
 void HostStage::release() {

@@ -275,6 +275,8 @@ void batch_pipeline_spectral(const BatchPipeline* p, double* rho_lanczos, double
 // page-locked is copied by DMA directly; any other goes through two page-locked chunk buffers,
 // the host side of a chunk (split over threads) overlapping the DMA of the previous one.
 bool host_is_pinned(const void* p);
+// First touch of every page of a (pageable) host buffer, split over the copy workers.
+void prefault_host(void* p, size_t bytes);
 struct HostStage {
   void* buf[2] = {nullptr, nullptr};
   cudaEvent_t ev[2] = {nullptr, nullptr};
